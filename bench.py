@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of the grid hot path: multigrid Poisson solves per second.
+
+Workload (one "step"): a batch of B independent Poisson solves on a 128^3
+zero-boundary grid (N_c = 128, 127^3 unknowns, h = 0.2 Angstrom), each
+density a sum of 8 normalised Gaussians (widths U[0.5, 1.5] A, charges +-1,
+re-centred to neutral; seeded synthetic data), solved with the reference's
+method -- PoissonSolver(nn=3, relax='J'), the V-cycle schedule of
+gpaw/poisson.py -- from a zero start to relative residual
+||A phi - rho|| / ||rho|| <= 1e-10, i.e. the reference's own stopping test
+sum(r^2) dv <= eps with eps = 1e-20 sum(rho^2) dv.
+
+  value  solves/s over all ranks, inputs resident in HBM (device tensors)
+  e2e    the same through the public API with pinned host buffers: the
+         step's densities copied in and potentials copied out inside the
+         timed region
+  roofline  the level-0 weighted-Jacobi sweep (the dominant kernel),
+         timed live with CUDA events on its stream: algorithmic bytes
+         (read phi, read rho, write phi = 24 B per point) / launch time
+  cpu_baseline  the reference's own C (oracle/_ref) driven by the restated
+         solver, one solve per host core in parallel, rank 0 only
+
+--impl reference times that CPU implementation alone, as its own arm.
+Multi-GPU (torchrun): every rank solves its own batch (weak scaling); the
+only collective is the max-over-ranks of the timings.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 128
+H_ANG = 0.2
+N_GAUSS = 8
+REL_TOL = 1e-10
+METRIC = 'poisson_solves_per_s_128^3_rel1e-10'
+
+
+def densities(B, seed0):
+    from gpawdft_b200.workloads import gaussian_density
+    rhos = []
+    L = None
+    for i in range(B):
+        rho, L = gaussian_density(N_GRID, H_ANG, N_GAUSS, seed0 + i)
+        rhos.append(rho)
+    return np.array(rhos), L
+
+
+def eps_for(rho, dv):
+    return REL_TOL ** 2 * float(np.dot(rho.ravel(), rho.ravel())) * dv
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,'
+         'clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.Q,
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ''
+        sm, smax, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+                 'sw_power_cap']
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == 'active':
+                    reasons.add(nm)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': max(smax),
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+# ------------------------------------------------------------------ CPU side
+def _cpu_solve(args):
+    """One reference-C solve (process-pool worker)."""
+    seed, backend = args
+    from gpawdft_b200.workloads import gaussian_density
+    from oracle import layer
+    from oracle.geometry import GridDescriptor
+    rho, L = gaussian_density(N_GRID, H_ANG, N_GAUSS, seed)
+    gd = GridDescriptor((N_GRID,) * 3, (L,) * 3, 0)
+    ps = layer.PoissonSolver(nn=3, relax='J', eps=eps_for(rho, gd.dv),
+                             maxiter=1000, backend=backend)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    phi = gd.zeros()
+    t = time.perf_counter()
+    n = ps.solve(phi, rho)
+    return n, time.perf_counter() - t
+
+
+def cpu_arm(rounds, warmup, seed0=10_000):
+    """Rounds of one solve per host core; returns per-round solves/s."""
+    import multiprocessing as mp
+    from oracle import ref
+    backend = 'ref' if ref.available() else 'numpy'
+    kind = 'reference' if backend == 'ref' else 'port'
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    ctx = mp.get_context('spawn')
+    rates, niters = [], []
+    with ctx.Pool(cores) as pool:
+        for r in range(warmup + rounds):
+            args = [(seed0 + r * cores + i, backend) for i in range(cores)]
+            t = time.perf_counter()
+            res = pool.map(_cpu_solve, args)
+            dt = time.perf_counter() - t
+            if r >= warmup:
+                rates.append(cores / dt)
+                niters.extend(n for n, _ in res)
+    return {'rates': rates, 'cores': cores, 'kind': kind,
+            'sample': '%d rounds x %d concurrent %d^3 solves (one per core), '
+                      'reference C via the restated solver, %s' %
+                      (rounds, cores, N_GRID - 1,
+                       'oracle/_ref' if kind == 'reference' else 'NumPy port'),
+            'vcycles_mean': float(np.mean(niters)) if niters else None}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    r = cpu_arm(args.steps, args.warmup)
+    v = float(np.mean(r['rates']))
+    line = {'metric': METRIC, 'value': v, 'unit': 'solves/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': 1000.0 * r['cores'] / v,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f64', 'data': 'synthetic', 'impl': 'reference',
+            'config': config_dict(args, world, r['cores']),
+            'cpu_baseline': {'value': v, 'unit': 'solves/s',
+                             'cores': r['cores'], 'kind': r['kind'],
+                             'sample': r['sample']},
+            'e2e': {'value': v, 'unit': 'solves/s', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0},
+            'vcycles_mean': r['vcycles_mean']}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args, world, batch):
+    return {'workload': 'Poisson FD multigrid, N_c=%d zero boundary (%d^3 '
+                        'unknowns), h=%.2f A, nn=3 Jacobi, %d Gaussians, '
+                        'relative residual %g' % (N_GRID, N_GRID - 1, H_ANG,
+                                                  N_GAUSS, REL_TOL),
+            'batch_per_gpu': batch, 'grid': [N_GRID - 1] * 3,
+            'precision': args.precision, 'parallelism': 'dp%d' % world,
+            'l2': 'inputs larger than L2 (%d grids x %.1f MB per array)' %
+                  (batch, (N_GRID - 1) ** 3 * 8 / 1e6)}
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_ours(args, rank, world, dist):
+    import torch
+    from gpawdft_b200 import _lib
+    from gpawdft_b200.fd_operators import Laplace
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+
+    dev = torch.device('cuda', int(os.environ.get('LOCAL_RANK', 0)))
+    torch.cuda.set_device(dev)
+    B = args.batch
+    rho_h, L = densities(B, 1 + 1000 * rank)
+    gd = GridDescriptor((N_GRID,) * 3, (L,) * 3, 0)
+    eps = [eps_for(r, gd.dv) for r in rho_h]
+    ps = PoissonSolver(nn=3, relax='J', maxiter=1000, precision=args.precision,
+                       batch=B)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    lib = _lib.load()
+    rho_d = torch.from_numpy(rho_h).to(dev)
+    phi_d = torch.zeros_like(rho_d)
+    rho_pin = torch.from_numpy(rho_h).pin_memory()
+    phi_pin = torch.empty_like(rho_pin).pin_memory()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def stats():
+        import ctypes
+        k = ctypes.c_int64()
+        g = ctypes.c_int64()
+        lib.gpw_poisson_last_stats(ps._engine[0], ctypes.byref(k),
+                                   ctypes.byref(g))
+        return k.value, g.value
+
+    # ---- device-resident throughput
+    niters = None
+    for _ in range(args.warmup):
+        phi_d.zero_()
+        niters = ps.solve_batch(phi_d, rho_d, eps=eps)
+    barrier()
+    clk = ClockSampler(dev.index)
+    clk.start()
+    launches = 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        phi_d.zero_()
+        niters = ps.solve_batch(phi_d, rho_d, eps=eps)
+        launches += stats()[0]
+    e1.record(stream)
+    barrier()
+    clocks = clk.stop()
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+    value = world * B * args.steps / t_dev
+
+    # ---- end to end through the public API from pinned host memory
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        rho_d.copy_(rho_pin, non_blocking=True)
+        phi_d.zero_()
+        ps.solve_batch(phi_d, rho_d, eps=eps)
+        phi_pin.copy_(phi_d, non_blocking=True)
+        stream.synchronize()
+    f1.record(stream)
+    barrier()
+    t_e2e = max_over_ranks(f0.elapsed_time(f1) / 1000.0)
+    e2e = world * B * args.steps / t_e2e
+    nbytes = rho_h.nbytes
+
+    # ---- dominant kernel: level-0 weighted-Jacobi sweep over the batch
+    op = ps.operators[0]
+    npts = int(np.prod(gd.n_c))
+    reps = 10
+    op.relax(2, phi_d, rho_d, 2, 2.0 / 3.0)
+    torch.cuda.synchronize()
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for _ in range(reps):
+        op.relax(2, phi_d, rho_d, 2, 2.0 / 3.0)
+    k1.record(stream)
+    torch.cuda.synchronize()
+    t_sweep = k0.elapsed_time(k1) / 1000.0 / (2 * reps)
+    sweep_bytes = 3 * 8 * npts * B
+    achieved = sweep_bytes / t_sweep / 1e9
+    peak, peak_src = measured_peak()
+
+    # ---- secondary: config (a) Laplace apply, 32 x 48^3 float64, zero BC
+    stencil = stencil_config_a(dev, stream)
+
+    out = {'metric': METRIC, 'value': value, 'unit': 'solves/s',
+           'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+           'ms_per_step': 1000.0 * t_dev / args.steps,
+           'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+           'dtype': 'f64' if args.precision == 'fp64' else 'f32+f64',
+           'data': 'synthetic (seeded Gaussian-sum densities)',
+           'config': config_dict(args, world, B),
+           'e2e': {'value': e2e, 'unit': 'solves/s',
+                   'h2d_bytes_per_step': nbytes,
+                   'd2h_bytes_per_step': nbytes},
+           'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+                        'unit': 'GB/s', 'frac': achieved / peak,
+                        'traffic': None,
+                        'kernel': 'star_stencil_kernel<double,3,JACOBI> '
+                                  '(level-0 sweep, batch %d)' % B,
+                        'algorithmic_bytes_per_launch': sweep_bytes,
+                        'launch_ms': t_sweep * 1e3,
+                        'peak_source': peak_src},
+           'gpu_launches': int(launches),
+           'clocks': clocks,
+           'vcycles': [int(x) for x in niters],
+           'stencil_config_a': stencil}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r = cpu_arm(1, 0)
+        out['cpu_baseline'] = {'value': float(np.mean(r['rates'])),
+                               'unit': 'solves/s', 'cores': r['cores'],
+                               'kind': r['kind'], 'sample': r['sample']}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def measured_peak():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(p) as f:
+            return float(json.load(f)['hbm_gbs']), 'MEASURED_PEAKS.json hbm_gbs (measured)'
+    except Exception:
+        return 6650.0, 'fallback 6.65 TB/s'
+
+
+def stencil_config_a(dev, stream):
+    """Laplace nn=3 apply on 32 x 48^3 float64 (and a 16x batch): GB/s."""
+    import torch
+    from gpawdft_b200.fd_operators import Laplace
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    h = 0.2 / 0.52917721
+    gd = GridDescriptor((49,) * 3, (49 * h,) * 3, 0)
+    op = Laplace(gd, 1.0, 3)
+    res = {}
+    peak, _ = measured_peak()
+    for nb in (32, 512):
+        g = torch.Generator(device=dev).manual_seed(0)
+        a = torch.randn((nb, 48, 48, 48), dtype=torch.float64, device=dev,
+                        generator=g)
+        o = torch.empty_like(a)
+        for _ in range(3):
+            op.apply(a, o)
+        torch.cuda.synchronize()
+        reps = 20 if nb == 32 else 5
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            op.apply(a, o)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1000.0 / reps
+        gbs = 2 * a.numel() * 8 / t / 1e9
+        res['batch%d' % nb] = {'ms': t * 1e3, 'GB/s': gbs, 'frac': gbs / peak,
+                               'l2_resident': nb == 32}
+        del a, o
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--batch', type=int, default=16)
+    ap.add_argument('--precision', default='fp64', choices=['fp64', 'fp32'])
+    ap.add_argument('--no-cpu', action='store_true',
+                    help='skip the cpu_baseline sample')
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == 'ours' else args.warmup
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    dist = None
+    if world > 1 and args.impl == 'ours':
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        tdist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

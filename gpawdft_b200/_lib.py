@@ -1,0 +1,111 @@
+"""ctypes binding of the C ABI in include/gpwgrid.h (libgpwgrid.so).
+
+This is the same binding a reference-side maintainer would add to call the
+library from GPAW's Python layer.  Loading fails loudly: there is no CPU
+fallback for any entry point.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libgpwgrid.so')
+
+GPW_OK = 0
+GPW_ENOMEM = 12
+GPW_EINVAL = 22
+GPW_ENOTSUP = 95
+GPW_ETIMEDOUT = 110
+GPW_ECONV = 1001
+GPW_ECUDA = 1002
+
+GPW_F64, GPW_C128, GPW_F32, GPW_C64 = 0, 1, 2, 3
+
+# every symbol include/gpwgrid.h declares
+EXPORTS = [
+    'gpw_last_error', 'gpw_version',
+    'gpw_operator_new', 'gpw_operator_apply', 'gpw_operator_relax',
+    'gpw_operator_get_diagonal_element', 'gpw_operator_residual',
+    'gpw_operator_free',
+    'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
+    'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_add_scalar',
+    'gpw_poisson_new', 'gpw_poisson_solve', 'gpw_poisson_last_stats',
+    'gpw_poisson_free',
+]
+
+_c_i64p = ctypes.POINTER(ctypes.c_int64)
+_c_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+_SIGS = {
+    'gpw_last_error': (ctypes.c_char_p, []),
+    'gpw_version': (ctypes.c_char_p, []),
+    'gpw_operator_new': (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp,
+                                        ctypes.c_int, _vp, ctypes.c_int,
+                                        ctypes.c_int, ctypes.POINTER(_vp)]),
+    'gpw_operator_apply': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp,
+                                          ctypes.c_int64, _vp, _vp]),
+    'gpw_operator_relax': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int,
+                                          _vp, _vp, ctypes.c_int64,
+                                          ctypes.c_int, ctypes.c_double,
+                                          _vp]),
+    'gpw_operator_get_diagonal_element': (ctypes.c_int, [_vp, _c_dp]),
+    'gpw_operator_residual': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp,
+                                             ctypes.c_int64, _vp, _vp]),
+    'gpw_operator_free': (None, [_vp]),
+    'gpw_transformer_new': (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp,
+                                           _vp, _vp, ctypes.c_int,
+                                           ctypes.c_int, ctypes.POINTER(_vp)]),
+    'gpw_transformer_apply': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp,
+                                             ctypes.c_int64, _vp, _vp]),
+    'gpw_transformer_free': (None, [_vp]),
+    'gpw_axpy': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_double,
+                                ctypes.c_double, _vp, _vp, _vp]),
+    'gpw_scal': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_double,
+                                ctypes.c_double, _vp, _vp]),
+    'gpw_sum': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
+                               _vp, _vp, _vp]),
+    'gpw_dot': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
+                               _vp, _vp, _vp, _vp]),
+    'gpw_add_scalar': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64,
+                                      ctypes.c_double, _vp, _vp, _vp]),
+    'gpw_poisson_new': (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
+                                       _vp, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_int64, ctypes.POINTER(_vp)]),
+    'gpw_poisson_solve': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, _vp,
+                                         ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                         _vp]),
+    'gpw_poisson_last_stats': (ctypes.c_int, [_vp, _vp, _vp]),
+    'gpw_poisson_free': (None, [_vp]),
+}
+
+_lib = None
+
+
+class GPWError(RuntimeError):
+    def __init__(self, code, msg):
+        RuntimeError.__init__(self, '%s (code %d)' % (msg, code))
+        self.code = code
+
+
+def load():
+    """Load libgpwgrid.so (built in-tree) and declare its signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError('libgpwgrid.so is not built (run '
+                          '`python -m gpawdft_b200.build`); there is no CPU '
+                          'fallback')
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGS.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != GPW_OK:
+        msg = load().gpw_last_error().decode()
+        raise GPWError(rc, msg)

@@ -1,0 +1,131 @@
+// Host-side internal interfaces shared by the C ABI (gpw_api.cu), the kernel
+// launchers (gpw_launch.cu) and the multigrid engine (gpw_poisson.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "gpw_common.cuh"
+#include "gpw_reduce.cuh"
+#include "gpw_stencil.cuh"
+
+namespace gpw {
+
+// Thread-local error message behind gpw_last_error().
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+inline size_t elt_size(int dtype) {
+  switch (dtype) {
+    case GPW_F64: return 8;
+    case GPW_C128: return 16;
+    case GPW_F32: return 4;
+    case GPW_C64: return 8;
+  }
+  return 0;
+}
+inline bool is_complex(int dtype) { return dtype == GPW_C128 || dtype == GPW_C64; }
+inline bool valid_dtype(int dtype) { return dtype >= 0 && dtype <= 3; }
+
+inline GridView contiguous_view(const int n[3]) {
+  GridView v;
+  v.n[0] = n[0];
+  v.n[1] = n[1];
+  v.n[2] = n[2];
+  v.s1 = n[2];
+  v.s0 = (int64_t)n[1] * n[2];
+  v.sb = (int64_t)n[0] * n[1] * n[2];
+  return v;
+}
+inline int64_t view_points(const GridView& v) { return (int64_t)v.n[0] * v.n[1] * v.n[2]; }
+
+// ---------------------------------------------------------------- operator
+struct OpDesc {
+  int n[3];
+  int mp;
+  int periodic[3];
+  int real, cfd;
+  int ncoef;
+  std::vector<double> coefs;
+  std::vector<int> off;  // ncoef * 3
+  bool star;             // star kernel eligible for APPLY / RESIDUAL
+  bool star_jacobi;      // star kernel eligible for JACOBI (centre first, unique)
+  int R;                 // star radius
+  StarCoefs sc;
+  GeneralCoefs gc;
+  double diag;           // get_diagonal_element
+};
+
+int build_opdesc(OpDesc& d, const double* coefs, const int64_t* offsets, int ncoef, const int64_t size[3],
+                 int range, const int64_t neighbors[6], int real, int cfd);
+
+// Fill the boundary description for an op / transformer input grid.
+Boundary make_boundary(const int periodic[3], int dtype, const double* phases);
+
+// Number of CTAs per batch member the stencil launch will use (for sizing the
+// residual partial buffer) and the launch itself.
+int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& vout, int nbatch);
+cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, void* out,
+                           const GridView& vout, const void* rho, const GridView& vrho, int nbatch,
+                           const Boundary& bc, double w, const unsigned char* active, const GridSum& gs,
+                           cudaStream_t st);
+
+// ---------------------------------------------------------------- transformer
+struct TrDesc {
+  int nin[3], nout[3];
+  int k;
+  int pad[3][2], npad[3][2], skip[3][2];
+  int periodic[3];
+  int real, interpolate;
+};
+
+// subtract != 0 (interpolation only): out = base - I(in); base may alias out.
+cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const GridView& vin, void* out,
+                            const GridView& vout, int nbatch, const Boundary& bc, int subtract,
+                            const void* base, const GridView* vbase, const unsigned char* active,
+                            cudaStream_t st);
+
+// ---------------------------------------------------------------- blas
+cudaError_t launch_axpy(int dtype, int64_t n, double ar, double ai, const void* x, void* y, cudaStream_t st);
+cudaError_t launch_scal(int dtype, int64_t n, double ar, double ai, void* x, cudaStream_t st);
+cudaError_t launch_reduce(int dtype, int op, int64_t nvec, int64_t n, const void* x, const void* y,
+                          const GridSum& gs, int nblk, cudaStream_t st);
+int reduce_blocks(int64_t n);
+cudaError_t launch_add_scalar(int dtype, int64_t n, double c, const void* x, void* y, cudaStream_t st);
+cudaError_t launch_zero(int dtype, const GridView& v, void* x, int nbatch, const unsigned char* active,
+                        cudaStream_t st);
+
+// Device workspace that grows on demand (stream-ordered frees are avoided:
+// growth synchronises the device first).
+struct Workspace {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need);
+  Workspace() = default;
+  Workspace(const Workspace&) = delete;
+  Workspace& operator=(const Workspace&) = delete;
+  Workspace(Workspace&& o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+    o.ptr = nullptr;
+    o.bytes = 0;
+  }
+  ~Workspace();
+};
+
+// Per-reduction scratch: partials + counters + results.
+struct SumScratch {
+  Workspace partial, counter, result;
+  int ensure(int64_t nseg, int64_t nblk_seg);
+  GridSum gs() const {
+    GridSum g;
+    g.partial = (double*)partial.ptr;
+    g.counter = (unsigned*)counter.ptr;
+    g.result = (double*)result.ptr;
+    return g;
+  }
+};
+
+int num_sms();
+
+}  // namespace gpw

@@ -1,0 +1,330 @@
+// Kernel launchers: dtype / radius / tap-count dispatch, launch geometry and
+// shared-memory opt-in for every device kernel of the library.
+#include <algorithm>
+#include <mutex>
+
+#include "gpw_blas.cuh"
+#include "gpw_internal.h"
+#include "gpw_stencil.cuh"
+#include "gpw_transfer.cuh"
+
+namespace gpw {
+
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+// Dynamic shared memory above 48 KB needs a one-time opt-in per kernel.
+template <typename F>
+static cudaError_t smem_optin(F* kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Chunking of axis 0: enough CTAs for ~4 per SM, but never chunks shorter
+// than `minz` planes (each chunk re-reads a 2R-plane warm-up).
+static void choose_chunks(int n0, int64_t tiles, int minz, int& zchunk, int& nchunk) {
+  const int64_t want = 4LL * num_sms();
+  int64_t nc = (want + tiles - 1) / std::max<int64_t>(tiles, 1);
+  const int64_t maxc = std::max(1, (n0 + minz - 1) / minz);
+  nc = std::max<int64_t>(1, std::min<int64_t>(nc, maxc));
+  zchunk = (int)((n0 + nc - 1) / nc);
+  nchunk = (n0 + zchunk - 1) / zchunk;
+}
+
+// ------------------------------------------------------------------ stencils
+template <typename T, int R, int MODE>
+static cudaError_t run_star(const StencilArgs& a0, const OpDesc& d, int nbatch, cudaStream_t st) {
+  using C = StarCfg<R, T>;
+  StencilArgs a = a0;
+  const GridView& v = a.vout;
+  dim3 grid((v.n[2] + C::TZ - 1) / C::TZ, (v.n[1] + C::TY - 1) / C::TY, 1);
+  choose_chunks(v.n[0], (int64_t)grid.x * grid.y * nbatch, 2 * R + 2, a.zchunk, a.nchunk);
+  grid.z = a.nchunk * nbatch;
+  a.nblk_seg = grid.x * grid.y * a.nchunk;
+  const size_t smem = (size_t)C::NSTAGE * C::PS * sizeof(T);
+  auto kern = star_stencil_kernel<T, R, MODE>;
+  static std::once_flag once;
+  cudaError_t e = cudaSuccess;
+  std::call_once(once, [&] { e = smem_optin(kern, smem); });
+  if (e != cudaSuccess) return e;
+  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, d.sc);
+  return cudaGetLastError();
+}
+
+template <typename T, int MODE>
+static cudaError_t run_general(const StencilArgs& a0, const OpDesc& d, int nbatch, cudaStream_t st) {
+  StencilArgs a = a0;
+  const GridView& v = a.vout;
+  const int mp = d.mp;
+  dim3 grid((v.n[2] + GEN_TZ - 1) / GEN_TZ, (v.n[1] + GEN_TY - 1) / GEN_TY, 1);
+  choose_chunks(v.n[0], (int64_t)grid.x * grid.y * nbatch, 2 * mp + 2, a.zchunk, a.nchunk);
+  grid.z = a.nchunk * nbatch;
+  a.nblk_seg = grid.x * grid.y * a.nchunk;
+  const size_t smem = (size_t)(2 * mp + 2) * (GEN_TY + 2 * mp) * (GEN_TZ + 2 * mp) * sizeof(T);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  auto kern = general_stencil_kernel<T, MODE>;
+  static std::once_flag once;
+  cudaError_t e = cudaSuccess;
+  std::call_once(once, [&] { e = smem_optin(kern, 227 * 1024); });
+  if (e != cudaSuccess) return e;
+  kern<<<grid, dim3(GEN_TZ, GEN_TY), smem, st>>>(a, d.gc);
+  return cudaGetLastError();
+}
+
+template <typename T, int MODE>
+static cudaError_t dispatch_star(const StencilArgs& a, const OpDesc& d, int nbatch, cudaStream_t st) {
+  switch (d.R) {
+    case 1: return run_star<T, 1, MODE>(a, d, nbatch, st);
+    case 2: return run_star<T, 2, MODE>(a, d, nbatch, st);
+    case 3: return run_star<T, 3, MODE>(a, d, nbatch, st);
+    case 4: return run_star<T, 4, MODE>(a, d, nbatch, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T, int MODE>
+static cudaError_t dispatch_mode(const StencilArgs& a, const OpDesc& d, int nbatch, cudaStream_t st) {
+  const bool use_star = (MODE == MODE_JACOBI) ? d.star_jacobi : d.star;
+  if (use_star) return dispatch_star<T, MODE>(a, d, nbatch, st);
+  return run_general<T, MODE>(a, d, nbatch, st);
+}
+
+static bool star_radius_ok(int R) { return R >= 1 && R <= 4; }
+
+int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& v, int nbatch) {
+  const bool use_star = ((mode == MODE_JACOBI) ? d.star_jacobi : d.star) && star_radius_ok(d.R);
+  int tz, ty, minz;
+  if (use_star) {
+    tz = 32;
+    ty = 32;
+    minz = 2 * d.R + 2;
+  } else {
+    tz = GEN_TZ;
+    ty = GEN_TY;
+    minz = 2 * d.mp + 2;
+  }
+  const int gx = (v.n[2] + tz - 1) / tz, gy = (v.n[1] + ty - 1) / ty;
+  int zc, nc;
+  choose_chunks(v.n[0], (int64_t)gx * gy * nbatch, minz, zc, nc);
+  return gx * gy * nc;
+}
+
+cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, void* out,
+                           const GridView& vout, const void* rho, const GridView& vrho, int nbatch,
+                           const Boundary& bc, double w, const unsigned char* active, const GridSum& gs,
+                           cudaStream_t st) {
+  StencilArgs a{};
+  a.in = in;
+  a.out = out;
+  a.rho = rho;
+  a.vin = vin;
+  a.vout = vout;
+  a.vrho = vrho;
+  a.bc = bc;
+  a.w = w;
+  a.c0 = d.coefs.empty() ? 1.0 : d.coefs[0];
+  a.active = active;
+  a.gsum = gs;
+  OpDesc dd = d;
+  if (!star_radius_ok(dd.R)) {
+    dd.star = false;
+    dd.star_jacobi = false;
+  }
+  switch (mode) {
+    case MODE_APPLY:
+      switch (dtype) {
+        case GPW_F64: return dispatch_mode<double, MODE_APPLY>(a, dd, nbatch, st);
+        case GPW_C128: return dispatch_mode<double2, MODE_APPLY>(a, dd, nbatch, st);
+        case GPW_F32: return dispatch_mode<float, MODE_APPLY>(a, dd, nbatch, st);
+        case GPW_C64: return dispatch_mode<float2, MODE_APPLY>(a, dd, nbatch, st);
+      }
+      break;
+    case MODE_RESIDUAL:
+      switch (dtype) {
+        case GPW_F64: return dispatch_mode<double, MODE_RESIDUAL>(a, dd, nbatch, st);
+        case GPW_F32: return dispatch_mode<float, MODE_RESIDUAL>(a, dd, nbatch, st);
+      }
+      break;
+    case MODE_JACOBI:
+      switch (dtype) {
+        case GPW_F64: return dispatch_mode<double, MODE_JACOBI>(a, dd, nbatch, st);
+        case GPW_F32: return dispatch_mode<float, MODE_JACOBI>(a, dd, nbatch, st);
+      }
+      break;
+  }
+  return cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------------------------ transfers
+template <typename T, int K>
+static cudaError_t run_restrict(TransferArgs a, int nbatch, cudaStream_t st) {
+  using C = RestrictCfg<T, K>;
+  dim3 grid((a.vout.n[2] + RS_OZ - 1) / RS_OZ, (a.vout.n[1] + RS_OY - 1) / RS_OY, 1);
+  choose_chunks(a.vout.n[0], (int64_t)grid.x * grid.y * nbatch, K, a.zchunk, a.nchunk);
+  grid.z = a.nchunk * nbatch;
+  auto kern = restrict_kernel<T, K>;
+  static std::once_flag once;
+  cudaError_t e = cudaSuccess;
+  std::call_once(once, [&] { e = smem_optin(kern, C::smem); });
+  if (e != cudaSuccess) return e;
+  kern<<<grid, dim3(RS_OZ, RS_OY), C::smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, int K>
+static cudaError_t run_interp(TransferArgs a, int nbatch, cudaStream_t st) {
+  using C = InterpCfg<T, K>;
+  dim3 grid((a.vout.n[2] + IP_OZ - 1) / IP_OZ, (a.vout.n[1] + IP_OY - 1) / IP_OY, 1);
+  choose_chunks(a.vout.n[0], (int64_t)grid.x * grid.y * nbatch, 2 * K, a.zchunk, a.nchunk);
+  grid.z = a.nchunk * nbatch;
+  auto kern = interpolate_kernel<T, K>;
+  static std::once_flag once;
+  cudaError_t e = cudaSuccess;
+  std::call_once(once, [&] { e = smem_optin(kern, C::smem); });
+  if (e != cudaSuccess) return e;
+  kern<<<grid, dim3(IP_OZ, IP_OY), C::smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t dispatch_transfer(const TransferArgs& a, int k, bool interp, int nbatch, cudaStream_t st) {
+  if (interp) {
+    switch (k) {
+      case 2: return run_interp<T, 2>(a, nbatch, st);
+      case 4: return run_interp<T, 4>(a, nbatch, st);
+      case 6: return run_interp<T, 6>(a, nbatch, st);
+      case 8: return run_interp<T, 8>(a, nbatch, st);
+    }
+  } else {
+    switch (k) {
+      case 2: return run_restrict<T, 2>(a, nbatch, st);
+      case 4: return run_restrict<T, 4>(a, nbatch, st);
+      case 6: return run_restrict<T, 6>(a, nbatch, st);
+      case 8: return run_restrict<T, 8>(a, nbatch, st);
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const GridView& vin, void* out,
+                            const GridView& vout, int nbatch, const Boundary& bc, int subtract,
+                            const void* base, const GridView* vbase, const unsigned char* active,
+                            cudaStream_t st) {
+  TransferArgs a{};
+  a.in = in;
+  a.out = out;
+  a.vin = vin;
+  a.vout = vout;
+  a.bc = bc;
+  for (int c = 0; c < 3; ++c) {
+    a.pad0[c] = d.pad[c][0];
+    a.skip0[c] = d.skip[c][0];
+  }
+  a.active = active;
+  a.subtract = subtract;
+  a.base = base;
+  if (vbase) a.vbase = *vbase;
+  const bool interp = d.interpolate != 0;
+  switch (dtype) {
+    case GPW_F64: return dispatch_transfer<double>(a, d.k, interp, nbatch, st);
+    case GPW_C128: return dispatch_transfer<double2>(a, d.k, interp, nbatch, st);
+    case GPW_F32: return dispatch_transfer<float>(a, d.k, interp, nbatch, st);
+    case GPW_C64: return dispatch_transfer<float2>(a, d.k, interp, nbatch, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------------------------ blas
+static dim3 ew_grid(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  b = std::min<int64_t>(b, 8LL * num_sms());
+  return dim3((unsigned)std::max<int64_t>(b, 1));
+}
+
+cudaError_t launch_axpy(int dtype, int64_t n, double ar, double ai, const void* x, void* y, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  switch (dtype) {
+    case GPW_F64: axpy_real_kernel<double><<<ew_grid(n), 256, 0, st>>>(n, ar, (const double*)x, (double*)y); break;
+    case GPW_F32: axpy_real_kernel<float><<<ew_grid(n), 256, 0, st>>>(n, (float)ar, (const float*)x, (float*)y); break;
+    case GPW_C128: axpy_cplx_kernel<double2><<<ew_grid(n), 256, 0, st>>>(n, ar, ai, (const double2*)x, (double2*)y); break;
+    case GPW_C64: axpy_cplx_kernel<float2><<<ew_grid(n), 256, 0, st>>>(n, ar, ai, (const float2*)x, (float2*)y); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scal(int dtype, int64_t n, double ar, double ai, void* x, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  switch (dtype) {
+    case GPW_F64: scal_real_kernel<double><<<ew_grid(n), 256, 0, st>>>(n, ar, (double*)x); break;
+    case GPW_F32: scal_real_kernel<float><<<ew_grid(n), 256, 0, st>>>(n, (float)ar, (float*)x); break;
+    case GPW_C128: scal_cplx_kernel<double2><<<ew_grid(n), 256, 0, st>>>(n, ar, ai, (double2*)x); break;
+    case GPW_C64: scal_cplx_kernel<float2><<<ew_grid(n), 256, 0, st>>>(n, ar, ai, (float2*)x); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_scalar(int dtype, int64_t n, double c, const void* x, void* y, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  switch (dtype) {
+    case GPW_F64: add_scalar_kernel<double><<<ew_grid(n), 256, 0, st>>>(n, c, (const double*)x, (double*)y); break;
+    case GPW_F32: add_scalar_kernel<float><<<ew_grid(n), 256, 0, st>>>(n, c, (const float*)x, (float*)y); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+int reduce_blocks(int64_t n) {
+  int64_t b = (n + 4095) / 4096;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 2LL * num_sms()));
+}
+
+cudaError_t launch_reduce(int dtype, int op, int64_t nvec, int64_t n, const void* x, const void* y,
+                          const GridSum& gs, int nblk, cudaStream_t st) {
+  dim3 grid(nblk, (unsigned)nvec);
+  const int ncomp = (op == 0 && is_complex(dtype)) ? 2 : 1;
+  switch (dtype) {
+    case GPW_F64:
+      if (op == 0) reduce_kernel<double, 0><<<grid, 256, 0, st>>>(n, (const double*)x, nullptr, gs, ncomp);
+      else reduce_kernel<double, 1><<<grid, 256, 0, st>>>(n, (const double*)x, (const double*)y, gs, ncomp);
+      break;
+    case GPW_F32:
+      if (op == 0) reduce_kernel<float, 0><<<grid, 256, 0, st>>>(n, (const float*)x, nullptr, gs, ncomp);
+      else reduce_kernel<float, 1><<<grid, 256, 0, st>>>(n, (const float*)x, (const float*)y, gs, ncomp);
+      break;
+    case GPW_C128:
+      if (op == 0) reduce_kernel<double2, 0><<<grid, 256, 0, st>>>(n, (const double2*)x, nullptr, gs, ncomp);
+      else reduce_kernel<double2, 1><<<grid, 256, 0, st>>>(n, (const double2*)x, (const double2*)y, gs, ncomp);
+      break;
+    case GPW_C64:
+      if (op == 0) reduce_kernel<float2, 0><<<grid, 256, 0, st>>>(n, (const float2*)x, nullptr, gs, ncomp);
+      else reduce_kernel<float2, 1><<<grid, 256, 0, st>>>(n, (const float2*)x, (const float2*)y, gs, ncomp);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zero(int dtype, const GridView& v, void* x, int nbatch, const unsigned char* active,
+                        cudaStream_t st) {
+  const int64_t tot = view_points(v);
+  dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, 4LL * num_sms())), nbatch);
+  switch (dtype) {
+    case GPW_F64: zero_kernel<double><<<grid, 256, 0, st>>>(v, (double*)x, active); break;
+    case GPW_F32: zero_kernel<float><<<grid, 256, 0, st>>>(v, (float*)x, active); break;
+    case GPW_C128: zero_kernel<double2><<<grid, 256, 0, st>>>(v, (double2*)x, active); break;
+    case GPW_C64: zero_kernel<float2><<<grid, 256, 0, st>>>(v, (float2*)x, active); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace gpw

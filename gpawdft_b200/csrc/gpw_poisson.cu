@@ -1,0 +1,401 @@
+// Multigrid Poisson engine: the V-cycle of FDPoissonSolver.iterate2 and the
+// convergence loop of solve_neutral (gpaw/poisson.py:306-366) on the device.
+//
+// One V-cycle for level l < L (L = coarsest):
+//   relax(l, presmooths[l])            Jacobi sweeps, ping-pong buffers
+//   r_l = A_l phi_l - rho_l            fused residual kernel
+//   rho_{l+1} = R r_l ; phi_{l+1} = 0
+//   V-cycle(l+1)
+//   phi_l = phi_l - I phi_{l+1}        interpolation with fused subtraction
+// then for every level relax(l, postsmooths[l]) and at level 0 the fused
+// residual + deterministic sum(r^2) that gives error = sum(r^2) dv.
+//
+// The whole V-cycle (plus the per-solve convergence update) is captured once
+// per batch size into a CUDA graph whose buffers are all engine-owned; a
+// solve copies phi / rho in, replays the graph until every solve of the batch
+// has converged, and copies phi out.  Independent same-grid solves are
+// batched through every kernel (grid z = chunks x batch); a per-solve
+// `active` mask freezes solves that have converged, so each solve's result
+// and iteration count equal those of solving it alone.
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "gpw_internal.h"
+#include "gpw_relax_gs.cuh"
+
+namespace gpw {
+
+struct Level {
+  const OpDesc* op = nullptr;
+  const TrDesc* restr = nullptr;   // level l -> l+1
+  const TrDesc* interp = nullptr;  // level l+1 -> l
+  GridView v;
+  int pre = 0, post = 0;
+  double w = 1.0;
+  // float64 buffers (nbatch_max grids each)
+  Workspace phi[2], rho, res;
+  // float32 buffers for the defect-correction form
+  Workspace phi32[2], rho32, res32;
+};
+
+__global__ void converge_update_kernel(int nbatch, const double* __restrict__ sumsq, double dv,
+                                       const double* __restrict__ eps, const int* __restrict__ maxiter_p,
+                                       double* __restrict__ err,
+                                       int* __restrict__ niter, unsigned char* __restrict__ active,
+                                       int* __restrict__ any_active) {
+  __shared__ int any;
+  const int maxiter = *maxiter_p;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int b = threadIdx.x; b < nbatch; b += blockDim.x) {
+    if (!active[b]) continue;
+    const double e = sumsq[b] * dv;
+    err[b] = e;
+    // while iterate2(step) > eps and niter < maxiter: niter += 1
+    if (e > eps[b] && niter[b] < maxiter) {
+      niter[b] += 1;
+      atomicOr(&any, 1);
+    } else {
+      active[b] = 0;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *any_active = any;
+}
+
+__global__ void to_f32_neg_kernel(int64_t n, const double* __restrict__ x, float* __restrict__ y,
+                                  const unsigned char* active, int64_t per) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (active && !active[i / per]) continue;
+    y[i] = (float)(-x[i]);
+  }
+}
+
+__global__ void add_f32_kernel(int64_t n, const float* __restrict__ e, double* __restrict__ phi,
+                               const unsigned char* active, int64_t per) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (active && !active[i / per]) continue;
+    phi[i] += (double)e[i];
+  }
+}
+
+}  // namespace gpw
+
+using namespace gpw;
+
+struct gpw_poisson {
+  std::vector<Level> lv;
+  int relax_method = 2;
+  double dv = 1.0;
+  int64_t nbmax = 1;
+  Workspace d_err, d_eps, d_niter, d_active, d_any, d_r64, d_gs_old, d_maxiter;
+  SumScratch sums;
+  int* h_any = nullptr;  // pinned
+  struct GraphKey {
+    int64_t nb;
+    int prec;
+    bool operator<(const GraphKey& o) const { return nb != o.nb ? nb < o.nb : prec < o.prec; }
+  };
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  std::map<GraphKey, int64_t> graph_kernels;  // kernel nodes per graph
+  int64_t last_kernels = 0, last_graphs = 0;
+  ~gpw_poisson() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (h_any) cudaFreeHost(h_any);
+  }
+};
+
+namespace {
+
+struct Rec {
+  gpw_poisson* ps;
+  int nb;
+  cudaStream_t st;
+  const unsigned char* active;
+  cudaError_t err = cudaSuccess;
+  void ok(cudaError_t e) {
+    if (err == cudaSuccess && e != cudaSuccess) err = e;
+  }
+};
+
+// Relax `n` sweeps on level l (dtype f64 or f32); returns the index of the
+// phi buffer holding the result.
+int rec_relax(Rec& r, int l, int cur, int nsweeps, bool f32) {
+  Level& L = r.ps->lv[l];
+  const int dt = f32 ? GPW_F32 : GPW_F64;
+  Boundary bc = make_boundary(L.op->periodic, dt, nullptr);
+  GridSum gs{};
+  Workspace* phi = f32 ? L.phi32 : L.phi;
+  const void* rho = f32 ? L.rho32.ptr : L.rho.ptr;
+  if (r.ps->relax_method == 1) {
+    for (int b = 0; b < r.nb; ++b) {
+      const size_t es = elt_size(dt) * (size_t)L.v.sb;
+      r.ok(launch_relax_gs_ws(*L.op, dt, (char*)phi[cur].ptr + b * es, L.v, (const char*)rho + b * es, L.v,
+                              nsweeps, bc, r.ps->d_gs_old.ptr, r.active ? r.active + b : nullptr, r.st));
+    }
+    return cur;
+  }
+  for (int s = 0; s < nsweeps; ++s) {
+    r.ok(launch_stencil(*L.op, dt, MODE_JACOBI, phi[cur].ptr, L.v, phi[1 - cur].ptr, L.v, rho, L.v, r.nb, bc, L.w,
+                        r.active, gs, r.st));
+    cur = 1 - cur;
+  }
+  return cur;
+}
+
+// Records iterate2(level l) starting from phi buffer `cur`; returns the buffer
+// holding phi_l afterwards.
+int rec_vcycle(Rec& r, int l, int cur, bool f32) {
+  gpw_poisson* ps = r.ps;
+  const int nl = (int)ps->lv.size();
+  Level& L = ps->lv[l];
+  const int dt = f32 ? GPW_F32 : GPW_F64;
+  Workspace* phi = f32 ? L.phi32 : L.phi;
+  Workspace& rho = f32 ? L.rho32 : L.rho;
+  Workspace& res = f32 ? L.res32 : L.res;
+  Boundary bc = make_boundary(L.op->periodic, dt, nullptr);
+  if (l < nl - 1) {
+    Level& C = ps->lv[l + 1];
+    Workspace* cphi = f32 ? C.phi32 : C.phi;
+    Workspace& crho = f32 ? C.rho32 : C.rho;
+    cur = rec_relax(r, l, cur, L.pre, f32);
+    r.ok(launch_stencil(*L.op, dt, MODE_RESIDUAL, phi[cur].ptr, L.v, res.ptr, L.v, rho.ptr, L.v, r.nb, bc, 1.0,
+                        r.active, ps->sums.gs(), r.st));
+    r.ok(launch_transfer(*L.restr, dt, res.ptr, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st));
+    r.ok(launch_zero(dt, C.v, cphi[0].ptr, r.nb, r.active, r.st));
+    int ccur = rec_vcycle(r, l + 1, 0, f32);
+    Boundary cbc = make_boundary(C.op->periodic, dt, nullptr);
+    r.ok(launch_transfer(*L.interp, dt, cphi[ccur].ptr, C.v, phi[1 - cur].ptr, L.v, r.nb, cbc, 1, phi[cur].ptr, &L.v,
+                         r.active, r.st));
+    cur = 1 - cur;
+  }
+  cur = rec_relax(r, l, cur, L.post, f32);
+  return cur;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer* const* restrictors,
+                    gpw_transformer* const* interpolators, const int* presmooths, const int* postsmooths,
+                    const double* weights, int relax_method, double dv, int64_t nbatch_max, gpw_poisson** out);
+int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t nbatch, const double* eps, int maxiter,
+                      int precision, int* niter, double* error, gpw_stream stream);
+void gpw_poisson_free(gpw_poisson* ps);
+
+}  // extern "C"
+
+// The opaque handle types are defined in gpw_api.cu; the engine only needs
+// their descriptors, exported through these accessors.
+namespace gpw {
+const OpDesc* operator_desc(const gpw_operator* op);
+const TrDesc* transformer_desc(const gpw_transformer* tr);
+}  // namespace gpw
+
+int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer* const* restrictors,
+                    gpw_transformer* const* interpolators, const int* presmooths, const int* postsmooths,
+                    const double* weights, int relax_method, double dv, int64_t nbatch_max, gpw_poisson** out) {
+  if (nlevels < 1 || nlevels > 16 || !operators || !presmooths || !postsmooths || !weights || !out)
+    return fail(GPW_EINVAL, "poisson: bad arguments");
+  if (nlevels > 1 && (!restrictors || !interpolators)) return fail(GPW_EINVAL, "poisson: missing transformers");
+  if (relax_method != 1 && relax_method != 2) return fail(GPW_EINVAL, "poisson: relax_method must be 1 or 2");
+  if (nbatch_max < 1 || nbatch_max > 4096) return fail(GPW_EINVAL, "poisson: nbatch_max out of range");
+  std::unique_ptr<gpw_poisson> ps(new gpw_poisson());
+  ps->relax_method = relax_method;
+  ps->dv = dv;
+  ps->nbmax = nbatch_max;
+  ps->lv.resize(nlevels);
+  for (int l = 0; l < nlevels; ++l) {
+    Level& L = ps->lv[l];
+    if (!operators[l]) return fail(GPW_EINVAL, "poisson: null operator");
+    L.op = operator_desc(operators[l]);
+    L.v = contiguous_view(L.op->n);
+    L.pre = presmooths[l];
+    L.post = postsmooths[l];
+    L.w = weights[l];
+    if (l < nlevels - 1) {
+      if (!restrictors[l] || !interpolators[l]) return fail(GPW_EINVAL, "poisson: null transformer");
+      L.restr = transformer_desc(restrictors[l]);
+      L.interp = transformer_desc(interpolators[l]);
+      if (L.restr->interpolate || !L.interp->interpolate) return fail(GPW_EINVAL, "poisson: transformer kinds");
+    }
+    const size_t pts = (size_t)view_points(L.v) * nbatch_max;
+    int rc;
+    if ((rc = L.phi[0].ensure(pts * 8)) || (rc = L.phi[1].ensure(pts * 8)) || (rc = L.rho.ensure(pts * 8)) ||
+        (rc = L.res.ensure(pts * 8)))
+      return rc;
+  }
+  // level shapes must chain through the transformers
+  for (int l = 0; l + 1 < nlevels; ++l) {
+    const Level &A = ps->lv[l], &B = ps->lv[l + 1];
+    for (int c = 0; c < 3; ++c)
+      if (A.restr->nin[c] != A.v.n[c] || A.restr->nout[c] != B.v.n[c] || A.interp->nin[c] != B.v.n[c] ||
+          A.interp->nout[c] != A.v.n[c])
+        return fail(GPW_EINVAL, "poisson: level shapes do not chain");
+  }
+  int rc;
+  if ((rc = ps->d_err.ensure(nbatch_max * 8)) || (rc = ps->d_eps.ensure(nbatch_max * 8)) ||
+      (rc = ps->d_niter.ensure(nbatch_max * 4)) || (rc = ps->d_active.ensure(nbatch_max)) ||
+      (rc = ps->d_any.ensure(16)) || (rc = ps->d_maxiter.ensure(16)) || (rc = ps->d_r64.ensure((size_t)view_points(ps->lv[0].v) * nbatch_max * 8)))
+    return rc;
+  if (relax_method == 1) {
+    size_t mx = 0;
+    for (auto& L : ps->lv) mx = std::max(mx, (size_t)view_points(L.v));
+    if ((rc = ps->d_gs_old.ensure(mx * 8))) return rc;
+  }
+  const int nblk = stencil_blocks_per_member(*ps->lv[0].op, MODE_RESIDUAL, ps->lv[0].v, 1);
+  // residual partial slots: enough for any level / batch size (blocks per member shrink with batch)
+  int64_t maxblk = 0;
+  for (auto& L : ps->lv) maxblk = std::max<int64_t>(maxblk, stencil_blocks_per_member(*L.op, MODE_RESIDUAL, L.v, 1));
+  (void)nblk;
+  if ((rc = ps->sums.ensure(nbatch_max, maxblk))) return rc;
+  cudaError_t e = cudaMallocHost(&ps->h_any, sizeof(int));
+  if (e != cudaSuccess) return cuda_fail(e, "pinned alloc");
+  *out = ps.release();
+  return GPW_OK;
+}
+
+void gpw_poisson_free(gpw_poisson* ps) { delete ps; }
+
+extern "C" int gpw_poisson_last_stats(const gpw_poisson* ps, int64_t* kernel_launches, int64_t* graph_launches) {
+  if (!ps) return fail(GPW_EINVAL, "null argument");
+  if (kernel_launches) *kernel_launches = ps->last_kernels;
+  if (graph_launches) *graph_launches = ps->last_graphs;
+  return GPW_OK;
+}
+
+static int ensure_f32(gpw_poisson* ps) {
+  for (auto& L : ps->lv) {
+    const size_t pts = (size_t)view_points(L.v) * ps->nbmax;
+    int rc;
+    if ((rc = L.phi32[0].ensure(pts * 4)) || (rc = L.phi32[1].ensure(pts * 4)) || (rc = L.rho32.ensure(pts * 4)) ||
+        (rc = L.res32.ensure(pts * 4)))
+      return rc;
+  }
+  return GPW_OK;
+}
+
+// Record one outer iteration (one V-cycle, or one defect-correction step)
+// plus the convergence update for batch size nb.
+static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, int maxiter_unused, cudaStream_t st) {
+  (void)maxiter_unused;
+  Rec r{ps, nb, st, (const unsigned char*)ps->d_active.ptr};
+  Level& L0 = ps->lv[0];
+  Boundary bc = make_boundary(L0.op->periodic, GPW_F64, nullptr);
+  const int64_t per = L0.v.sb;
+  const int64_t n = per * nb;
+  const int thr = 256;
+  const int blocks = (int)std::min<int64_t>((n + thr - 1) / thr, 4LL * num_sms());
+  if (prec == 0) {
+    const int cur = rec_vcycle(r, 0, 0, false);
+    if (cur != 0) r.ok(cudaMemcpyAsync(L0.phi[0].ptr, L0.phi[1].ptr, n * 8, cudaMemcpyDeviceToDevice, st));
+  } else {
+    // defect correction: rhs32 = -(A phi - rho) (residual computed at the end
+    // of the previous iteration into d_r64), e = FP32 V-cycle(rhs32), phi += e
+    to_f32_neg_kernel<<<blocks, thr, 0, st>>>(n, (const double*)ps->d_r64.ptr, (float*)L0.rho32.ptr, r.active, per);
+    r.ok(cudaGetLastError());
+    r.ok(launch_zero(GPW_F32, L0.v, L0.phi32[0].ptr, nb, r.active, st));
+    const int cur = rec_vcycle(r, 0, 0, true);
+    add_f32_kernel<<<blocks, thr, 0, st>>>(n, (const float*)L0.phi32[cur].ptr, (double*)L0.phi[0].ptr, r.active, per);
+    r.ok(cudaGetLastError());
+  }
+  // error = sum(r^2) dv on level 0 after post-smoothing (gpaw/poisson.py:357-361)
+  r.ok(launch_stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, L0.v, ps->d_r64.ptr, L0.v, L0.rho.ptr, L0.v, nb,
+                      bc, 1.0, r.active, ps->sums.gs(), st));
+  converge_update_kernel<<<1, 256, 0, st>>>(nb, ps->sums.gs().result, ps->dv, (const double*)ps->d_eps.ptr,
+                                            (const int*)ps->d_maxiter.ptr,
+                                            (double*)ps->d_err.ptr, (int*)ps->d_niter.ptr,
+                                            (unsigned char*)ps->d_active.ptr, (int*)ps->d_any.ptr);
+  r.ok(cudaGetLastError());
+  return r.err;
+}
+
+int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t nbatch, const double* eps, int maxiter,
+                      int precision, int* niter, double* error, gpw_stream stream) {
+  if (!ps || !phi || !rho || !eps || !niter || !error) return fail(GPW_EINVAL, "null argument");
+  if (nbatch < 1 || nbatch > ps->nbmax) return fail(GPW_EINVAL, "poisson: nbatch out of range");
+  if (precision != 0 && precision != 1) return fail(GPW_EINVAL, "poisson: precision must be 0 or 1");
+  if (precision == 1 && ps->relax_method != 2) return fail(GPW_ENOTSUP, "poisson: float32 form needs Jacobi");
+  if (maxiter < 1) return fail(GPW_EINVAL, "poisson: maxiter < 1");
+  cudaStream_t st = (cudaStream_t)stream;
+  Level& L0 = ps->lv[0];
+  const int nb = (int)nbatch;
+  const size_t bytes = (size_t)L0.v.sb * nb * 8;
+  int rc;
+  if (precision == 1 && (rc = ensure_f32(ps))) return rc;
+  cudaError_t e;
+  // state: eps, niter = 1, active = 1
+  std::vector<int> ones(nb, 1);
+  std::vector<unsigned char> act(nb, 1);
+  if ((e = cudaMemcpyAsync(ps->d_eps.ptr, eps, nb * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(ps->d_niter.ptr, ones.data(), nb * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(ps->d_active.ptr, act.data(), nb, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(ps->d_maxiter.ptr, &maxiter, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(L0.phi[0].ptr, phi, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(L0.rho.ptr, rho, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+    return cuda_fail(e, "poisson setup copies");
+  if (precision == 1) {
+    // initial residual for the first defect-correction step
+    Boundary bc = make_boundary(L0.op->periodic, GPW_F64, nullptr);
+    e = launch_stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, L0.v, ps->d_r64.ptr, L0.v, L0.rho.ptr, L0.v, nb,
+                       bc, 1.0, (const unsigned char*)ps->d_active.ptr, ps->sums.gs(), st);
+    if (e != cudaSuccess) return cuda_fail(e, "poisson initial residual");
+  }
+  // get (or capture) the graph of one iteration for this batch size
+  gpw_poisson::GraphKey key{nbatch, precision};
+  auto it = ps->graphs.find(key);
+  if (it == ps->graphs.end()) {
+    // eager warm-up run of the launch sequence is avoided: capture directly
+    cudaGraph_t g;
+    cudaStream_t cs;
+    if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e, "stream");
+    if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+      cudaStreamDestroy(cs);
+      return cuda_fail(e, "begin capture");
+    }
+    cudaError_t re = record_iteration(ps, nb, precision, maxiter, cs);
+    e = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (re != cudaSuccess) return cuda_fail(re, "record V-cycle");
+    if (e != cudaSuccess) return cuda_fail(e, "end capture");
+    size_t nnodes = 0;
+    int64_t nkern = 0;
+    if (cudaGraphGetNodes(g, nullptr, &nnodes) == cudaSuccess && nnodes) {
+      std::vector<cudaGraphNode_t> nodes(nnodes);
+      if (cudaGraphGetNodes(g, nodes.data(), &nnodes) == cudaSuccess)
+        for (auto n : nodes) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(n, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nkern;
+        }
+    }
+    cudaGraphExec_t ge;
+    e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+    it = ps->graphs.emplace(key, ge).first;
+    ps->graph_kernels[key] = nkern;
+  }
+  ps->last_kernels = (precision == 1) ? 1 : 0;
+  ps->last_graphs = 0;
+  // replay until no solve of the batch is active
+  for (int iter = 0; iter < maxiter + 1; ++iter) {
+    if ((e = cudaGraphLaunch(it->second, st)) != cudaSuccess) return cuda_fail(e, "graph launch");
+    ps->last_graphs += 1;
+    ps->last_kernels += ps->graph_kernels[key];
+    if ((e = cudaMemcpyAsync(ps->h_any, ps->d_any.ptr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return cuda_fail(e, "flag copy");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "V-cycle");
+    if (!*ps->h_any) break;
+  }
+  if ((e = cudaMemcpyAsync(phi, L0.phi[0].ptr, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(niter, ps->d_niter.ptr, nb * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(error, ps->d_err.ptr, nb * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cuda_fail(e, "poisson result copies");
+  for (int b = 0; b < nb; ++b)
+    if (niter[b] >= maxiter) return fail(GPW_ECONV, "Poisson solver did not converge in maxiter iterations");
+  return GPW_OK;
+}

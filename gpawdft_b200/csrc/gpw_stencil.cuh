@@ -1,0 +1,386 @@
+// Finite-difference stencil kernels with fused halo fill.
+//
+// Reference semantics (c/operators.c:109-157 + c/bc.c:138-250 +
+// c/bmgs/fd.c:16-51 / relax.c:46-71): every apply / relax sweep first builds
+// a zero-filled padded copy of the grid, pastes the interior and copies
+// periodic slabs (times Bloch phases) into the halo, then runs the stencil
+// over the padded copy.  Here the padded copy never exists: each CTA streams
+// the planes it needs through shared memory (cp.async, zero-fill for zero
+// boundaries, wrapped addresses plus a phase fix-up for periodic ones) and
+// the halo is produced on the fly.
+//
+// Two kernels:
+//  * general_stencil_kernel -- any offsets within [-mp, mp]^3 (GUC Laplacians
+//    with diagonal directions, Mehrstellen, gradients of skew cells).  A ring
+//    of 2mp+2 planes lives in shared memory; every output gathers its
+//    coefficients in the reference's order with unfused multiply / add, so
+//    float64 results are bit-identical to c/bmgs/fd.c.
+//  * star_stencil_kernel -- star (cfd) stencils of radius R: register-blocked
+//    march along axis 0.  Each arriving plane contributes its in-plane part
+//    (axes 1, 2 from shared memory, PY rows per thread held in registers) and
+//    its axis-0 terms to 2R+1 running accumulators; an output plane is
+//    complete R planes after its centre arrives.  Fused multiply-adds; float64
+//    results agree with the reference to ~1e-16 relative.
+// Both support three epilogues: APPLY (out = A in), RESIDUAL (out = A in -
+// rho and a deterministic sum of |out|^2) and JACOBI (one weighted-Jacobi
+// sweep, out = (1-w) in + w (rho - sum_{p!=0} c_p in[x+o_p]) / c_0).
+#pragma once
+#include "gpw_common.cuh"
+#include "gpw_reduce.cuh"
+
+namespace gpw {
+
+enum StencilMode { MODE_APPLY = 0, MODE_RESIDUAL = 1, MODE_JACOBI = 2 };
+
+constexpr int PMAX = 80;  // GUC n<=6 with 6 directions needs 73
+
+struct StencilArgs {
+  const void* in;
+  void* out;        // may be null in RESIDUAL mode (norm only)
+  const void* rho;  // RESIDUAL / JACOBI
+  GridView vin, vout, vrho;
+  Boundary bc;
+  int zchunk;       // output planes of axis 0 per CTA
+  int nchunk;       // chunks along axis 0 (gridDim.z = nchunk * nbatch)
+  double w;         // Jacobi weight
+  double c0;        // Jacobi diagonal coefficient
+  const unsigned char* active;  // optional per-batch-member mask (null: all)
+  GridSum gsum;     // RESIDUAL: per-batch-member segmented sum
+  int nblk_seg;     // CTAs per batch member
+};
+
+struct GeneralCoefs {
+  int ncoef, mp;
+  double coef[PMAX];
+  signed char off[PMAX][3];
+};
+
+// ------------------------------------------------------------------ loaders
+// Issue cp.async copies of plane p (tile rows y0-mp .. y0+TY+mp, columns
+// x0-mp .. x0+TZ+mp) into `slot`.  Cells that fall in a zero halo are
+// zero-filled by the copy engine.
+template <typename T>
+__device__ __forceinline__ void load_plane(T* slot, const T* in, const GridView& v, const Boundary& bc,
+                                           int p, int y0, int x0, int mp, int H, int W) {
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int nthr = blockDim.x * blockDim.y;
+  int j0, s0;
+  bool ok0 = wrap_axis(p, v.n[0], bc.periodic[0], j0, s0);
+  for (int idx = tid; idx < H * W; idx += nthr) {
+    int r = idx / W, c = idx - r * W;
+    int j1, j2, s1, s2;
+    bool ok = ok0 && wrap_axis(y0 - mp + r, v.n[1], bc.periodic[1], j1, s1) &&
+              wrap_axis(x0 - mp + c, v.n[2], bc.periodic[2], j2, s2);
+    const T* src = ok ? in + (int64_t)j0 * v.s0 + (int64_t)j1 * v.s1 + j2 : in;
+    cp_async<sizeof(T)>(slot + idx, src, ok);
+  }
+}
+
+// Multiply the periodic-halo cells of a landed plane by their Bloch phase
+// product (same cell walk as load_plane, so each thread fixes its own copies).
+template <typename T>
+__device__ __forceinline__ void fix_plane(T* slot, const GridView& v, const Boundary& bc, int p, int y0,
+                                          int x0, int mp, int H, int W) {
+  if constexpr (EltTraits<T>::cpx) {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nthr = blockDim.x * blockDim.y;
+    int j0, s0;
+    bool ok0 = wrap_axis(p, v.n[0], bc.periodic[0], j0, s0);
+    if (!ok0) return;
+    for (int idx = tid; idx < H * W; idx += nthr) {
+      int r = idx / W, c = idx - r * W;
+      int j1, j2, s1, s2;
+      bool ok = wrap_axis(y0 - mp + r, v.n[1], bc.periodic[1], j1, s1) &&
+                wrap_axis(x0 - mp + c, v.n[2], bc.periodic[2], j2, s2);
+      if (!ok || (s0 < 0 && s1 < 0 && s2 < 0)) continue;
+      // axis by axis, as the reference's chained halo copies apply them
+      T val = slot[idx];
+      if (s0 >= 0) val = phase_mul(bc.ph[0][s0], val);
+      if (s1 >= 0) val = phase_mul(bc.ph[1][s1], val);
+      if (s2 >= 0) val = phase_mul(bc.ph[2][s2], val);
+      slot[idx] = val;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ general
+constexpr int GEN_TZ = 32, GEN_TY = 8;
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(GEN_TZ* GEN_TY)
+    general_stencil_kernel(const StencilArgs a, const GeneralCoefs k) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = reinterpret_cast<T*>(smem_raw);
+  __shared__ double red[32];
+  using S = typename EltTraits<T>::S;
+
+  const int mp = k.mp;
+  const int H = GEN_TY + 2 * mp, W = GEN_TZ + 2 * mp, PS = H * W, NP = 2 * mp + 2;
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int x0 = blockIdx.x * GEN_TZ, y0 = blockIdx.y * GEN_TY;
+  const int n0 = a.vout.n[0];
+  const int z0 = chunk * a.zchunk;
+  const int z1 = min(n0, z0 + a.zchunk);
+  const T* in = static_cast<const T*>(a.in) + (int64_t)b * a.vin.sb;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int y = y0 + ty, x = x0 + tx;
+  const bool inside = (y < a.vout.n[1]) && (x < a.vout.n[2]);
+  double sumsq = 0.0;
+
+  if (z0 < z1) {
+    // prologue: planes z0-mp .. z0+mp
+    for (int p = z0 - mp; p <= z0 + mp; ++p)
+      load_plane<T>(ring + ((p - z0 + mp) % NP) * PS, in, a.vin, a.bc, p, y0, x0, mp, H, W);
+    cp_async_commit();
+    for (int o = z0; o < z1; ++o) {
+      const int pn = o + mp + 1;
+      if (o + 1 < z1) load_plane<T>(ring + ((pn - z0 + mp) % NP) * PS, in, a.vin, a.bc, pn, y0, x0, mp, H, W);
+      cp_async_commit();
+      cp_async_wait<1>();
+      if (a.bc.use_phase) {
+        if (o == z0) {
+          for (int p = z0 - mp; p <= z0 + mp; ++p)
+            fix_plane<T>(ring + ((p - z0 + mp) % NP) * PS, a.vin, a.bc, p, y0, x0, mp, H, W);
+        } else {
+          fix_plane<T>(ring + ((o + mp - z0 + mp) % NP) * PS, a.vin, a.bc, o + mp, y0, x0, mp, H, W);
+        }
+      }
+      __syncthreads();
+      if (inside) {
+        T acc = zero<T>();
+        const int cstart = (MODE == MODE_JACOBI) ? 1 : 0;
+        for (int c = cstart; c < k.ncoef; ++c) {
+          const int p = o + k.off[c][0];
+          const T* sl = ring + ((p - z0 + mp) % NP) * PS;
+          const T v = sl[(ty + mp + k.off[c][1]) * W + tx + mp + k.off[c][2]];
+          acc = mac_rn((S)k.coef[c], v, acc);
+        }
+        const int64_t oi = (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
+        if constexpr (MODE == MODE_APPLY) {
+          static_cast<T*>(a.out)[oi] = acc;
+        } else {
+          const int64_t ri = (int64_t)b * a.vrho.sb + (int64_t)o * a.vrho.s0 + (int64_t)y * a.vrho.s1 + x;
+          const T rho = static_cast<const T*>(a.rho)[ri];
+          if constexpr (MODE == MODE_RESIDUAL) {
+            const T r = sub(acc, rho);
+            if (a.out) static_cast<T*>(a.out)[oi] = r;
+            sumsq += norm2(r);
+          } else {
+            // (1 - w) * b + w * (src - x) / c0   (c/bmgs/relax.c:62)
+            const T* sl = ring + ((o - z0 + mp) % NP) * PS;
+            const T cur = sl[(ty + mp) * W + tx + mp];
+            if constexpr (EltTraits<T>::cpx) {
+              static_cast<T*>(a.out)[oi] = cur;  // relax is real-only (asserted on host)
+            } else {
+              const S w = (S)a.w, c0 = (S)a.c0;
+              static_cast<T*>(a.out)[oi] = (S(1) - w) * cur + (w * (rho - acc)) / c0;
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if constexpr (MODE == MODE_RESIDUAL) {
+    double tot = block_sum(sumsq, red);
+    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
+    grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);
+  }
+}
+
+// ------------------------------------------------------------------ star
+// Tile TZ (axis 2) x TY (axis 1); PY consecutive axis-1 rows per thread.
+template <int R, typename T>
+struct StarCfg {
+  static constexpr int TZ = 32;
+  static constexpr int PY = (sizeof(T) >= 16) ? 2 : 4;
+  static constexpr int TY = 32;
+  static constexpr int NTY = TY / PY;
+  static constexpr int H = TY + 2 * R, W = TZ + 2 * R, PS = H * W;
+  static constexpr int NSTAGE = 3;
+};
+
+struct StarCoefs {
+  double cx[13], cy[13], cz[13];  // per-axis coefficients indexed offset + R (centres zero)
+  double cc;                      // total centre (diagonal) coefficient
+};
+
+template <typename T, int R>
+__device__ __forceinline__ void star_load(T* slot, const T* in, const GridView& v, const Boundary& bc, int p,
+                                          int y0, int x0) {
+  using C = StarCfg<R, T>;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  constexpr int NT = C::TZ * C::NTY;
+  int j0, s0;
+  const bool ok0 = wrap_axis(p, v.n[0], bc.periodic[0], j0, s0);
+  const T* base = in + (int64_t)j0 * v.s0;
+#pragma unroll 4
+  for (int idx = tid; idx < C::PS; idx += NT) {
+    const int r = idx / C::W, c = idx - r * C::W;
+    int j1, j2, s1, s2;
+    const bool ok = ok0 && wrap_axis(y0 - R + r, v.n[1], bc.periodic[1], j1, s1) &&
+                    wrap_axis(x0 - R + c, v.n[2], bc.periodic[2], j2, s2);
+    const T* src = ok ? base + (int64_t)j1 * v.s1 + j2 : in;
+    cp_async<sizeof(T)>(slot + idx, src, ok);
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void star_fix(T* slot, const GridView& v, const Boundary& bc, int p, int y0,
+                                         int x0) {
+  using C = StarCfg<R, T>;
+  fix_plane<T>(slot, v, bc, p, y0, x0, R, C::H, C::W);
+}
+
+template <typename T, int R, int MODE>
+__global__ void __launch_bounds__(StarCfg<R, T>::TZ* StarCfg<R, T>::NTY)
+    star_stencil_kernel(const StencilArgs a, const StarCoefs k) {
+  using C = StarCfg<R, T>;
+  using S = typename EltTraits<T>::S;
+  constexpr int PY = C::PY, W = C::W, PS = C::PS, NS = C::NSTAGE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = reinterpret_cast<T*>(smem_raw);
+  __shared__ double red[32];
+
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int x0 = blockIdx.x * C::TZ, y0 = blockIdx.y * C::TY;
+  const int n0 = a.vout.n[0];
+  const int z0 = chunk * a.zchunk;
+  const int z1 = min(n0, z0 + a.zchunk);
+  const T* in = static_cast<const T*>(a.in) + (int64_t)b * a.vin.sb;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x = x0 + tx;
+  const int yb = ty * PY;  // first local row of this thread
+  const bool xin = x < a.vout.n[2];
+  double sumsq = 0.0;
+
+  // Per-axis coefficients as compile-time-indexed registers.
+  S cx[2 * R + 1], cy[2 * R + 1], cz[2 * R + 1];
+#pragma unroll
+  for (int i = 0; i < 2 * R + 1; ++i) {
+    cx[i] = (S)k.cx[i];
+    cy[i] = (S)k.cy[i];
+    cz[i] = (S)k.cz[i];
+  }
+  const S cc = (MODE == MODE_JACOBI) ? S(0) : (S)k.cc;
+
+  T acc[PY][2 * R + 1];
+  T cur[PY][R + 1];  // JACOBI: centre values of the last R+1 planes
+#pragma unroll
+  for (int j = 0; j < PY; ++j) {
+#pragma unroll
+    for (int m = 0; m < 2 * R + 1; ++m) acc[j][m] = zero<T>();
+#pragma unroll
+    for (int m = 0; m < R + 1; ++m) cur[j][m] = zero<T>();
+  }
+
+  if (z0 < z1) {
+    const int pfirst = z0 - R, plast = z1 - 1 + R;
+    const int nsteps = plast - pfirst + 1;
+#pragma unroll
+    for (int st = 0; st < NS - 1; ++st) {
+      if (st < nsteps) star_load<T, R>(ring + st * PS, in, a.vin, a.bc, pfirst + st, y0, x0);
+      cp_async_commit();
+    }
+    for (int s = 0; s < nsteps; ++s) {
+      const int p = pfirst + s;
+      {
+        const int sn = s + NS - 1;
+        if (sn < nsteps) star_load<T, R>(ring + (sn % NS) * PS, in, a.vin, a.bc, pfirst + sn, y0, x0);
+        cp_async_commit();
+      }
+      // prefetch rho for the output plane that completes at this step
+      const int o = p - R;
+      T rho[PY];
+      if constexpr (MODE != MODE_APPLY) {
+#pragma unroll
+        for (int j = 0; j < PY; ++j) {
+          const int y = y0 + yb + j;
+          rho[j] = zero<T>();
+          if (o >= z0 && xin && y < a.vout.n[1])
+            rho[j] = static_cast<const T*>(a.rho)[(int64_t)b * a.vrho.sb + (int64_t)o * a.vrho.s0 +
+                                                  (int64_t)y * a.vrho.s1 + x];
+        }
+      }
+      cp_async_wait<NS - 1>();
+      T* sl = ring + (s % NS) * PS;
+      if (a.bc.use_phase) star_fix<T, R>(sl, a.vin, a.bc, p, y0, x0);
+      __syncthreads();
+
+      // column of PY + 2R values along axis 1 at this thread's x
+      T col[PY + 2 * R];
+#pragma unroll
+      for (int i = 0; i < PY + 2 * R; ++i) col[i] = sl[(yb + i) * W + tx + R];
+#pragma unroll
+      for (int j = 0; j < PY; ++j) {
+        const T v = col[j + R];
+        // in-plane part: centre + axis-1 + axis-2 neighbours
+        T part = scale(cc, v);
+#pragma unroll
+        for (int q = 1; q <= R; ++q) {
+          part = fmac(cy[R + q], col[j + R + q], part);
+          part = fmac(cy[R - q], col[j + R - q], part);
+        }
+        const T* row = sl + (yb + j + R) * W + tx + R;
+#pragma unroll
+        for (int q = 1; q <= R; ++q) {
+          part = fmac(cz[R + q], row[q], part);
+          part = fmac(cz[R - q], row[-q], part);
+        }
+        // scatter along axis 0: output plane p-R+m receives offset R-m
+#pragma unroll
+        for (int m = 0; m < 2 * R + 1; ++m) {
+          if (m == R)
+            acc[j][m] = add(acc[j][m], part);
+          else
+            acc[j][m] = fmac(cx[2 * R - m], v, acc[j][m]);
+        }
+        if constexpr (MODE == MODE_JACOBI) {
+#pragma unroll
+          for (int m = 0; m < R; ++m) cur[j][m] = cur[j][m + 1];
+          cur[j][R] = v;
+        }
+      }
+      // output plane o = p - R is complete
+      if (o >= z0) {
+#pragma unroll
+        for (int j = 0; j < PY; ++j) {
+          const int y = y0 + yb + j;
+          if (xin && y < a.vout.n[1]) {
+            const int64_t oi = (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
+            const T av = acc[j][0];
+            if constexpr (MODE == MODE_APPLY) {
+              static_cast<T*>(a.out)[oi] = av;
+            } else if constexpr (MODE == MODE_RESIDUAL) {
+              const T r = sub(av, rho[j]);
+              if (a.out) static_cast<T*>(a.out)[oi] = r;
+              sumsq += norm2(r);
+            } else {
+              if constexpr (!EltTraits<T>::cpx) {
+                const S w = (S)a.w;
+                const S wc = w / (S)a.c0;
+                static_cast<T*>(a.out)[oi] = (S(1) - w) * cur[j][0] + wc * (rho[j] - av);
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < PY; ++j) {
+#pragma unroll
+        for (int m = 0; m < 2 * R; ++m) acc[j][m] = acc[j][m + 1];
+        acc[j][2 * R] = zero<T>();
+      }
+      __syncthreads();
+    }
+  }
+  if constexpr (MODE == MODE_RESIDUAL) {
+    double tot = block_sum(sumsq, red);
+    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
+    grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);
+  }
+}
+
+}  // namespace gpw

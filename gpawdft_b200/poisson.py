@@ -1,0 +1,326 @@
+"""Multigrid Poisson solver on the GPU (drop-in for gpaw.poisson.PoissonSolver).
+
+``PoissonSolver(nn=3, relax='J', eps=2e-10, maxiter=1000,
+remove_moment=None, use_charge_center=False)`` with ``set_grid_descriptor``,
+``initialize``, ``solve(phi, rho, charge=None, eps=None, maxcharge=1e-6,
+zero_initial_phi=False) -> niter`` and ``PoissonConvergenceError`` as in
+gpaw/poisson.py:55-366.  The level hierarchy, smoothing schedule and the three
+charge branches follow the reference line by line; the V-cycles and their
+convergence loop run on the device in libgpwgrid.so (``gpw_poisson_*``).
+
+Two options go beyond the reference:
+  precision='fp32'  float32 V-cycles inside a float64 defect-correction loop
+                    (float64 residual, update, charge integral and norms);
+  solve_batch()     many independent same-grid solves in one batched launch
+                    sequence, each with its own convergence test.
+"""
+import ctypes
+import warnings
+from math import pi
+
+import numpy as np
+
+from . import _lib, arrays, blas
+from .fd_operators import Laplace, LaplaceA, LaplaceB
+from .gauss import Gaussian
+from .transformers import Transformer
+
+
+class PoissonConvergenceError(ArithmeticError):
+    """Raised when the V-cycles reach ``maxiter`` (gpaw/__init__.py:37)."""
+
+
+POISSON_GRID_WARNING = ('Grid unsuitable for Poisson solver!  The coarsest '
+                        'multigrid level has more than 36 points per axis.')
+
+
+def create_poisson_solver(name='fd', **kwargs):
+    if name == 'fd':
+        return PoissonSolver(**kwargs)
+    raise NotImplementedError('only the finite-difference solver is built')
+
+
+def PoissonSolver(dipolelayer=None, **kwargs):
+    if dipolelayer is not None:
+        raise NotImplementedError('DipoleCorrection is not part of this build')
+    return FDPoissonSolver(**kwargs)
+
+
+_PREC = {'fp64': 0, 'fp32': 1}
+
+
+class FDPoissonSolver:
+    def __init__(self, nn=3, relax='J', eps=2e-10, maxiter=1000,
+                 remove_moment=None, use_charge_center=False,
+                 precision='fp64', batch=1):
+        self.relax = relax
+        self.nn = nn
+        self.eps = eps
+        self.charged_periodic_correction = None
+        self.maxiter = maxiter
+        self.remove_moment = remove_moment
+        self.use_charge_center = use_charge_center
+        if relax == 'GS':
+            self.relax_method = 1
+        elif relax == 'J':
+            self.relax_method = 2
+        else:
+            raise NotImplementedError('Relaxation method %s' % relax)
+        if precision not in _PREC:
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.precision = precision
+        self.batch = int(batch)
+        self.description = None
+        self._engine = None
+        self.last_errors = None
+
+    def todict(self):
+        return {'name': 'fd', 'nn': self.nn, 'relax': self.relax,
+                'eps': self.eps, 'remove_moment': self.remove_moment}
+
+    def get_stencil(self):
+        return self.nn
+
+    def set_grid_descriptor(self, gd):
+        """gpaw/poisson.py:91-149."""
+        self.gd = gd
+        scale = -0.25 / pi
+        if self.nn == 'M':
+            if not gd.orthogonal:
+                raise RuntimeError('Cannot use Mehrstellen stencil with '
+                                   'non orthogonal cell.')
+            self.operators = [LaplaceA(gd, -scale)]
+            self.B = LaplaceB(gd)
+        else:
+            self.operators = [Laplace(gd, scale, self.nn)]
+            self.B = None
+        self.interpolators = []
+        self.restrictors = []
+        level = 0
+        self.presmooths = [2]
+        self.postsmooths = [1]
+        self.weights = [2.0 / 3.0]
+        while level < 8:
+            try:
+                gd2 = gd.coarsen()
+            except ValueError:
+                break
+            self.operators.append(Laplace(gd2, scale, 1))
+            self.interpolators.append(Transformer(gd2, gd))
+            self.restrictors.append(Transformer(gd, gd2))
+            self.presmooths.append(4)
+            self.postsmooths.append(4)
+            self.weights.append(1.0)
+            level += 1
+            gd = gd2
+        self.levels = level
+        self._engine = None
+        if self.operators[-1].gd.N_c.max() > 36:
+            warnings.warn(POISSON_GRID_WARNING + '\n' + self.get_description(),
+                          stacklevel=2)
+
+    def get_description(self):
+        name = {1: 'Gauss-Seidel', 2: 'Jacobi'}[self.relax_method]
+        coarsest_grid = self.operators[-1].gd.N_c
+        lines = ['%s solver with %d multi-grid levels'
+                 % (name, self.levels + 1),
+                 '    Coarsest grid: %s points' %
+                 ' x '.join([str(N) for N in coarsest_grid])]
+        if coarsest_grid.max() > 24:
+            lines.extend(['    Warning: Coarse grid has more than 24 points.',
+                          '             More multi-grid levels recommended.'])
+        lines.extend(['    Stencil: %s' % self.operators[0].description,
+                      '    Tolerance: %e' % self.eps,
+                      '    Max iterations: %d' % self.maxiter])
+        if self.remove_moment is not None:
+            lines.append('    Remove moments up to L=%d' % self.remove_moment)
+        if self.use_charge_center:
+            lines.append('    Compensate for charged system using center of '
+                         'majority charge')
+        return '\n'.join(lines)
+
+    def initialize(self, load_gauss=False):
+        """gpaw/poisson.py:174-195 (+ the device engine)."""
+        level = self.levels
+        self.step = 0.66666666 / self.operators[0].get_diagonal_element()
+        self.presmooths[level] = 8
+        self.postsmooths[level] = 8
+        self._make_engine(self.batch)
+        if load_gauss:
+            self.load_gauss()
+
+    def _make_engine(self, nbatch):
+        lib = _lib.load()
+        if self._engine is not None and self._engine[1] >= nbatch:
+            return
+        self._free_engine()
+        L = self.levels + 1
+        VP = ctypes.c_void_p
+        ops = (VP * L)(*[op.handle for op in self.operators])
+        rs = (VP * max(L - 1, 1))(*([t.handle for t in self.restrictors] or
+                                    [None]))
+        ips = (VP * max(L - 1, 1))(*([t.handle for t in self.interpolators] or
+                                     [None]))
+        pre = (ctypes.c_int * L)(*self.presmooths)
+        post = (ctypes.c_int * L)(*self.postsmooths)
+        w = (ctypes.c_double * L)(*self.weights)
+        h = VP()
+        _lib.check(lib.gpw_poisson_new(L, ops, rs, ips, pre, post, w,
+                                       self.relax_method, float(self.gd.dv),
+                                       int(nbatch), ctypes.byref(h)))
+        self._engine = (h, int(nbatch))
+        self._lib = lib
+
+    def _free_engine(self):
+        if self._engine is not None:
+            self._lib.gpw_poisson_free(self._engine[0])
+            self._engine = None
+
+    def __del__(self):
+        try:
+            self._free_engine()
+        except Exception:
+            pass
+
+    def load_gauss(self, center=None):
+        if not hasattr(self, 'rho_gauss') or center is not None:
+            gauss = Gaussian(self.gd, center=center)
+            self.rho_gauss = arrays.to_device(gauss.get_gauss(0))
+            self.phi_gauss = arrays.to_device(gauss.get_gauss_pot(0))
+
+    # ------------------------------------------------------------ solving
+    def solve(self, phi, rho, charge=None, eps=None, maxcharge=1e-6,
+              zero_initial_phi=False):
+        """gpaw/poisson.py:203-304; returns the number of V-cycles."""
+        assert np.all(tuple(phi.shape) == tuple(self.gd.n_c))
+        assert np.all(tuple(rho.shape) == tuple(self.gd.n_c))
+        if self._engine is None:
+            self.initialize()
+        if eps is None:
+            eps = self.eps
+        phi_d = arrays.to_device(phi)
+        rho_d = arrays.to_device(rho)
+        actual_charge = self.gd.integrate(rho_d)
+        background = (actual_charge / self.gd.dv /
+                      self.gd.get_size_of_global_array().prod())
+        if self.remove_moment:
+            raise NotImplementedError('remove_moment is not part of this '
+                                      'build')
+        if charge is None:
+            charge = actual_charge
+        if abs(charge) <= maxcharge:
+            niter = self.solve_neutral(phi_d, self._shifted(rho_d, background),
+                                       eps=eps)
+        elif abs(charge) > maxcharge and self.gd.pbc_c.all():
+            if zero_initial_phi:
+                phi_d.zero_()
+            niter = self.solve_neutral(phi_d, self._shifted(rho_d, background),
+                                       eps=eps)
+        elif abs(charge) > maxcharge and not self.gd.pbc_c.any():
+            if self.use_charge_center:
+                rho_h = rho if not arrays.is_device(rho) else \
+                    rho.cpu().numpy()
+                charge_sign = actual_charge / abs(actual_charge)
+                rho_sign = rho_h * charge_sign
+                rho_sign[np.where(rho_sign < 0)] = 0
+                absolute_charge = self.gd.integrate(rho_sign)
+                center = - self.gd.calculate_dipole_moment(rho_sign) \
+                    / absolute_charge
+                border_offset = np.inner(self.gd.h_cv, np.array((7, 7, 7)))
+                borders = np.inner(self.gd.h_cv, self.gd.N_c)
+                borders -= border_offset
+                if np.any(center > borders) or np.any(center < border_offset):
+                    raise RuntimeError('Poisson solver: center of charge '
+                                       'outside borders - please increase box')
+                self.load_gauss(center=center)
+            else:
+                self.load_gauss()
+            q = actual_charge / np.sqrt(4 * pi)
+            rho_neutral = rho_d.clone()
+            blas.axpy(-q, self.rho_gauss, rho_neutral)
+            if zero_initial_phi:
+                phi_d.zero_()
+            else:
+                blas.axpy(-q, self.phi_gauss, phi_d)
+            niter = self.solve_neutral(phi_d, rho_neutral, eps=eps)
+            blas.axpy(q, self.phi_gauss, phi_d)
+        else:
+            raise NotImplementedError('Charged systems with mixed periodic/'
+                                      'zero boundary conditions')
+        if not arrays.is_device(phi):
+            arrays.writeback(phi, phi_d)
+        return niter
+
+    def _shifted(self, rho_d, background):
+        out = rho_d.clone()
+        blas.add_scalar(rho_d, -background, out)
+        return out
+
+    def solve_neutral(self, phi, rho, eps=2e-10):
+        """gpaw/poisson.py:306-329 (one grid)."""
+        phi_d = arrays.to_device(phi)
+        niters = self._run(phi_d, arrays.to_device(rho), 1, [eps])
+        if not arrays.is_device(phi):
+            arrays.writeback(phi, phi_d)
+        return int(niters[0])
+
+    def _run(self, phi_d, rho_d, nb, eps_list):
+        if self.B is not None:
+            rho2 = arrays.empty_like_device(rho_d.shape,
+                                            arrays.np_dtype_of(rho_d))
+            self.B.apply(rho_d, rho2)
+            rho_d = rho2
+        self._make_engine(nb)
+        eps_a = np.ascontiguousarray(eps_list, float)
+        niter = np.zeros(nb, np.int32)
+        err = np.zeros(nb, float)
+        rc = self._lib.gpw_poisson_solve(
+            self._engine[0], arrays.ptr(phi_d), arrays.ptr(rho_d), nb,
+            eps_a.ctypes.data, int(self.maxiter), _PREC[self.precision],
+            niter.ctypes.data, err.ctypes.data, arrays.stream())
+        self.last_errors = err
+        if rc == _lib.GPW_ECONV:
+            raise PoissonConvergenceError(
+                'Poisson solver did not converge in %d iterations!' %
+                self.maxiter)
+        _lib.check(rc)
+        if self.gd.pbc_c.all():
+            # set the average potential to zero in periodic systems
+            npts = int(np.prod(self.gd.get_size_of_global_array()))
+            sums = blas.vector_sums(phi_d, nb)
+            for b in range(nb):
+                blas.add_scalar(phi_d[b] if nb > 1 else phi_d,
+                                -sums[b] / npts)
+        return niter
+
+    def solve_batch(self, phi_b, rho_b, eps=None):
+        """Independent neutral solves of a batch (nb, *n_c) on one grid.
+
+        Each solve stops at its own ``error <= eps``; results and V-cycle
+        counts equal those of solving each grid alone.  Returns the per-solve
+        iteration counts.
+        """
+        if self._engine is None:
+            self.initialize()
+        nb = int(phi_b.shape[0])
+        if eps is None:
+            eps = self.eps
+        eps_list = np.broadcast_to(np.asarray(eps, float), (nb,))
+        phi_d = arrays.to_device(phi_b)
+        rho_d = arrays.to_device(rho_b)
+        niter = self._run(phi_d, rho_d, nb, eps_list)
+        if not arrays.is_device(phi_b):
+            arrays.writeback(phi_b, phi_d)
+        return niter
+
+    def estimate_memory(self, mem=None):
+        gdbytes = int(np.prod(self.gd.n_c)) * 8
+        nbytes = 0
+        for level in range(self.levels + 1):
+            nbytes += 4 * gdbytes
+            gdbytes //= 8
+        return nbytes
+
+    def __repr__(self):
+        return 'PoissonSolver(relax=\'%s\', nn=%s, eps=%e)' % (
+            self.relax, repr(self.nn), self.eps)

@@ -1,0 +1,198 @@
+/*
+ * gpwgrid.h -- C ABI of the B200 (sm_100a) implementation of GPAW's
+ * real-space grid hot path: finite-difference stencils with halo fill,
+ * restriction / interpolation transformers, weighted-Jacobi relaxation and
+ * the multigrid Poisson V-cycle.
+ *
+ * The entry points replace the reference's extension types for this path,
+ *   _gpaw.Operator     c/operators.c:462-495   (registered at c/_gpaw.c:154)
+ *   _gpaw.Transformer  c/transformers.c:219-262 (registered at c/_gpaw.c:157)
+ * and the kernels beneath them (c/bmgs/fd.c, relax.c, restrict.c,
+ * interpolate.c, cut.c, paste.c, translate.c, zero.c and the serial halo fill
+ * of c/bc.c).  Constructor arguments keep the reference's meaning and
+ * layout; arrays are device pointers owned by the caller (as in the
+ * reference, where the caller owns every NumPy array and C keeps raw pointers
+ * only for the duration of a call).
+ *
+ * Conventions
+ *   - Grids are C-contiguous (..., n0, n1, n2); `nin` leading grids are
+ *     processed by one call (c/operators.c:325-327).
+ *   - `phases` is the (3, 2) complex Bloch phase table phase_cd as 12 doubles
+ *     (re, im interleaved), host memory, required for complex data on periodic
+ *     axes; NULL means all phases 1.
+ *   - `stream` is a cudaStream_t (NULL: legacy default stream).  Calls are
+ *     asynchronous on that stream unless stated otherwise.
+ *   - Every function returns GPW_OK or an error code; gpw_last_error() gives
+ *     a message.  Handles are not thread-safe.
+ *   - No handle or function here uses MPI; the reference's `comm` argument is
+ *     dropped (single GPU, no domain decomposition).
+ */
+#ifndef GPWGRID_H
+#define GPWGRID_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define GPW_OK 0
+#define GPW_ENOMEM 12     /* device allocation failed */
+#define GPW_EINVAL 22     /* bad shape / dtype / argument */
+#define GPW_ENOTSUP 95    /* valid request this build does not implement */
+#define GPW_ETIMEDOUT 110 /* a bounded device-side wait gave up */
+#define GPW_ECONV 1001    /* Poisson V-cycles reached maxiter (PoissonConvergenceError) */
+#define GPW_ECUDA 1002    /* a CUDA runtime call failed */
+
+/* ------------------------------------------------------------ element types */
+#define GPW_F64 0  /* float64     (reference NPY_DOUBLE) */
+#define GPW_C128 1 /* complex128  (reference NPY_CDOUBLE) */
+#define GPW_F32 2  /* float32     (new form, no reference counterpart) */
+#define GPW_C64 3  /* complex64   (new form, no reference counterpart) */
+
+typedef struct gpw_operator gpw_operator;
+typedef struct gpw_transformer gpw_transformer;
+typedef struct gpw_poisson gpw_poisson;
+typedef void *gpw_stream; /* cudaStream_t */
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char *gpw_last_error(void);
+/* Library version string. */
+const char *gpw_version(void);
+
+/* ------------------------------------------------------------ FD operator */
+
+/* Replaces _gpaw.Operator(coefs, offsets, size, range, neighbors, real, comm,
+ * cfd), c/operators.c:462-495 (built by gpaw/fd_operators.py:75-77).
+ *   coefs[ncoefs]     stencil coefficients (float64)
+ *   offsets[ncoefs]   linear offsets into the grid padded by `range` on all
+ *                     six faces (gpaw/fd_operators.py:50-52)
+ *   size[3]           interior extent n_c
+ *   range             padding mp (largest offset)
+ *   neighbors[3][2]   neighbor_cd: 0 = this domain (periodic wrap), -1 = zero
+ *                     boundary (gpaw/domain.py:111-139, serial)
+ *   real              1 for float data, 0 for complex (sets the halo type)
+ *   cfd               1 if every offset lies on one axis (star stencil)     */
+int gpw_operator_new(const double *coefs, const int64_t *offsets, int ncoefs,
+                     const int64_t size[3], int range,
+                     const int64_t neighbors[6], int real, int cfd,
+                     gpw_operator **out);
+
+/* Operator.apply(input, output, phases), c/operators.c:316-405:
+ * out[x] = sum_p coef_p * in_padded[x + offset_p] for `nin` grids.  `in` may
+ * equal `out` (in-place, as the reference allows).                          */
+int gpw_operator_apply(gpw_operator *op, int dtype, const void *in, void *out,
+                       int64_t nin, const double *phases, gpw_stream stream);
+
+/* Operator.relax(relax_method, func, source, nrelax, w), c/operators.c:49-91
+ * and c/bmgs/relax.c:7-73.  relax_method 2 = weighted Jacobi (each sweep
+ * func = (1-w) func + w (source - sum_{p!=0} c_p func[x+o_p]) / c_0);
+ * relax_method 1 = lexicographic Gauss-Seidel (w ignored), computed as a
+ * hyperplane wavefront that reproduces the lexicographic update order.
+ * dtype GPW_F64 (reference) or GPW_F32.  func is updated in place.
+ * `nin` independent grids (func, source of shape (nin, n0, n1, n2)) are
+ * relaxed by one call (nin = 1 is the reference's call).                    */
+int gpw_operator_relax(gpw_operator *op, int dtype, int relax_method,
+                       void *func, const void *source, int64_t nin,
+                       int nrelax, double w, gpw_stream stream);
+
+/* Operator.get_diagonal_element(), c/operators.c:408-421.                   */
+int gpw_operator_get_diagonal_element(const gpw_operator *op, double *out);
+
+/* Fused residual r = A func - source and sum |r|^2 (new; replaces the
+ * apply + `residual -= rho` + np.dot sequence of gpaw/poisson.py:357-361).
+ * r may be NULL (norm only).  *sumsq_dev is a device double receiving the
+ * deterministic sum over all `nin` grids.                                  */
+int gpw_operator_residual(gpw_operator *op, int dtype, const void *func,
+                          const void *source, void *r, int64_t nin,
+                          double *sumsq_dev, gpw_stream stream);
+
+void gpw_operator_free(gpw_operator *op);
+
+/* ------------------------------------------------------------ transformer */
+
+/* Replaces _gpaw.Transformer(size_in, size_out, k, paddings, npaddings, skip,
+ * neighbors, real, comm, interpolate), c/transformers.c:219-262 (built by
+ * gpaw/transformers.py:71-76).  k = 2 nn in {2, 4, 6, 8}; paddings,
+ * npaddings, skip and neighbors are (3, 2) tables as the reference computes
+ * them (gpaw/transformers.py:31-54).                                        */
+int gpw_transformer_new(const int64_t size_in[3], const int64_t size_out[3],
+                        int k, const int64_t paddings[6],
+                        const int64_t npaddings[6], const int64_t skip[6],
+                        const int64_t neighbors[6], int real, int interpolate,
+                        gpw_transformer **out);
+
+/* Transformer.apply(input, output, phases), c/transformers.c:127-185:
+ * halo fill then restriction (c/bmgs/restrict.c:137-154) or interpolation
+ * (c/bmgs/interpolate.c:141-168) of `nin` grids.                            */
+int gpw_transformer_apply(gpw_transformer *tr, int dtype, const void *in,
+                          void *out, int64_t nin, const double *phases,
+                          gpw_stream stream);
+
+void gpw_transformer_free(gpw_transformer *tr);
+
+/* ------------------------------------------------------------ grid BLAS */
+/* The NumPy / BLAS glue around the hot path (gpaw/utilities/blas.py axpy,
+ * scal; gpaw/grid_descriptor.py:263-292 integrate) as device kernels.
+ * n counts elements of `dtype`.                                             */
+
+/* y = alpha * x + y   (complex alpha as (re, im); imaginary part ignored for
+ * real dtypes)                                                              */
+int gpw_axpy(int dtype, int64_t n, double alpha_re, double alpha_im,
+             const void *x, void *y, gpw_stream stream);
+/* x = alpha * x                                                             */
+int gpw_scal(int dtype, int64_t n, double alpha_re, double alpha_im, void *x,
+             gpw_stream stream);
+/* out[m] = sum_i x[m, i] for m < nvec vectors of length n (real dtypes; for
+ * complex dtypes out holds (re, im) pairs).  Deterministic order.          */
+int gpw_sum(int dtype, int64_t nvec, int64_t n, const void *x, double *out_dev,
+            gpw_stream stream);
+/* out[m] = sum_i conj(x[m, i]) y[m, i] (real part only for complex).        */
+int gpw_dot(int dtype, int64_t nvec, int64_t n, const void *x, const void *y,
+            double *out_dev, gpw_stream stream);
+/* y = x + c (real dtypes, c added to every element)                         */
+int gpw_add_scalar(int dtype, int64_t n, double c, const void *x, void *y,
+                   gpw_stream stream);
+
+/* ------------------------------------------------------------ Poisson */
+
+/* Multigrid engine behind FDPoissonSolver (gpaw/poisson.py:61-366).  The
+ * level hierarchy is the one gpaw/poisson.py:91-132 builds: operators[0..L]
+ * (level 0 the caller's Laplacian, coarse levels nn=1), restrictors[0..L-1]
+ * (level l -> l+1) and interpolators[0..L-1] (level l+1 -> l), smoothing
+ * counts presmooths/postsmooths[0..L] and Jacobi weights[0..L] (schedule of
+ * gpaw/poisson.py:111-128, 191-192).  The handles must outlive the engine.
+ * nbatch_max: largest number of independent same-grid solves per call.      */
+int gpw_poisson_new(int nlevels, gpw_operator *const *operators,
+                    gpw_transformer *const *restrictors,
+                    gpw_transformer *const *interpolators,
+                    const int *presmooths, const int *postsmooths,
+                    const double *weights, int relax_method, double dv,
+                    int64_t nbatch_max, gpw_poisson **out);
+
+/* solve_neutral + iterate2 (gpaw/poisson.py:306-366) for `nbatch`
+ * independent grids phi[b], rho[b] (device, float64, contiguous n_c):
+ * V-cycles until error = sum r^2 dv <= eps[b] or niter == maxiter.
+ * precision 0: plain float64 V-cycles (the reference's method).
+ * precision 1: float32 V-cycles inside a float64 defect-correction loop
+ *              (float64 residual, update and norms).
+ * Writes niter[b] and the final error[b] (host arrays).  Synchronises the
+ * stream.  Returns GPW_ECONV if any solve reached maxiter.                  */
+int gpw_poisson_solve(gpw_poisson *ps, double *phi, const double *rho,
+                      int64_t nbatch, const double *eps, int maxiter,
+                      int precision, int *niter, double *error,
+                      gpw_stream stream);
+
+/* Counters of the last gpw_poisson_solve call: device kernels launched
+ * (graph kernel nodes x replays + direct launches) and graph replays.       */
+int gpw_poisson_last_stats(const gpw_poisson *ps, int64_t *kernel_launches,
+                           int64_t *graph_launches);
+
+void gpw_poisson_free(gpw_poisson *ps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPWGRID_H */

@@ -1,0 +1,22 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line('markers',
+                            'gpu: needs a CUDA device (B200, sm_100a)')
+
+
+@pytest.fixture(scope='session')
+def cuda():
+    import torch
+    assert torch.cuda.is_available(), 'GPU tests need a CUDA device'
+    from gpawdft_b200 import _lib
+    _lib.load()
+    return torch.device('cuda:0')

@@ -1,0 +1,149 @@
+"""GPU parity of the multigrid Poisson solver (gpaw/poisson.py path).
+
+The plain float64 method must reproduce the oracle's V-cycle count, its
+potential to the solver tolerance and the Hartree energy E_H = 1/2 dv
+sum(phi rho) to 1e-8 Ha.  Also: charged periodic / zero-boundary branches,
+Gauss-Seidel, batched solves (each equal to its single solve) and the
+float32 defect-correction form (its error vs the float64 result stated).
+"""
+import numpy as np
+import pytest
+
+from gpawdft_b200.workloads import gaussian_density
+from oracle import layer as ol
+from oracle.geometry import GridDescriptor as OGD
+
+pytestmark = pytest.mark.gpu
+
+
+def solvers(N, L, pbc, **kw):
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    gd = GridDescriptor((N,) * 3, (L,) * 3, pbc)
+    ogd = OGD((N,) * 3, (L,) * 3, pbc)
+    ps = PoissonSolver(**kw)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    ops = ol.PoissonSolver(**kw)
+    ops.set_grid_descriptor(ogd)
+    ops.initialize()
+    return gd, ogd, ps, ops
+
+
+def hartree(gd, phi, rho):
+    return 0.5 * gd.dv * float(np.dot(phi.ravel(), rho.ravel()))
+
+
+@pytest.mark.parametrize('N', [32, 64])
+def test_neutral_zero_boundary(cuda, N):
+    """Benchmark config (b) recipe: 8 neutral Gaussians, nn=3, Jacobi."""
+    rho, L = gaussian_density(N, 0.2, 8, 1)
+    gd, ogd, ps, ops = solvers(N, L, 0, nn=3, relax='J', eps=2e-10)
+    phi = gd.zeros()
+    n = ps.solve(phi, rho)
+    ophi = ogd.zeros()
+    on = ops.solve(ophi, rho)
+    assert n == on
+    # both stop at sum(r^2) dv <= eps: compare potentials at that accuracy
+    assert np.abs(phi - ophi).max() < 1e-6 * np.abs(ophi).max()
+    assert abs(hartree(ogd, phi, rho) - hartree(ogd, ophi, rho)) < 1e-8
+    assert np.allclose(ps.last_errors, ops.errors[-1], rtol=1e-6)
+
+
+def test_tight_tolerance_trajectory(cuda):
+    """To relative residual 1e-10: every V-cycle's error follows the oracle."""
+    N = 32
+    rho, L = gaussian_density(N, 0.2, 8, 3)
+    gd, ogd, ps, ops = solvers(N, L, 0, nn=3, relax='J', maxiter=200)
+    eps = 1e-20 * float(np.dot(rho.ravel(), rho.ravel())) * gd.dv
+    phi = gd.zeros()
+    n = ps.solve(phi, rho, eps=eps)
+    ophi = ogd.zeros()
+    on = ops.solve(ophi, rho, eps=eps)
+    assert n == on
+    assert np.abs(phi - ophi).max() < 1e-12 * np.abs(ophi).max() + 1e-14
+    assert abs(hartree(ogd, phi, rho) - hartree(ogd, ophi, rho)) < 1e-8
+
+
+def test_charged_periodic(cuda):
+    N = 32
+    rho, L = gaussian_density(N, 0.25, 4, 7, pbc=True)
+    rho += 0.01  # net charge -> homogeneous background branch
+    gd, ogd, ps, ops = solvers(N, L, 1, nn=2, relax='J', eps=1e-14)
+    phi = gd.zeros()
+    n = ps.solve(phi, rho)
+    ophi = ogd.zeros()
+    on = ops.solve(ophi, rho)
+    assert abs(n - on) <= 1
+    assert np.abs(phi - ophi).max() < 1e-7 * np.abs(ophi).max()
+    assert abs(phi.mean()) < 1e-12
+
+
+@pytest.mark.parametrize('center', [False, True])
+def test_charged_zero_boundary(cuda, center):
+    """Gaussian-compensation branch (gpaw/poisson.py:249-299)."""
+    N = 48
+    a = 20.0
+    from oracle.gauss import Gaussian as OGauss
+    ogd0 = OGD((N,) * 3, (a,) * 3, 0)
+    rho = OGauss(ogd0, a=19, center=(a / 2, a / 2, 3 * a / 4)).get_gauss(0)
+    gd, ogd, ps, ops = solvers(N, a, 0, nn=3, use_charge_center=center)
+    phi = gd.zeros()
+    n = ps.solve(phi, rho, charge=1.0)
+    ophi = ogd.zeros()
+    on = ops.solve(ophi, rho, charge=1.0)
+    assert n == on
+    assert np.abs(phi - ophi).max() < 1e-6 * np.abs(ophi).max()
+
+
+def test_gauss_seidel_solver(cuda):
+    N = 16
+    rho, L = gaussian_density(N, 0.3, 4, 9)
+    gd, ogd, ps, ops = solvers(N, L, 0, nn=1, relax='GS', eps=1e-12)
+    phi = gd.zeros()
+    n = ps.solve(phi, rho)
+    ophi = ogd.zeros()
+    on = ops.solve(ophi, rho)
+    assert n == on
+    assert np.abs(phi - ophi).max() <= 1e-13 * np.abs(ophi).max()
+
+
+def test_batch_equals_single(cuda):
+    N = 32
+    rhos = []
+    for s in range(3):
+        rho, L = gaussian_density(N, 0.2, 4 + 4 * s, 30 + s)
+        rhos.append(rho)
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    ps = PoissonSolver(nn=3, batch=3)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    phib = np.zeros((3,) + tuple(gd.n_c))
+    nb = ps.solve_batch(phib, np.array(rhos), eps=2e-10)
+    for s in range(3):
+        phi = gd.zeros()
+        n = ps.solve_neutral(phi, rhos[s] - rhos[s].mean(), eps=2e-10)
+        assert n == nb[s]
+        assert np.array_equal(phi, phib[s])
+
+
+def test_fp32_defect_correction(cuda):
+    """FP32 V-cycles inside FP64 defect correction reach the same residual."""
+    N = 64
+    rho, L = gaussian_density(N, 0.2, 8, 1)
+    gd, ogd, ps, ops = solvers(N, L, 0, nn=3, maxiter=200)
+    eps = 1e-20 * float(np.dot(rho.ravel(), rho.ravel())) * gd.dv
+    phi64 = gd.zeros()
+    ps.solve(phi64, rho, eps=eps)
+    ps32 = type(ps)(nn=3, maxiter=200, precision='fp32')
+    ps32.set_grid_descriptor(gd)
+    ps32.initialize()
+    phi32 = gd.zeros()
+    n32 = ps32.solve(phi32, rho, eps=eps)
+    assert ps32.last_errors[0] <= eps
+    e64 = hartree(ogd, phi64, rho)
+    e32 = hartree(ogd, phi32, rho)
+    assert abs(e64 - e32) < 1e-8
+    assert n32 < 200
