@@ -196,6 +196,7 @@ int gpw_operator_new(const double* coefs, const int64_t* offsets, int ncoefs, co
                      const int64_t neighbors[6], int real, int cfd, gpw_operator** out) {
   if (!coefs || !offsets || !size || !neighbors || !out) return fail(GPW_EINVAL, "null argument");
   gpw_operator* op = new gpw_operator();
+  device_status_word();  // allocate outside any stream capture
   int rc = build_opdesc(op->d, coefs, offsets, ncoefs, size, range, neighbors, real, cfd);
   if (rc) {
     delete op;

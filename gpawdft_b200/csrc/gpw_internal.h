@@ -41,6 +41,20 @@ inline GridView contiguous_view(const int n[3]) {
 }
 inline int64_t view_points(const GridView& v) { return (int64_t)v.n[0] * v.n[1] * v.n[2]; }
 
+// Engine-owned grids: rows padded to a multiple of 8 elements (64 bytes for
+// float64), so every row, plane and batch member starts 16-byte aligned as
+// the TMA tile loads and the 2-point vector stores require.
+inline GridView pitched_view(const int n[3]) {
+  GridView v;
+  v.n[0] = n[0];
+  v.n[1] = n[1];
+  v.n[2] = n[2];
+  v.s1 = ((int64_t)n[2] + 7) / 8 * 8;
+  v.s0 = (int64_t)n[1] * v.s1;
+  v.sb = (int64_t)n[0] * v.s0;
+  return v;
+}
+
 // ---------------------------------------------------------------- operator
 struct OpDesc {
   int n[3];
@@ -127,5 +141,10 @@ struct SumScratch {
 };
 
 int num_sms();
+
+// Device status word written by kernels whose bounded waits expire
+// (GPW_ETIMEDOUT); allocated on first use, which must not happen inside a
+// stream capture (handle constructors call it).
+int* device_status_word();
 
 }  // namespace gpw

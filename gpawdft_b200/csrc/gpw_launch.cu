@@ -3,10 +3,14 @@
 #include <algorithm>
 #include <mutex>
 
+#include <cudaTypedefs.h>
+
 #include "gpw_blas.cuh"
 #include "gpw_internal.h"
+#include "gpw_star_tma.cuh"
 #include "gpw_stencil.cuh"
 #include "gpw_transfer.cuh"
+#include "gpw_transfer_k2.cuh"
 
 namespace gpw {
 
@@ -54,7 +58,7 @@ static cudaError_t run_star(const StencilArgs& a0, const OpDesc& d, int nbatch, 
   cudaError_t e = cudaSuccess;
   std::call_once(once, [&] { e = smem_optin(kern, smem); });
   if (e != cudaSuccess) return e;
-  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, d.sc);
+  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, d.sc);  // NT threads
   return cudaGetLastError();
 }
 
@@ -103,7 +107,7 @@ int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& v, int 
   int tz, ty, minz;
   if (use_star) {
     tz = 32;
-    ty = 32;
+    ty = GPW_STAR_TY;
     minz = 2 * d.R + 2;
   } else {
     tz = GEN_TZ;
@@ -113,7 +117,111 @@ int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& v, int 
   const int gx = (v.n[2] + tz - 1) / tz, gy = (v.n[1] + ty - 1) / ty;
   int zc, nc;
   choose_chunks(v.n[0], (int64_t)gx * gy * nbatch, minz, zc, nc);
-  return gx * gy * nc;
+  int nblk = gx * gy * nc;
+  if (use_star) {  // the TMA tile (64 x 16, 4R+4 minimum chunk) may be chosen instead
+    // smallest TMA tile of any epilogue: an upper bound on the CTA count
+    constexpr int TTY = TmaCfg<double, 1, MODE_APPLY>::TY, TTZ = TmaCfg<double, 1, MODE_APPLY>::TZ;
+    const int tx2 = (v.n[2] + TTZ - 1) / TTZ, ty2 = (v.n[1] + TTY - 1) / TTY;
+    choose_chunks(v.n[0], (int64_t)tx2 * ty2 * nbatch, 4 * d.R + 4, zc, nc);
+    nblk = std::max(nblk, tx2 * ty2 * nc);
+  }
+  return nblk;
+}
+
+// ------------------------------------------------------------------ TMA path
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+static int* g_status_dev = nullptr;  // device status word of TMA kernels
+
+int* device_status_word() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    if (cudaMalloc(&g_status_dev, sizeof(int)) == cudaSuccess) cudaMemset(g_status_dev, 0, sizeof(int));
+    tensor_map_encoder();  // resolve the driver entry point outside any capture too
+  });
+  return g_status_dev;
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+static bool view_tma_ok(const GridView& v, size_t es, int nbatch) {
+  // strides (bytes) multiples of 16 and even element strides (2-point stores)
+  if ((v.s1 * es) % 16 || (v.s0 * es) % 16) return false;
+  if (nbatch > 1 && (v.sb * es) % 16) return false;
+  if (v.s1 % 2 || v.s0 % 2 || (nbatch > 1 && v.sb % 2)) return false;
+  return true;
+}
+
+template <typename S, int R, int MODE>
+static cudaError_t run_star_tma(const StencilArgs& a0, int nbatch, const StarCoefs& sc, cudaStream_t st) {
+  using C = TmaCfg<S, R, MODE>;
+  auto enc = tensor_map_encoder();
+  if (!enc) return cudaErrorNotSupported;
+  StencilArgs a = a0;
+  const GridView& vi = a.vin;
+  CUtensorMap map;
+  cuuint64_t dims[4] = {(cuuint64_t)vi.n[2], (cuuint64_t)vi.n[1], (cuuint64_t)vi.n[0], (cuuint64_t)nbatch};
+  cuuint64_t strides[3] = {(cuuint64_t)(vi.s1 * sizeof(S)), (cuuint64_t)(vi.s0 * sizeof(S)),
+                           (cuuint64_t)(std::max<int64_t>(vi.sb, vi.s0 * vi.n[0]) * sizeof(S))};
+  cuuint32_t box[4] = {(cuuint32_t)C::W, (cuuint32_t)C::H, 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(&map, sizeof(S) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                   const_cast<void*>(a.in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  const GridView& v = a.vout;
+  dim3 grid((v.n[2] + C::TZ - 1) / C::TZ, (v.n[1] + C::TY - 1) / C::TY, 1);
+  choose_chunks(v.n[0], (int64_t)grid.x * grid.y * nbatch, 4 * R + 4, a.zchunk, a.nchunk);
+  grid.z = a.nchunk * nbatch;
+  a.nblk_seg = grid.x * grid.y * a.nchunk;
+  TmaArgs ta{a, device_status_word()};
+  auto kern = star_tma_kernel<S, R, MODE>;
+  static std::once_flag once;
+  cudaError_t e = cudaSuccess;
+  std::call_once(once, [&] { e = smem_optin(kern, C::smem); });
+  if (e != cudaSuccess) return e;
+  kern<<<grid, dim3(C::NTX, C::NTY), C::smem, st>>>(map, ta, sc);
+  return cudaGetLastError();
+}
+
+template <typename S, int MODE>
+static cudaError_t dispatch_star_tma(const StencilArgs& a, const OpDesc& d, int nbatch, cudaStream_t st) {
+  switch (d.R) {
+    case 1: return run_star_tma<S, 1, MODE>(a, nbatch, d.sc, st);
+    case 2: return run_star_tma<S, 2, MODE>(a, nbatch, d.sc, st);
+    case 3: return run_star_tma<S, 3, MODE>(a, nbatch, d.sc, st);
+    case 4: return run_star_tma<S, 4, MODE>(a, nbatch, d.sc, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// The TMA path serves real zero-boundary star stencils whose arrays are
+// 16-byte aligned with 16-byte (and even-element) strides.
+static bool tma_path_ok(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, const void* out,
+                        const GridView& vout, const void* rho, const GridView& vrho, int nbatch) {
+  if (dtype != GPW_F64 && dtype != GPW_F32) return false;
+  if (d.periodic[0] || d.periodic[1] || d.periodic[2]) return false;
+  const bool star = (mode == MODE_JACOBI) ? d.star_jacobi : d.star;
+  if (!star || !star_radius_ok(d.R)) return false;
+  if (in == out) return false;
+  if (!tensor_map_encoder()) return false;
+  const size_t es = elt_size(dtype);
+  if (!aligned16(in) || !view_tma_ok(vin, es, nbatch)) return false;
+  if (out && (!aligned16(out) || !view_tma_ok(vout, es, nbatch))) return false;
+  if (mode != MODE_APPLY && (!aligned16(rho) || !view_tma_ok(vrho, es, nbatch))) return false;
+  return true;
 }
 
 cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, void* out,
@@ -132,6 +240,21 @@ cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in,
   a.c0 = d.coefs.empty() ? 1.0 : d.coefs[0];
   a.active = active;
   a.gsum = gs;
+  if (tma_path_ok(d, dtype, mode, in, vin, out, vout, rho, vrho, nbatch)) {
+    if (dtype == GPW_F64) {
+      switch (mode) {
+        case MODE_APPLY: return dispatch_star_tma<double, MODE_APPLY>(a, d, nbatch, st);
+        case MODE_RESIDUAL: return dispatch_star_tma<double, MODE_RESIDUAL>(a, d, nbatch, st);
+        case MODE_JACOBI: return dispatch_star_tma<double, MODE_JACOBI>(a, d, nbatch, st);
+      }
+    } else {
+      switch (mode) {
+        case MODE_APPLY: return dispatch_star_tma<float, MODE_APPLY>(a, d, nbatch, st);
+        case MODE_RESIDUAL: return dispatch_star_tma<float, MODE_RESIDUAL>(a, d, nbatch, st);
+        case MODE_JACOBI: return dispatch_star_tma<float, MODE_JACOBI>(a, d, nbatch, st);
+      }
+    }
+  }
   OpDesc dd = d;
   if (!star_radius_ok(dd.R)) {
     dd.star = false;
@@ -232,6 +355,24 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
   a.base = base;
   if (vbase) a.vbase = *vbase;
   const bool interp = d.interpolate != 0;
+  if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32)) {
+    dim3 grid((vout.n[2] + K2_TX - 1) / K2_TX, (vout.n[1] + K2_TY - 1) / K2_TY, 1);
+    choose_chunks(vout.n[0], (int64_t)grid.x * grid.y * nbatch, 4, a.zchunk, a.nchunk);
+    grid.z = a.nchunk * nbatch;
+    const dim3 blk(K2_TX, K2_TY);
+    if (dtype == GPW_F64) {
+      if (interp)
+        interpolate_k2_kernel<double><<<grid, blk, 0, st>>>(a);
+      else
+        restrict_k2_kernel<double><<<grid, blk, 0, st>>>(a);
+    } else {
+      if (interp)
+        interpolate_k2_kernel<float><<<grid, blk, 0, st>>>(a);
+      else
+        restrict_k2_kernel<float><<<grid, blk, 0, st>>>(a);
+    }
+    return cudaGetLastError();
+  }
   switch (dtype) {
     case GPW_F64: return dispatch_transfer<double>(a, d.k, interp, nbatch, st);
     case GPW_C128: return dispatch_transfer<double2>(a, d.k, interp, nbatch, st);

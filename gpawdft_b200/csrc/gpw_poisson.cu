@@ -212,7 +212,7 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
     Level& L = ps->lv[l];
     if (!operators[l]) return fail(GPW_EINVAL, "poisson: null operator");
     L.op = operator_desc(operators[l]);
-    L.v = contiguous_view(L.op->n);
+    L.v = pitched_view(L.op->n);
     L.pre = presmooths[l];
     L.post = postsmooths[l];
     L.w = weights[l];
@@ -222,11 +222,13 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
       L.interp = transformer_desc(interpolators[l]);
       if (L.restr->interpolate || !L.interp->interpolate) return fail(GPW_EINVAL, "poisson: transformer kinds");
     }
-    const size_t pts = (size_t)view_points(L.v) * nbatch_max;
+    const size_t pts = (size_t)L.v.sb * nbatch_max;
     int rc;
     if ((rc = L.phi[0].ensure(pts * 8)) || (rc = L.phi[1].ensure(pts * 8)) || (rc = L.rho.ensure(pts * 8)) ||
         (rc = L.res.ensure(pts * 8)))
       return rc;
+    // row padding is never read as data; keep it finite
+    for (Workspace* w : {&L.phi[0], &L.phi[1], &L.rho, &L.res}) cudaMemset(w->ptr, 0, w->bytes);
   }
   // level shapes must chain through the transformers
   for (int l = 0; l + 1 < nlevels; ++l) {
@@ -239,7 +241,7 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
   int rc;
   if ((rc = ps->d_err.ensure(nbatch_max * 8)) || (rc = ps->d_eps.ensure(nbatch_max * 8)) ||
       (rc = ps->d_niter.ensure(nbatch_max * 4)) || (rc = ps->d_active.ensure(nbatch_max)) ||
-      (rc = ps->d_any.ensure(16)) || (rc = ps->d_maxiter.ensure(16)) || (rc = ps->d_r64.ensure((size_t)view_points(ps->lv[0].v) * nbatch_max * 8)))
+      (rc = ps->d_any.ensure(16)) || (rc = ps->d_maxiter.ensure(16)) || (rc = ps->d_r64.ensure((size_t)ps->lv[0].v.sb * nbatch_max * 8)))
     return rc;
   if (relax_method == 1) {
     size_t mx = 0;
@@ -252,6 +254,7 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
   for (auto& L : ps->lv) maxblk = std::max<int64_t>(maxblk, stencil_blocks_per_member(*L.op, MODE_RESIDUAL, L.v, 1));
   (void)nblk;
   if ((rc = ps->sums.ensure(nbatch_max, maxblk))) return rc;
+  if (!device_status_word()) return fail(GPW_ENOMEM, "status word allocation");
   cudaError_t e = cudaMallocHost(&ps->h_any, sizeof(int));
   if (e != cudaSuccess) return cuda_fail(e, "pinned alloc");
   *out = ps.release();
@@ -269,11 +272,12 @@ extern "C" int gpw_poisson_last_stats(const gpw_poisson* ps, int64_t* kernel_lau
 
 static int ensure_f32(gpw_poisson* ps) {
   for (auto& L : ps->lv) {
-    const size_t pts = (size_t)view_points(L.v) * ps->nbmax;
+    const size_t pts = (size_t)L.v.sb * ps->nbmax;
     int rc;
     if ((rc = L.phi32[0].ensure(pts * 4)) || (rc = L.phi32[1].ensure(pts * 4)) || (rc = L.rho32.ensure(pts * 4)) ||
         (rc = L.res32.ensure(pts * 4)))
       return rc;
+    for (Workspace* w : {&L.phi32[0], &L.phi32[1], &L.rho32, &L.res32}) cudaMemset(w->ptr, 0, w->bytes);
   }
   return GPW_OK;
 }
@@ -303,7 +307,9 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, int maxit
     r.ok(cudaGetLastError());
   }
   // error = sum(r^2) dv on level 0 after post-smoothing (gpaw/poisson.py:357-361)
-  r.ok(launch_stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, L0.v, ps->d_r64.ptr, L0.v, L0.rho.ptr, L0.v, nb,
+  // (the float64 residual itself is kept only as the next defect-correction right-hand side)
+  r.ok(launch_stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, L0.v, prec == 1 ? ps->d_r64.ptr : nullptr, L0.v,
+                      L0.rho.ptr, L0.v, nb,
                       bc, 1.0, r.active, ps->sums.gs(), st));
   converge_update_kernel<<<1, 256, 0, st>>>(nb, ps->sums.gs().result, ps->dv, (const double*)ps->d_eps.ptr,
                                             (const int*)ps->d_maxiter.ptr,
@@ -334,8 +340,10 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
       (e = cudaMemcpyAsync(ps->d_niter.ptr, ones.data(), nb * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(ps->d_active.ptr, act.data(), nb, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(ps->d_maxiter.ptr, &maxiter, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(L0.phi[0].ptr, phi, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(L0.rho.ptr, rho, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+      (e = cudaMemcpy2DAsync(L0.phi[0].ptr, L0.v.s1 * 8, phi, (size_t)L0.v.n[2] * 8, (size_t)L0.v.n[2] * 8,
+                             (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpy2DAsync(L0.rho.ptr, L0.v.s1 * 8, rho, (size_t)L0.v.n[2] * 8, (size_t)L0.v.n[2] * 8,
+                             (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return cuda_fail(e, "poisson setup copies");
   if (precision == 1) {
     // initial residual for the first defect-correction step
@@ -390,7 +398,8 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "V-cycle");
     if (!*ps->h_any) break;
   }
-  if ((e = cudaMemcpyAsync(phi, L0.phi[0].ptr, bytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
+  if ((e = cudaMemcpy2DAsync(phi, (size_t)L0.v.n[2] * 8, L0.phi[0].ptr, L0.v.s1 * 8, (size_t)L0.v.n[2] * 8,
+                             (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(niter, ps->d_niter.ptr, nb * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(error, ps->d_err.ptr, nb * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st)) != cudaSuccess)

@@ -191,14 +191,25 @@ __global__ void __launch_bounds__(GEN_TZ* GEN_TY)
 
 // ------------------------------------------------------------------ star
 // Tile TZ (axis 2) x TY (axis 1); PY consecutive axis-1 rows per thread.
+#ifndef GPW_STAR_TY
+#define GPW_STAR_TY 32
+#endif
+#ifndef GPW_STAR_PY
+#define GPW_STAR_PY 4
+#endif
+#ifndef GPW_STAR_NS
+#define GPW_STAR_NS 3
+#endif
 template <int R, typename T>
 struct StarCfg {
   static constexpr int TZ = 32;
-  static constexpr int PY = (sizeof(T) >= 16) ? 2 : 4;
-  static constexpr int TY = 32;
+  static constexpr int PY = (sizeof(T) >= 16) ? (GPW_STAR_PY > 2 ? 2 : GPW_STAR_PY) : GPW_STAR_PY;
+  static constexpr int TY = GPW_STAR_TY;
   static constexpr int NTY = TY / PY;
+  static constexpr int NT = TZ * NTY;
   static constexpr int H = TY + 2 * R, W = TZ + 2 * R, PS = H * W;
-  static constexpr int NSTAGE = 3;
+  static constexpr int NLD = (PS + NT - 1) / NT;  // plane cells loaded per thread
+  static constexpr int NSTAGE = GPW_STAR_NS;
 };
 
 struct StarCoefs {
@@ -206,35 +217,71 @@ struct StarCoefs {
   double cc;                      // total centre (diagonal) coefficient
 };
 
+// Per-thread plane-load descriptors: the tile position in (axis 1, axis 2) is
+// fixed for the CTA, so each cell's in-plane source offset, validity and
+// wrap sides are computed once; a plane load is then one cp.async per cell.
 template <typename T, int R>
-__device__ __forceinline__ void star_load(T* slot, const T* in, const GridView& v, const Boundary& bc, int p,
-                                          int y0, int x0) {
+struct StarLoader {
   using C = StarCfg<R, T>;
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  constexpr int NT = C::TZ * C::NTY;
-  int j0, s0;
-  const bool ok0 = wrap_axis(p, v.n[0], bc.periodic[0], j0, s0);
-  const T* base = in + (int64_t)j0 * v.s0;
-#pragma unroll 4
-  for (int idx = tid; idx < C::PS; idx += NT) {
-    const int r = idx / C::W, c = idx - r * C::W;
-    int j1, j2, s1, s2;
-    const bool ok = ok0 && wrap_axis(y0 - R + r, v.n[1], bc.periodic[1], j1, s1) &&
-                    wrap_axis(x0 - R + c, v.n[2], bc.periodic[2], j2, s2);
-    const T* src = ok ? base + (int64_t)j1 * v.s1 + j2 : in;
-    cp_async<sizeof(T)>(slot + idx, src, ok);
-  }
-}
+  int off[C::NLD];      // j1 * s1 + j2 (element offset inside a plane)
+  unsigned valid = 0;   // bit k: cell k is inside the grid or a periodic image
+  unsigned char side[C::NLD];  // wrap sides: bits 0-1 axis 1 (+1), bits 2-3 axis 2 (+1)
 
-template <typename T, int R>
-__device__ __forceinline__ void star_fix(T* slot, const GridView& v, const Boundary& bc, int p, int y0,
-                                         int x0) {
-  using C = StarCfg<R, T>;
-  fix_plane<T>(slot, v, bc, p, y0, x0, R, C::H, C::W);
-}
+  __device__ __forceinline__ void init(const GridView& v, const Boundary& bc, int y0, int x0) {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < C::NLD; ++k) {
+      const int idx = tid + k * C::NT;
+      const int r = idx / C::W, c = idx - r * C::W;
+      int j1 = 0, j2 = 0, s1 = -1, s2 = -1;
+      const bool ok = idx < C::PS && wrap_axis(y0 - R + r, v.n[1], bc.periodic[1], j1, s1) &&
+                      wrap_axis(x0 - R + c, v.n[2], bc.periodic[2], j2, s2);
+      off[k] = ok ? (int)((int64_t)j1 * v.s1 + j2) : 0;
+      if (ok) valid |= 1u << k;
+      side[k] = (unsigned char)((s1 + 1) | ((s2 + 1) << 2));
+    }
+  }
+
+  __device__ __forceinline__ void load(T* slot, const T* in, const GridView& v, const Boundary& bc, int p) const {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    int j0, s0;
+    const bool ok0 = wrap_axis(p, v.n[0], bc.periodic[0], j0, s0);
+    const T* base = in + (int64_t)j0 * v.s0;
+#pragma unroll
+    for (int k = 0; k < C::NLD; ++k) {
+      const int idx = tid + k * C::NT;
+      if (C::PS % C::NT == 0 || idx < C::PS) {
+        const bool ok = ok0 && ((valid >> k) & 1u);
+        cp_async<sizeof(T)>(slot + idx, ok ? base + off[k] : in, ok);
+      }
+    }
+  }
+
+  // Bloch phases of the periodic images, axis by axis as the reference's
+  // chained halo copies apply them (each thread fixes its own copies).
+  __device__ __forceinline__ void fix(T* slot, const GridView& v, const Boundary& bc, int p) const {
+    if constexpr (EltTraits<T>::cpx) {
+      const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+      int j0, s0;
+      if (!wrap_axis(p, v.n[0], bc.periodic[0], j0, s0)) return;
+#pragma unroll
+      for (int k = 0; k < C::NLD; ++k) {
+        const int idx = tid + k * C::NT;
+        if (idx >= C::PS || !((valid >> k) & 1u)) continue;
+        const int s1 = (side[k] & 3) - 1, s2 = ((side[k] >> 2) & 3) - 1;
+        if (s0 < 0 && s1 < 0 && s2 < 0) continue;
+        T val = slot[idx];
+        if (s0 >= 0) val = phase_mul(bc.ph[0][s0], val);
+        if (s1 >= 0) val = phase_mul(bc.ph[1][s1], val);
+        if (s2 >= 0) val = phase_mul(bc.ph[2][s2], val);
+        slot[idx] = val;
+      }
+    }
+  }
+};
 
 template <typename T, int R, int MODE>
-__global__ void __launch_bounds__(StarCfg<R, T>::TZ* StarCfg<R, T>::NTY)
+__global__ void __launch_bounds__(StarCfg<R, T>::NT)
     star_stencil_kernel(const StencilArgs a, const StarCoefs k) {
   using C = StarCfg<R, T>;
   using S = typename EltTraits<T>::S;
@@ -256,15 +303,8 @@ __global__ void __launch_bounds__(StarCfg<R, T>::TZ* StarCfg<R, T>::NTY)
   const bool xin = x < a.vout.n[2];
   double sumsq = 0.0;
 
-  // Per-axis coefficients as compile-time-indexed registers.
-  S cx[2 * R + 1], cy[2 * R + 1], cz[2 * R + 1];
-#pragma unroll
-  for (int i = 0; i < 2 * R + 1; ++i) {
-    cx[i] = (S)k.cx[i];
-    cy[i] = (S)k.cy[i];
-    cz[i] = (S)k.cz[i];
-  }
-  const S cc = (MODE == MODE_JACOBI) ? S(0) : (S)k.cc;
+  StarLoader<T, R> ld;
+  ld.init(a.vin, a.bc, y0, x0);
 
   T acc[PY][2 * R + 1];
   T cur[PY][R + 1];  // JACOBI: centre values of the last R+1 planes
@@ -281,14 +321,14 @@ __global__ void __launch_bounds__(StarCfg<R, T>::TZ* StarCfg<R, T>::NTY)
     const int nsteps = plast - pfirst + 1;
 #pragma unroll
     for (int st = 0; st < NS - 1; ++st) {
-      if (st < nsteps) star_load<T, R>(ring + st * PS, in, a.vin, a.bc, pfirst + st, y0, x0);
+      if (st < nsteps) ld.load(ring + st * PS, in, a.vin, a.bc, pfirst + st);
       cp_async_commit();
     }
     for (int s = 0; s < nsteps; ++s) {
       const int p = pfirst + s;
       {
         const int sn = s + NS - 1;
-        if (sn < nsteps) star_load<T, R>(ring + (sn % NS) * PS, in, a.vin, a.bc, pfirst + sn, y0, x0);
+        if (sn < nsteps) ld.load(ring + (sn % NS) * PS, in, a.vin, a.bc, pfirst + sn);
         cp_async_commit();
       }
       // prefetch rho for the output plane that completes at this step
@@ -306,7 +346,7 @@ __global__ void __launch_bounds__(StarCfg<R, T>::TZ* StarCfg<R, T>::NTY)
       }
       cp_async_wait<NS - 1>();
       T* sl = ring + (s % NS) * PS;
-      if (a.bc.use_phase) star_fix<T, R>(sl, a.vin, a.bc, p, y0, x0);
+      if (EltTraits<T>::cpx && a.bc.use_phase) ld.fix(sl, a.vin, a.bc, p);
       __syncthreads();
 
       // column of PY + 2R values along axis 1 at this thread's x
@@ -316,18 +356,19 @@ __global__ void __launch_bounds__(StarCfg<R, T>::TZ* StarCfg<R, T>::NTY)
 #pragma unroll
       for (int j = 0; j < PY; ++j) {
         const T v = col[j + R];
-        // in-plane part: centre + axis-1 + axis-2 neighbours
-        T part = scale(cc, v);
+        // in-plane part: centre + axis-1 + axis-2 neighbours (coefficients
+        // are read from the kernel-parameter bank)
+        T part = scale((MODE == MODE_JACOBI) ? S(0) : (S)k.cc, v);
 #pragma unroll
         for (int q = 1; q <= R; ++q) {
-          part = fmac(cy[R + q], col[j + R + q], part);
-          part = fmac(cy[R - q], col[j + R - q], part);
+          part = fmac((S)k.cy[R + q], col[j + R + q], part);
+          part = fmac((S)k.cy[R - q], col[j + R - q], part);
         }
         const T* row = sl + (yb + j + R) * W + tx + R;
 #pragma unroll
         for (int q = 1; q <= R; ++q) {
-          part = fmac(cz[R + q], row[q], part);
-          part = fmac(cz[R - q], row[-q], part);
+          part = fmac((S)k.cz[R + q], row[q], part);
+          part = fmac((S)k.cz[R - q], row[-q], part);
         }
         // scatter along axis 0: output plane p-R+m receives offset R-m
 #pragma unroll
@@ -335,7 +376,7 @@ __global__ void __launch_bounds__(StarCfg<R, T>::TZ* StarCfg<R, T>::NTY)
           if (m == R)
             acc[j][m] = add(acc[j][m], part);
           else
-            acc[j][m] = fmac(cx[2 * R - m], v, acc[j][m]);
+            acc[j][m] = fmac((S)k.cx[2 * R - m], v, acc[j][m]);
         }
         if constexpr (MODE == MODE_JACOBI) {
 #pragma unroll

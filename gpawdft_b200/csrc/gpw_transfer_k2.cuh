@@ -1,0 +1,160 @@
+// Direct-evaluation restriction and interpolation for K = 2 (nn = 1) on real
+// grids -- the transfers of every multigrid level of the Poisson solver and of
+// the eigensolver preconditioner.
+//
+// The K = 2 operators touch 3 (restriction) or 2 (interpolation) input points
+// per axis, so instead of staging tiles in shared memory each thread reads
+// its few input values straight through L1 and evaluates the three
+// separable 1D passes in the reference's order and expression form
+// (axis 2, then axis 1, then axis 0; c/bmgs/restrict.c:37-39,
+// c/bmgs/interpolate.c:31-33), unfused -- bit-identical to the reference.
+// A thread owns one (axis-1, axis-2) output column and marches along axis 0,
+// carrying the axis-0 partial results of the previous plane.  The in-plane
+// addresses and boundary handling of a column are resolved once per thread
+// (zero boundary: a zero weight on an out-of-grid input; periodic: the
+// wrapped index; real data carries no Bloch phase), so the march itself is
+// loads and arithmetic only.
+#pragma once
+#include <climits>
+
+#include "gpw_common.cuh"
+#include "gpw_transfer.cuh"
+
+namespace gpw {
+
+constexpr int K2_TX = 32, K2_TY = 8;
+
+// 0.5 * (a0 + 0.5 * (a1 + a_1))   (c/bmgs/restrict.c:38-39)
+template <typename S>
+__device__ __forceinline__ S r2(S am, S a0, S ap) {
+  return rmul(S(0.5), radd(a0, rmul(S(0.5), radd(ap, am))));
+}
+// 0.5 * (a0 + a1)                 (c/bmgs/interpolate.c:33)
+template <typename S>
+__device__ __forceinline__ S i2h(S a0, S a1) {
+  return rmul(S(0.5), radd(a0, a1));
+}
+
+// Resolve index i along an axis: element offset (times stride) and a
+// validity flag (false: zero-boundary halo, value 0).
+__device__ __forceinline__ bool k2_axis(int i, int n, int periodic, int64_t stride, int64_t& off) {
+  int j, s;
+  if (!wrap_axis(i, n, periodic, j, s)) {
+    off = 0;
+    return false;
+  }
+  off = (int64_t)j * stride;
+  return true;
+}
+
+template <typename S>
+__device__ __forceinline__ S k2_ld(const S* __restrict__ p, bool ok) {
+  return ok ? __ldg(p) : S(0);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(K2_TX* K2_TY) restrict_k2_kernel(const TransferArgs a) {
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int I2 = blockIdx.x * K2_TX + threadIdx.x, I1 = blockIdx.y * K2_TY + threadIdx.y;
+  if (I1 >= a.vout.n[1] || I2 >= a.vout.n[2]) return;
+  const int I0s = chunk * a.zchunk, I0e = min(a.vout.n[0], I0s + a.zchunk);
+  const S* in = static_cast<const S*>(a.in) + (int64_t)b * a.vin.sb;
+  S* out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)I1 * a.vout.s1 + I2;
+  // fine centres (unpadded): c = 1 + 2 I - pad0; taps c-1, c, c+1
+  const int c1 = 1 + 2 * I1 - a.pad0[1], c2 = 1 + 2 * I2 - a.pad0[2];
+  int64_t off[3][3];  // [axis-1 tap][axis-2 tap] in-plane element offsets
+  bool ok[3][3];
+#pragma unroll
+  for (int d1 = 0; d1 < 3; ++d1) {
+    int64_t o1, o2;
+    const bool v1 = k2_axis(c1 - 1 + d1, a.vin.n[1], a.bc.periodic[1], a.vin.s1, o1);
+#pragma unroll
+    for (int d2 = 0; d2 < 3; ++d2) {
+      const bool v2 = k2_axis(c2 - 1 + d2, a.vin.n[2], a.bc.periodic[2], 1, o2);
+      off[d1][d2] = o1 + o2;
+      ok[d1][d2] = v1 && v2;
+    }
+  }
+  auto Y = [&](int f0) -> S {
+    int64_t o0;
+    const bool v0 = k2_axis(f0, a.vin.n[0], a.bc.periodic[0], a.vin.s0, o0);
+    const S* pl = in + o0;
+    S z[3];
+#pragma unroll
+    for (int d1 = 0; d1 < 3; ++d1)
+      z[d1] = r2(k2_ld(pl + off[d1][0], v0 && ok[d1][0]), k2_ld(pl + off[d1][1], v0 && ok[d1][1]),
+                 k2_ld(pl + off[d1][2], v0 && ok[d1][2]));
+    return r2(z[0], z[1], z[2]);
+  };
+  S ylo = Y(1 + 2 * I0s - a.pad0[0] - 1);
+  for (int I0 = I0s; I0 < I0e; ++I0) {
+    const int c0 = 1 + 2 * I0 - a.pad0[0];
+    const S ym = Y(c0), yp = Y(c0 + 1);
+    out[(int64_t)I0 * a.vout.s0] = r2(ylo, ym, yp);
+    ylo = yp;
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(K2_TX* K2_TY) interpolate_k2_kernel(const TransferArgs a) {
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int o2 = blockIdx.x * K2_TX + threadIdx.x, o1 = blockIdx.y * K2_TY + threadIdx.y;
+  if (o1 >= a.vout.n[1] || o2 >= a.vout.n[2]) return;
+  const int O0s = chunk * a.zchunk, O0e = min(a.vout.n[0], O0s + a.zchunk);
+  const S* in = static_cast<const S*>(a.in) + (int64_t)b * a.vin.sb;
+  S* out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)o1 * a.vout.s1 + o2;
+  const S* base = a.subtract ? static_cast<const S*>(a.base) + (int64_t)b * a.vbase.sb + (int64_t)o1 * a.vbase.s1 + o2
+                             : nullptr;
+  // per axis: o + skip0 = 2 i + e; coarse (unpadded) index u = i - pad0
+  const int t1 = o1 + a.skip0[1], t2 = o2 + a.skip0[2];
+  const int u1 = (t1 >> 1) - a.pad0[1], e1 = t1 & 1;
+  const int u2 = (t2 >> 1) - a.pad0[2], e2 = t2 & 1;
+  int64_t off[2][2];
+  bool ok[2][2];
+#pragma unroll
+  for (int d1 = 0; d1 < 2; ++d1) {
+    int64_t q1, q2;
+    const bool v1 = k2_axis(u1 + d1, a.vin.n[1], a.bc.periodic[1], a.vin.s1, q1);
+#pragma unroll
+    for (int d2 = 0; d2 < 2; ++d2) {
+      const bool v2 = k2_axis(u2 + d2, a.vin.n[2], a.bc.periodic[2], 1, q2);
+      off[d1][d2] = q1 + q2;
+      ok[d1][d2] = v1 && v2;
+    }
+  }
+  auto Y = [&](int u0) -> S {
+    int64_t q0;
+    const bool v0 = k2_axis(u0, a.vin.n[0], a.bc.periodic[0], a.vin.s0, q0);
+    const S* pl = in + q0;
+    S z0 = k2_ld(pl + off[0][0], v0 && ok[0][0]);
+    if (e2) z0 = i2h(z0, k2_ld(pl + off[0][1], v0 && ok[0][1]));
+    if (!e1) return z0;
+    S z1 = k2_ld(pl + off[1][0], v0 && ok[1][0]);
+    if (e2) z1 = i2h(z1, k2_ld(pl + off[1][1], v0 && ok[1][1]));
+    return i2h(z0, z1);
+  };
+  // march over fine planes; two consecutive outputs share a coarse plane
+  int ucur = INT_MIN;
+  S ya = S(0), yb = S(0);  // Y(ucur), Y(ucur + 1)
+  for (int o0 = O0s; o0 < O0e; ++o0) {
+    const int t0 = o0 + a.skip0[0];
+    const int u0 = (t0 >> 1) - a.pad0[0], e0 = t0 & 1;
+    if (u0 != ucur) {
+      if (u0 == ucur + 1) {
+        ya = yb;
+        yb = Y(u0 + 1);
+      } else {
+        ya = Y(u0);
+        yb = Y(u0 + 1);
+      }
+      ucur = u0;
+    }
+    const S val = e0 ? i2h(ya, yb) : ya;
+    S* dst = out + (int64_t)o0 * a.vout.s0;
+    *dst = a.subtract ? base[(int64_t)o0 * a.vbase.s0] - val : val;
+  }
+}
+
+}  // namespace gpw

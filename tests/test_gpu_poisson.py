@@ -124,7 +124,7 @@ def test_batch_equals_single(cuda):
     nb = ps.solve_batch(phib, np.array(rhos), eps=2e-10)
     for s in range(3):
         phi = gd.zeros()
-        n = ps.solve_neutral(phi, rhos[s] - rhos[s].mean(), eps=2e-10)
+        n = ps.solve_neutral(phi, rhos[s], eps=2e-10)
         assert n == nb[s]
         assert np.array_equal(phi, phib[s])
 
