@@ -58,6 +58,23 @@ def eps_for(rho, dv):
     return REL_TOL ** 2 * float(np.dot(rho.ravel(), rho.ravel())) * dv
 
 
+# ------------------------------------------------------------------ sharding
+# The path shards by independent solves: each rank solves its own batch of
+# densities (seeds disjoint across ranks, up to 1000 solves per rank) with no
+# data exchange; the only collective is the max over ranks of the timings.
+def shard_seed0(rank):
+    return 1 + 1000 * rank
+
+
+def reduce_max(x, dist, device):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi clock / throttle-reason samples during the timed region."""
@@ -201,7 +218,7 @@ def run_ours(args, rank, world, dist):
     dev = torch.device('cuda', int(os.environ.get('LOCAL_RANK', 0)))
     torch.cuda.set_device(dev)
     B = args.batch
-    rho_h, L = densities(B, 1 + 1000 * rank)
+    rho_h, L = densities(B, shard_seed0(rank))
     gd = GridDescriptor((N_GRID,) * 3, (L,) * 3, 0)
     eps = [eps_for(r, gd.dv) for r in rho_h]
     ps = PoissonSolver(nn=3, relax='J', maxiter=1000, precision=args.precision,
@@ -221,11 +238,7 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, dev)
 
     def stats():
         import ctypes
