@@ -74,10 +74,18 @@ static cudaError_t run_general(const StencilArgs& a0, const OpDesc& d, int nbatc
   const size_t smem = (size_t)(2 * mp + 2) * (GEN_TY + 2 * mp) * (GEN_TZ + 2 * mp) * sizeof(T);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   auto kern = general_stencil_kernel<T, MODE>;
-  static std::once_flag once;
-  cudaError_t e = cudaSuccess;
-  std::call_once(once, [&] { e = smem_optin(kern, 227 * 1024); });
-  if (e != cudaSuccess) return e;
+  // opt in to exactly the dynamic shared memory needed (the largest so far):
+  // the static part of the kernel counts against the same per-CTA limit
+  static std::mutex mu;
+  static size_t opted = 48 * 1024;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (smem > opted) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      opted = smem;
+    }
+  }
   kern<<<grid, dim3(GEN_TZ, GEN_TY), smem, st>>>(a, d.gc);
   return cudaGetLastError();
 }

@@ -192,6 +192,26 @@ def test_float32_relax(cuda):
     assert relerr(g, r) < 2e-6
 
 
+def test_residual_general_stencil(cuda):
+    """Residual epilogue on the general-offset kernel (GUC fcc, periodic)."""
+    import torch
+    from gpawdft_b200.fd_operators import Laplace
+    cell = [(0, 1.7, 1.7), (1.7, 0, 1.7), (1.7, 1.7, 0)]
+    gd, ogd = gds((10, 10, 10), cell, 1)
+    f = rand((2,) + tuple(gd.n_c), np.float64, 14)
+    s = rand((2,) + tuple(gd.n_c), np.float64, 15)
+    op = Laplace(gd, 1.0, 2)
+    assert not op.cfd
+    r = torch.empty(f.shape, dtype=torch.float64, device='cuda')
+    ss = op.residual(torch.from_numpy(f).cuda(), torch.from_numpy(s).cuda(), r)
+    ref = np.zeros_like(f)
+    ol.Laplace(ogd, 1.0, 2).apply(f, ref)
+    ref -= s
+    assert np.array_equal(r.cpu().numpy(), ref)
+    assert np.allclose(ss.cpu().numpy(), (ref.reshape(2, -1) ** 2).sum(1),
+                       rtol=1e-12)
+
+
 def test_residual_and_norm(cuda):
     import torch
     from gpawdft_b200.fd_operators import Laplace
