@@ -25,7 +25,7 @@ EXPORTS = [
     'gpw_last_error', 'gpw_version',
     'gpw_operator_new', 'gpw_operator_apply', 'gpw_operator_relax',
     'gpw_operator_get_diagonal_element', 'gpw_operator_residual',
-    'gpw_operator_free',
+    'gpw_operator_residual_noalloc', 'gpw_operator_free',
     'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
     'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_add_scalar',
     'gpw_poisson_new', 'gpw_poisson_solve', 'gpw_poisson_last_stats',
@@ -51,6 +51,9 @@ _SIGS = {
     'gpw_operator_get_diagonal_element': (ctypes.c_int, [_vp, _c_dp]),
     'gpw_operator_residual': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp,
                                              ctypes.c_int64, _vp, _vp]),
+    'gpw_operator_residual_noalloc': (ctypes.c_int, [_vp, ctypes.c_int, _vp,
+                                                     _vp, _vp, ctypes.c_int64,
+                                                     _vp, _vp]),
     'gpw_operator_free': (None, [_vp]),
     'gpw_transformer_new': (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp,
                                            _vp, _vp, ctypes.c_int,

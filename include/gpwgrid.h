@@ -109,6 +109,21 @@ int gpw_operator_residual(gpw_operator *op, int dtype, const void *func,
                           const void *source, void *r, int64_t nin,
                           double *sumsq_dev, gpw_stream stream);
 
+/* Allocation-free gpw_operator_residual (no counterpart in the reference).
+ * For callers that must not allocate device memory during a call -- code
+ * running inside another framework's memory pool or allocator hook, or a
+ * process that reserves all device memory up front: the partial sums of the
+ * norm reduction live in a fixed ~272 KB array compiled into the library
+ * (resident on every GPU that loads it until exit) instead of a workspace
+ * grown with cudaMalloc.  Same arguments and results as
+ * gpw_operator_residual.  Limits: nin <= 4096 grids and at most 65536
+ * reduction blocks per call (blocks x nin), else GPW_EINVAL.  The first call
+ * on a device looks the array's address up (keep that call outside stream
+ * capture).  Calls share the array: calls that overlap on the GPU race.     */
+int gpw_operator_residual_noalloc(gpw_operator *op, int dtype, const void *func,
+                                  const void *source, void *r, int64_t nin,
+                                  double *sumsq_dev, gpw_stream stream);
+
 void gpw_operator_free(gpw_operator *op);
 
 /* ------------------------------------------------------------ transformer */
