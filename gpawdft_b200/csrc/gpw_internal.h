@@ -86,6 +86,16 @@ cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in,
                            const Boundary& bc, double w, const unsigned char* active, const GridSum& gs,
                            cudaStream_t st);
 
+// Fused defect-correction steps (TMA kernel; zero boundaries, 16-byte-pitched
+// engine buffers).  mode MODE_RESID_DC: in/rho float64, out (rhs) and out2
+// (first inner iterate) float32.  mode MODE_JACOBI_ADD64: in/rho float32,
+// out2 = float64 phi that receives the sweep's result.  Returns
+// cudaErrorNotSupported when the TMA path does not apply.
+bool dc_fusable(const OpDesc& d);
+cudaError_t launch_stencil_dc(const OpDesc& d, int mode, const void* in, const GridView& v, void* out, void* out2,
+                              const void* rho, int nbatch, double w, double w2, const unsigned char* active,
+                              const GridSum& gs, cudaStream_t st);
+
 // ---------------------------------------------------------------- transformer
 struct TrDesc {
   int nin[3], nout[3];

@@ -293,6 +293,35 @@ cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in,
   return cudaErrorInvalidValue;
 }
 
+bool dc_fusable(const OpDesc& d) {
+  return !d.periodic[0] && !d.periodic[1] && !d.periodic[2] && d.star_jacobi && star_radius_ok(d.R) &&
+         tensor_map_encoder() != nullptr;
+}
+
+cudaError_t launch_stencil_dc(const OpDesc& d, int mode, const void* in, const GridView& v, void* out, void* out2,
+                              const void* rho, int nbatch, double w, double w2, const unsigned char* active,
+                              const GridSum& gs, cudaStream_t st) {
+  if (!dc_fusable(d)) return cudaErrorNotSupported;
+  const size_t es_in = (mode == MODE_RESID_DC) ? 8 : 4;
+  if (!aligned16(in) || !aligned16(rho) || !aligned16(out2) || (out && !aligned16(out)) ||
+      !view_tma_ok(v, es_in, nbatch) || !view_tma_ok(v, 4, nbatch))
+    return cudaErrorNotSupported;
+  StencilArgs a{};
+  a.in = in;
+  a.out = out;
+  a.out2 = out2;
+  a.rho = rho;
+  a.vin = a.vout = a.vrho = v;
+  a.w = w;
+  a.w2 = w2;
+  a.c0 = d.coefs[0];
+  a.active = active;
+  a.gsum = gs;
+  if (mode == MODE_RESID_DC) return dispatch_star_tma<double, MODE_RESID_DC>(a, d, nbatch, st);
+  if (mode == MODE_JACOBI_ADD64) return dispatch_star_tma<float, MODE_JACOBI_ADD64>(a, d, nbatch, st);
+  return cudaErrorInvalidValue;
+}
+
 // ------------------------------------------------------------------ transfers
 template <typename T, int K>
 static cudaError_t run_restrict(TransferArgs a, int nbatch, cudaStream_t st) {

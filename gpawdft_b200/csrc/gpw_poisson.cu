@@ -284,6 +284,13 @@ static int ensure_f32(gpw_poisson* ps) {
 
 // Record one outer iteration (one V-cycle, or one defect-correction step)
 // plus the convergence update for batch size nb.
+// The fused float32 defect-correction iteration applies to zero-boundary star
+// Laplacians with at least one pre- and one post-sweep on level 0.
+static bool fused_dc(const gpw_poisson* ps) {
+  const Level& L0 = ps->lv[0];
+  return ps->relax_method == 2 && ps->lv.size() >= 2 && L0.pre >= 1 && L0.post >= 1 && dc_fusable(*L0.op);
+}
+
 static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, int maxiter_unused, cudaStream_t st) {
   (void)maxiter_unused;
   Rec r{ps, nb, st, (const unsigned char*)ps->d_active.ptr};
@@ -296,6 +303,37 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, int maxit
   if (prec == 0) {
     const int cur = rec_vcycle(r, 0, 0, false);
     if (cur != 0) r.ok(cudaMemcpyAsync(L0.phi[0].ptr, L0.phi[1].ptr, n * 8, cudaMemcpyDeviceToDevice, st));
+  } else if (fused_dc(ps)) {
+    // Fused defect correction.  On entry L0.rho32 holds rhs = -(A phi - rho)
+    // and L0.phi32[0] the first level-0 sweep from zero (both written by the
+    // previous MODE_RESID_DC launch).  Finish the float32 V-cycle; its last
+    // level-0 post-sweep adds e into float64 phi; then the fused residual
+    // writes the next rhs / first sweep and the norm.
+    Level& C = ps->lv[1];
+    int cur = rec_relax(r, 0, 0, L0.pre - 1, true);
+    Boundary bc32 = make_boundary(L0.op->periodic, GPW_F32, nullptr);
+    r.ok(launch_stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[cur].ptr, L0.v, L0.res32.ptr, L0.v, L0.rho32.ptr,
+                        L0.v, nb, bc32, 1.0, r.active, ps->sums.gs(), st));
+    r.ok(launch_transfer(*L0.restr, GPW_F32, L0.res32.ptr, L0.v, C.rho32.ptr, C.v, nb, bc32, 0, nullptr, nullptr,
+                         r.active, st));
+    r.ok(launch_zero(GPW_F32, C.v, C.phi32[0].ptr, nb, r.active, st));
+    const int ccur = rec_vcycle(r, 1, 0, true);
+    Boundary cbc = make_boundary(C.op->periodic, GPW_F32, nullptr);
+    r.ok(launch_transfer(*L0.interp, GPW_F32, C.phi32[ccur].ptr, C.v, L0.phi32[1 - cur].ptr, L0.v, nb, cbc, 1,
+                         L0.phi32[cur].ptr, &L0.v, r.active, st));
+    cur = 1 - cur;
+    cur = rec_relax(r, 0, cur, L0.post - 1, true);
+    GridSum none{};
+    r.ok(launch_stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[cur].ptr, L0.v, nullptr, L0.phi[0].ptr,
+                           L0.rho32.ptr, nb, L0.w, 0.0, r.active, none, st));
+    r.ok(launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr,
+                           nb, 1.0, L0.w, r.active, ps->sums.gs(), st));
+    converge_update_kernel<<<1, 256, 0, st>>>(nb, ps->sums.gs().result, ps->dv, (const double*)ps->d_eps.ptr,
+                                              (const int*)ps->d_maxiter.ptr, (double*)ps->d_err.ptr,
+                                              (int*)ps->d_niter.ptr, (unsigned char*)ps->d_active.ptr,
+                                              (int*)ps->d_any.ptr);
+    r.ok(cudaGetLastError());
+    return r.err;
   } else {
     // defect correction: rhs32 = -(A phi - rho) (residual computed at the end
     // of the previous iteration into d_r64), e = FP32 V-cycle(rhs32), phi += e
@@ -345,7 +383,12 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
       (e = cudaMemcpy2DAsync(L0.rho.ptr, L0.v.s1 * 8, rho, (size_t)L0.v.n[2] * 8, (size_t)L0.v.n[2] * 8,
                              (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return cuda_fail(e, "poisson setup copies");
-  if (precision == 1) {
+  if (precision == 1 && fused_dc(ps)) {
+    // initial defect: float32 rhs and first level-0 sweep, fused
+    e = launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr, nb,
+                          1.0, L0.w, (const unsigned char*)ps->d_active.ptr, ps->sums.gs(), st);
+    if (e != cudaSuccess) return cuda_fail(e, "poisson initial defect");
+  } else if (precision == 1) {
     // initial residual for the first defect-correction step
     Boundary bc = make_boundary(L0.op->periodic, GPW_F64, nullptr);
     e = launch_stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, L0.v, ps->d_r64.ptr, L0.v, L0.rho.ptr, L0.v, nb,

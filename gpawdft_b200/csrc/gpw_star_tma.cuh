@@ -196,8 +196,9 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
           const V c = col[j + R];
           nb[C::XL] = c.x;
           nb[C::XL + 1] = c.y;
-          S p0 = (MODE == MODE_JACOBI) ? S(0) : (S)k.cc * c.x;
-          S p1 = (MODE == MODE_JACOBI) ? S(0) : (S)k.cc * c.y;
+          constexpr bool sweep = (MODE == MODE_JACOBI || MODE == MODE_JACOBI_ADD64);
+          S p0 = sweep ? S(0) : (S)k.cc * c.x;
+          S p1 = sweep ? S(0) : (S)k.cc * c.y;
 #pragma unroll
           for (int q = 1; q <= R; ++q) {
             p0 = fma((S)k.cy[R + q], col[j + R + q].x, p0);
@@ -231,9 +232,11 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
             if (y < a.vout.n[1] && xin0) {
               V av = acc[j][ph];
               V res;
+              const int64_t oidx =
+                  (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
               if constexpr (MODE == MODE_APPLY) {
                 res = av;
-              } else if constexpr (MODE == MODE_RESIDUAL) {
+              } else if constexpr (MODE == MODE_RESIDUAL || MODE == MODE_RESID_DC) {
                 res.x = av.x - rho[j].x;
                 res.y = av.y - rho[j].y;
                 sumsq += (double)res.x * res.x + (xin1 ? (double)res.y * res.y : 0.0);
@@ -243,7 +246,32 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
                 res.x = (S(1) - w) * cur.x + wc * (rho[j].x - av.x);
                 res.y = (S(1) - w) * cur.y + wc * (rho[j].y - av.y);
               }
-              if (MODE != MODE_RESIDUAL || a.out) {
+              if constexpr (MODE == MODE_RESID_DC) {
+                // float32 defect and first inner Jacobi iterate from zero
+                const float2 rhs = make_float2((float)(-res.x), (float)(-res.y));
+                const float wc = (float)a.w2 / (float)a.c0;
+                const float2 e1 = make_float2(wc * rhs.x, wc * rhs.y);
+                float* rp = static_cast<float*>(a.out) + oidx;
+                float* ep = static_cast<float*>(a.out2) + oidx;
+                if (xin1) {
+                  *reinterpret_cast<float2*>(rp) = rhs;
+                  *reinterpret_cast<float2*>(ep) = e1;
+                } else {
+                  rp[0] = rhs.x;
+                  ep[0] = e1.x;
+                }
+              } else if constexpr (MODE == MODE_JACOBI_ADD64) {
+                // phi64 += e (the inner correction), e never stored
+                double* pp = static_cast<double*>(a.out2) + oidx;
+                if (xin1) {
+                  double2 pv = *reinterpret_cast<double2*>(pp);
+                  pv.x += (double)res.x;
+                  pv.y += (double)res.y;
+                  *reinterpret_cast<double2*>(pp) = pv;
+                } else {
+                  pp[0] += (double)res.x;
+                }
+              } else if (MODE != MODE_RESIDUAL || a.out) {
                 S* op = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 +
                         (int64_t)y * a.vout.s1 + x;
                 if (xin1)
@@ -267,7 +295,7 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
     }
   }
   if (timed_out && ta.status) atomicExch(ta.status, GPW_ETIMEDOUT);
-  if constexpr (MODE == MODE_RESIDUAL) {
+  if constexpr (MODE == MODE_RESIDUAL || MODE == MODE_RESID_DC) {
     double tot = block_sum(sumsq, red);
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
     grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);

@@ -30,7 +30,13 @@
 
 namespace gpw {
 
-enum StencilMode { MODE_APPLY = 0, MODE_RESIDUAL = 1, MODE_JACOBI = 2 };
+// MODE_RESID_DC and MODE_JACOBI_ADD64 are the fused steps of the float32
+// defect-correction form (TMA kernel only): RESID_DC reads float64 phi / rho
+// and writes the float32 defect rhs = -(A phi - rho) to `out` and the first
+// inner Jacobi iterate from zero, (w2 / c0) rhs, to `out2`, plus sum r^2;
+// JACOBI_ADD64 is a float32 Jacobi sweep whose result is added to the float64
+// array `out2` (phi += e) instead of being stored.
+enum StencilMode { MODE_APPLY = 0, MODE_RESIDUAL = 1, MODE_JACOBI = 2, MODE_RESID_DC = 3, MODE_JACOBI_ADD64 = 4 };
 
 constexpr int PMAX = 80;  // GUC n<=6 with 6 directions needs 73
 
@@ -47,6 +53,8 @@ struct StencilArgs {
   const unsigned char* active;  // optional per-batch-member mask (null: all)
   GridSum gsum;     // RESIDUAL: per-batch-member segmented sum
   int nblk_seg;     // CTAs per batch member
+  void* out2;       // RESID_DC: first inner iterate (float); JACOBI_ADD64: float64 phi
+  double w2;        // RESID_DC: Jacobi weight of that first inner sweep
 };
 
 struct GeneralCoefs {
