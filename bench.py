@@ -58,6 +58,15 @@ def eps_for(rho, dv):
     return REL_TOL ** 2 * float(np.dot(rho.ravel(), rho.ravel())) * dv
 
 
+def _plain(o):
+    """JSON fallback for ctypes / NumPy scalars."""
+    if hasattr(o, 'value'):
+        return o.value
+    if isinstance(o, np.generic):
+        return o.item()
+    raise TypeError(type(o).__name__)
+
+
 # ------------------------------------------------------------------ sharding
 # The path shards by independent solves: each rank solves its own batch of
 # densities (seeds disjoint across ranks, up to 1000 solves per rank) with no
@@ -287,23 +296,53 @@ def run_ours(args, rank, world, dist):
     e2e = world * B * args.steps / t_e2e
     nbytes = rho_h.nbytes
 
-    # ---- dominant kernel: level-0 weighted-Jacobi sweep over the batch
-    op = ps.operators[0]
-    npts = int(np.prod(gd.n_c))
-    reps = 10
-    op.relax(2, phi_d, rho_d, 2, 2.0 / 3.0)
-    torch.cuda.synchronize()
-    k0 = torch.cuda.Event(enable_timing=True)
-    k1 = torch.cuda.Event(enable_timing=True)
-    k0.record(stream)
-    for _ in range(reps):
-        op.relax(2, phi_d, rho_d, 2, 2.0 / 3.0)
-    k1.record(stream)
-    torch.cuda.synchronize()
-    t_sweep = k0.elapsed_time(k1) / 1000.0 / (2 * reps)
-    sweep_bytes = 3 * 8 * npts * B
+    # ---- dominant kernels, timed live on the engine's stream and buffers:
+    # float64 form: the level-0 Jacobi sweep; float32 form: the fused
+    # level-0 float32 sweep that adds its result into float64 phi
+    import ctypes
+    kernels = {}
+    names = {0: 'star_tma_kernel<double,3,JACOBI> level-0 sweep',
+             1: 'star_tma_kernel<double,3,RESIDUAL> level-0 residual+norm',
+             2: 'star_tma_kernel<float,3,JACOBI> level-0 sweep',
+             3: 'star_tma_kernel<float,3,JACOBI_ADD64> level-0 sweep + phi64 update',
+             4: 'star_tma_kernel<double,3,RESID_DC> level-0 fp64 defect'}
+    for which in ((0, 1) if args.precision == 'fp64' else (3, 4, 2)):
+        ms, nbytes = ctypes.c_double(), ctypes.c_double()
+        _lib.check(lib.gpw_poisson_time_level0(
+            ps._engine[0], B, which, 20, ctypes.byref(ms), ctypes.byref(nbytes),
+            stream.cuda_stream))
+        kernels[which] = (ms.value / 1e3, nbytes.value)
+    dom = 0 if args.precision == 'fp64' else 3
+    t_sweep, sweep_bytes = kernels[dom]
     achieved = sweep_bytes / t_sweep / 1e9
     peak, peak_src = measured_peak()
+    kernel_table = {names[w]: {'ms': t * 1e3, 'GB/s': b / t / 1e9,
+                               'frac': b / t / 1e9 / peak}
+                    for w, (t, b) in kernels.items()}
+
+    # ---- the plain float64 method on the same batch, for the ratio
+    fp64_plain = None
+    if args.precision == 'fp32':
+        ps64 = PoissonSolver(nn=3, relax='J', maxiter=1000, precision='fp64',
+                             batch=B)
+        ps64.set_grid_descriptor(gd)
+        ps64.initialize()
+        for _ in range(2):
+            phi_d.zero_()
+            ps64.solve_batch(phi_d, rho_d, eps=eps)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            phi_d.zero_()
+            n64 = ps64.solve_batch(phi_d, rho_d, eps=eps)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        t64 = max_over_ranks(g0.elapsed_time(g1) / 1000.0)
+        fp64_plain = {'value': world * B * args.steps / t64,
+                      'unit': 'solves/s', 'vcycles_mean': float(np.mean(n64))}
+        del ps64
 
     # ---- secondary: config (a) Laplace apply, 32 x 48^3 float64, zero BC
     stencil = stencil_config_a(dev, stream)
@@ -321,11 +360,12 @@ def run_ours(args, rank, world, dist):
            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                         'unit': 'GB/s', 'frac': achieved / peak,
                         'traffic': None,
-                        'kernel': 'star_stencil_kernel<double,3,JACOBI> '
-                                  '(level-0 sweep, batch %d)' % B,
+                        'kernel': names[dom] + ' (batch %d)' % B,
                         'algorithmic_bytes_per_launch': sweep_bytes,
                         'launch_ms': t_sweep * 1e3,
-                        'peak_source': peak_src},
+                        'peak_source': peak_src,
+                        'level0_kernels': kernel_table},
+           'fp64_plain': fp64_plain,
            'gpu_launches': int(launches),
            'clocks': clocks,
            'vcycles': [int(x) for x in niters],
@@ -336,7 +376,7 @@ def run_ours(args, rank, world, dist):
                                'unit': 'solves/s', 'cores': r['cores'],
                                'kind': r['kind'], 'sample': r['sample']}
     if rank == 0:
-        print(json.dumps(out), flush=True)
+        print(json.dumps(out, default=_plain), flush=True)
 
 
 def measured_peak():
@@ -382,6 +422,212 @@ def stencil_config_a(dev, stream):
     return res
 
 
+# ------------------------------------------------------------------ other configs
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_mixed192(args):
+    """Mixed precision: one 191^3 solve (N_c=192, h=0.15 A, 64 Gaussians with
+    log-uniform widths 0.3-2.0 A and N(0,1) charges re-centred to neutral,
+    seed 4) to relative residual 1e-10: float32 V-cycles inside float64
+    defect correction vs the plain float64 method (same schedule); E_H error
+    of the float32 form against the float64 result."""
+    import torch
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    from gpawdft_b200.workloads import gaussian_density
+    N = 192
+    rho, L = gaussian_density(N, 0.15, 64, 4, sigma_range=(0.3, 2.0),
+                              log_sigma=True, charges='normal')
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    eps = eps_for(rho, gd.dv)
+    rho_d = torch.from_numpy(rho).cuda()
+    res = {}
+    for prec in ('fp64', 'fp32'):
+        ps = PoissonSolver(nn=3, relax='J', maxiter=1000, precision=prec)
+        ps.set_grid_descriptor(gd)
+        ps.initialize()
+        phi = torch.zeros_like(rho_d)
+        for _ in range(max(1, args.warmup)):
+            phi.zero_()
+            ps.solve_batch(phi.unsqueeze(0), rho_d.unsqueeze(0), eps=eps)
+        ts = []
+        for _ in range(args.steps):
+            phi.zero_()
+            e0, e1 = _events()
+            e0.record()
+            n = ps.solve_batch(phi.unsqueeze(0), rho_d.unsqueeze(0), eps=eps)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        ph = phi.cpu().numpy()
+        res[prec] = {'time_s': float(np.median(ts)), 'vcycles': int(n[0]),
+                     'E_H': 0.5 * gd.dv * float(np.dot(ph.ravel(), rho.ravel())),
+                     'final_error': float(ps.last_errors[0])}
+    line = {'metric': 'poisson_time_to_solution_191^3_rel1e-10',
+            'value': res['fp32']['time_s'], 'unit': 's',
+            'higher_is_better': False, 'n_gpus': 1, 'steps': args.steps,
+            'warmup': args.warmup, 'dtype': 'f32+f64', 'data': 'synthetic',
+            'config': {'workload': 'mixed-precision Poisson, N_c=192 zero '
+                                   'boundary (191^3), h=0.15 A, 64 Gaussians'},
+            'fp64_plain': res['fp64'], 'fp32_dc': res['fp32'],
+            'E_H_error_Ha': abs(res['fp32']['E_H'] - res['fp64']['E_H']),
+            'speedup_vs_fp64': res['fp64']['time_s'] / res['fp32']['time_s']}
+    print(json.dumps(line), flush=True)
+
+
+def run_uneven(args):
+    """512 independent solves, cubic N_c log-uniform in [32, 128] rounded to
+    multiples of 8 (seed 5), each density 4-32 neutral Gaussians (h = 0.2 A),
+    relative residual 1e-10, float32 inner / float64 outer.  Solves of one
+    size form one batched engine (one captured graph per iteration); the size
+    groups run concurrently on separate streams.  Reports solves/s and p50/p99
+    per-solve latency (completion of its group, from the common start)."""
+    import threading
+    import torch
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    from gpawdft_b200.workloads import gaussian_density
+    rng = np.random.default_rng(5)
+    NS = 512
+    Ns = np.exp(rng.uniform(np.log(32), np.log(128), NS))
+    Ns = (np.round(Ns / 8) * 8).astype(int)
+    ngs = rng.integers(4, 33, NS)
+    groups = {}
+    for i, (N, ng) in enumerate(zip(Ns, ngs)):
+        groups.setdefault(int(N), []).append((i, int(ng)))
+    work = []
+    for N, members in sorted(groups.items()):
+        rhos, L = [], None
+        for i, ng in members:
+            r, L = gaussian_density(N, 0.2, ng, 5000 + i)
+            rhos.append(r)
+        gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+        eps = [eps_for(r, gd.dv) for r in rhos]
+        ps = PoissonSolver(nn=3, relax='J', maxiter=1000, precision='fp32',
+                           batch=len(rhos))
+        ps.set_grid_descriptor(gd)
+        ps.initialize()
+        rho_d = torch.from_numpy(np.array(rhos)).cuda()
+        work.append(dict(N=N, n=len(rhos), ps=ps, rho=rho_d, eps=eps,
+                         phi=torch.zeros_like(rho_d),
+                         stream=torch.cuda.Stream()))
+
+    def run_all(record):
+        start = torch.cuda.Event(enable_timing=True)
+        start.record()
+        ends = []
+
+        def worker(w):
+            with torch.cuda.stream(w['stream']):
+                w['stream'].wait_event(start)
+                w['phi'].zero_()
+                w['niter'] = w['ps'].solve_batch(w['phi'], w['rho'],
+                                                 eps=w['eps'])
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record()
+                w['end'] = ev
+        ths = [threading.Thread(target=worker, args=(w,)) for w in work]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        torch.cuda.synchronize()
+        lat = []
+        for w in work:
+            t = start.elapsed_time(w['end']) / 1e3
+            lat.extend([t] * w['n'])
+        return max(lat), lat
+
+    for _ in range(max(1, args.warmup)):
+        run_all(False)
+    tots, lats = [], []
+    for _ in range(args.steps):
+        t, lat = run_all(True)
+        tots.append(t)
+        lats.extend(lat)
+    T = float(np.median(tots))
+    line = {'metric': 'batched_uneven_poisson_solves_per_s', 'value': NS / T,
+            'unit': 'solves/s', 'higher_is_better': True, 'n_gpus': 1,
+            'steps': args.steps, 'warmup': args.warmup, 'dtype': 'f32+f64',
+            'data': 'synthetic',
+            'config': {'workload': '512 solves, N_c log-uniform 32-128 (x8), '
+                                   '4-32 Gaussians, rel 1e-10, fp32 inner',
+                       'sizes': {str(w['N']): w['n'] for w in work}},
+            'p50_latency_s': float(np.percentile(lats, 50)),
+            'p99_latency_s': float(np.percentile(lats, 99)),
+            'ms_per_step': 1e3 * T,
+            'vcycles_mean': float(np.mean(np.concatenate(
+                [w['niter'] for w in work])))}
+    print(json.dumps(line), flush=True)
+
+
+def run_bands(args):
+    """256 complex Bloch bands on a 96^3 periodic grid (h = 0.18 A, random k,
+    phase-wrapped halos): Laplace nn=3 (scale -1/2), Gradient x/y/z n=3,
+    restriction / interpolation nn=3 96^3 <-> 48^3, complex128 and complex64.
+    GB/s of algorithmic bytes (input read once + output written once)."""
+    import torch
+    from gpawdft_b200.fd_operators import Gradient, Laplace
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.transformers import Transformer
+    h = 0.18 / 0.52917721
+    gd = GridDescriptor((96,) * 3, (96 * h,) * 3, 1)
+    gc = gd.coarsen()
+    k = np.random.default_rng(2).uniform(-0.5, 0.5, 3)
+    ph = np.exp(2j * np.pi * gd.sdisp_cd * k[:, None])
+    peak, _ = measured_peak()
+    NB = args.batch if args.batch != 16 else 256
+    res = {}
+
+    def timeit(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    for dt, tdt in ((complex, torch.complex128), (np.complex64, torch.complex64)):
+        g = torch.Generator(device='cuda').manual_seed(3)
+        a = torch.randn((NB, 96, 96, 96), dtype=tdt, device='cuda', generator=g)
+        o = torch.empty_like(a)
+        es = a.element_size()
+        name = 'c128' if tdt == torch.complex128 else 'c64'
+        ops = [('laplace', Laplace(gd, -0.5, 3, dt))] + \
+            [('grad%s' % 'xyz'[v], Gradient(gd, v, 1.0, 3, dt)) for v in range(3)]
+        for nm, op in ops:
+            t = timeit(lambda: op.apply(a, o, ph), args.steps)
+            gbs = 2 * a.numel() * es / t / 1e9
+            res['%s_%s' % (name, nm)] = {'ms': t * 1e3, 'GB/s': gbs,
+                                         'frac': gbs / peak}
+        del o
+        R = Transformer(gd, gc, 3, dt)
+        Ip = Transformer(gc, gd, 3, dt)
+        c = R.apply(a, None, ph)
+        for nm, fn in (('restrict', lambda: R.apply(a, c, ph)),
+                       ('interpolate', lambda: Ip.apply(c, a, ph))):
+            t = timeit(fn, args.steps)
+            gbs = (a.numel() + c.numel()) * es / t / 1e9
+            res['%s_%s' % (name, nm)] = {'ms': t * 1e3, 'GB/s': gbs,
+                                         'frac': gbs / peak}
+        del a, c
+        torch.cuda.empty_cache()
+    line = {'metric': 'band_stencil_GBps_256x96^3_bloch', 'value':
+            res['c128_laplace']['GB/s'], 'unit': 'GB/s',
+            'higher_is_better': True, 'n_gpus': 1, 'steps': args.steps,
+            'dtype': 'c128', 'data': 'synthetic', 'peak_GBps': peak,
+            'config': {'workload': '%d complex Bloch bands, 96^3 periodic' % NB},
+            'ops': res}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -389,10 +635,16 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--batch', type=int, default=16)
-    ap.add_argument('--precision', default='fp64', choices=['fp64', 'fp32'])
+    ap.add_argument('--precision', default='fp32', choices=['fp64', 'fp32'])
+    ap.add_argument('--workload', default='poisson128',
+                    choices=['poisson128', 'mixed192', 'uneven512', 'bands96'])
     ap.add_argument('--no-cpu', action='store_true',
                     help='skip the cpu_baseline sample')
     args = ap.parse_args()
+    if args.workload != 'poisson128':
+        {'mixed192': run_mixed192, 'uneven512': run_uneven,
+         'bands96': run_bands}[args.workload](args)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == 'ours' else args.warmup
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))

@@ -263,6 +263,65 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
 
 void gpw_poisson_free(gpw_poisson* ps) { delete ps; }
 
+static int ensure_f32(gpw_poisson* ps);
+static bool fused_dc(const gpw_poisson* ps);
+
+extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int which, int reps, double* ms_per_launch,
+                                       double* bytes_per_launch, gpw_stream stream) {
+  if (!ps || !ms_per_launch || !bytes_per_launch) return fail(GPW_EINVAL, "null argument");
+  if (nbatch < 1 || nbatch > ps->nbmax || reps < 1 || which < 0 || which > 4)
+    return fail(GPW_EINVAL, "time_level0: bad arguments");
+  if (which >= 2) {
+    int rc = ensure_f32(ps);
+    if (rc) return rc;
+  }
+  if ((which == 3 || which == 4) && !fused_dc(ps)) return fail(GPW_ENOTSUP, "time_level0: no fused path here");
+  cudaStream_t st = (cudaStream_t)stream;
+  Level& L0 = ps->lv[0];
+  const int nb = (int)nbatch;
+  const double pts = (double)view_points(L0.v) * nb;
+  const unsigned char* act = nullptr;
+  auto launch = [&]() -> cudaError_t {
+    switch (which) {
+      case 0:
+        return launch_stencil(*L0.op, GPW_F64, MODE_JACOBI, L0.phi[0].ptr, L0.v, L0.phi[1].ptr, L0.v, L0.rho.ptr,
+                              L0.v, nb, make_boundary(L0.op->periodic, GPW_F64, nullptr), L0.w, act, GridSum{}, st);
+      case 1:
+        return launch_stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, L0.v, nullptr, L0.v, L0.rho.ptr, L0.v,
+                              nb, make_boundary(L0.op->periodic, GPW_F64, nullptr), 1.0, act, ps->sums.gs(), st);
+      case 2:
+        return launch_stencil(*L0.op, GPW_F32, MODE_JACOBI, L0.phi32[0].ptr, L0.v, L0.phi32[1].ptr, L0.v,
+                              L0.rho32.ptr, L0.v, nb, make_boundary(L0.op->periodic, GPW_F32, nullptr), L0.w, act,
+                              GridSum{}, st);
+      case 3:
+        return launch_stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[0].ptr, L0.v, nullptr, L0.phi[1].ptr,
+                                 L0.rho32.ptr, nb, L0.w, 0.0, act, GridSum{}, st);
+      default:
+        return launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[1].ptr,
+                                 L0.rho.ptr, nb, 1.0, L0.w, act, ps->sums.gs(), st);
+    }
+  };
+  static const double bytes_pp[5] = {24.0, 16.0, 12.0, 24.0, 24.0};
+  cudaError_t e = launch();  // warm-up (and lazy kernel setup)
+  if (e != cudaSuccess) return cuda_fail(e, "time_level0 launch");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  for (int i = 0; i < reps && e == cudaSuccess; ++i) e = launch();
+  cudaEventRecord(e1, st);
+  cudaError_t se = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_fail(e, "time_level0 launch");
+  if (se != cudaSuccess) return cuda_fail(se, "time_level0 sync");
+  *ms_per_launch = ms / reps;
+  *bytes_per_launch = bytes_pp[which] * pts;
+  return GPW_OK;
+}
+
 extern "C" int gpw_poisson_last_stats(const gpw_poisson* ps, int64_t* kernel_launches, int64_t* graph_launches) {
   if (!ps) return fail(GPW_EINVAL, "null argument");
   if (kernel_launches) *kernel_launches = ps->last_kernels;

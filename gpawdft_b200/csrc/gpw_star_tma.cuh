@@ -173,6 +173,23 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
             }
           }
         }
+        // JACOBI_ADD64: prefetch the float64 phi that receives this plane's update
+        double2 phi64[PY];
+        if constexpr (MODE == MODE_JACOBI_ADD64) {
+#pragma unroll
+          for (int j = 0; j < PY; ++j) {
+            phi64[j] = make_double2(0.0, 0.0);
+            const int y = y0 + yb + j;
+            if (o >= z0 && y < a.vout.n[1] && xin0) {
+              const double* pp = static_cast<const double*>(a.out2) + (int64_t)b * a.vout.sb +
+                                 (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
+              if (xin1)
+                phi64[j] = *reinterpret_cast<const double2*>(pp);
+              else
+                phi64[j].x = pp[0];
+            }
+          }
+        }
         if (!mbar_wait_bounded(mbar_u32(&bars[slot]), (unsigned)((s / NS) & 1))) timed_out = true;
 
         // column of PY + 2R rows (2 points each) at this thread's columns
@@ -263,14 +280,13 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
               } else if constexpr (MODE == MODE_JACOBI_ADD64) {
                 // phi64 += e (the inner correction), e never stored
                 double* pp = static_cast<double*>(a.out2) + oidx;
-                if (xin1) {
-                  double2 pv = *reinterpret_cast<double2*>(pp);
-                  pv.x += (double)res.x;
-                  pv.y += (double)res.y;
+                double2 pv = phi64[j];
+                pv.x += (double)res.x;
+                pv.y += (double)res.y;
+                if (xin1)
                   *reinterpret_cast<double2*>(pp) = pv;
-                } else {
-                  pp[0] += (double)res.x;
-                }
+                else
+                  pp[0] = pv.x;
               } else if (MODE != MODE_RESIDUAL || a.out) {
                 S* op = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 +
                         (int64_t)y * a.vout.s1 + x;

@@ -35,7 +35,7 @@ struct TransferArgs {
   int zchunk, nchunk; // output planes of axis 0 per CTA
   const unsigned char* active;
   int subtract;       // interpolation: out = base - I(in) instead of out = I(in)
-  const void* base;   // (base may alias out: the reference's phi -= I(e))
+  const void* base;   // (the reference's phi -= I(e) into another buffer; must not alias out)
   GridView vbase;
 };
 

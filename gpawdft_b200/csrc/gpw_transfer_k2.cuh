@@ -59,8 +59,8 @@ __global__ void __launch_bounds__(K2_TX* K2_TY) restrict_k2_kernel(const Transfe
   const int I2 = blockIdx.x * K2_TX + threadIdx.x, I1 = blockIdx.y * K2_TY + threadIdx.y;
   if (I1 >= a.vout.n[1] || I2 >= a.vout.n[2]) return;
   const int I0s = chunk * a.zchunk, I0e = min(a.vout.n[0], I0s + a.zchunk);
-  const S* in = static_cast<const S*>(a.in) + (int64_t)b * a.vin.sb;
-  S* out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)I1 * a.vout.s1 + I2;
+  const S* __restrict__ in = static_cast<const S*>(a.in) + (int64_t)b * a.vin.sb;
+  S* __restrict__ out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)I1 * a.vout.s1 + I2;
   // fine centres (unpadded): c = 1 + 2 I - pad0; taps c-1, c, c+1
   const int c1 = 1 + 2 * I1 - a.pad0[1], c2 = 1 + 2 * I2 - a.pad0[2];
   int64_t off[3][3];  // [axis-1 tap][axis-2 tap] in-plane element offsets
@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(K2_TX* K2_TY) restrict_k2_kernel(const Transfe
     return r2(z[0], z[1], z[2]);
   };
   S ylo = Y(1 + 2 * I0s - a.pad0[0] - 1);
+#pragma unroll 2
   for (int I0 = I0s; I0 < I0e; ++I0) {
     const int c0 = 1 + 2 * I0 - a.pad0[0];
     const S ym = Y(c0), yp = Y(c0 + 1);
@@ -103,10 +104,11 @@ __global__ void __launch_bounds__(K2_TX* K2_TY) interpolate_k2_kernel(const Tran
   const int o2 = blockIdx.x * K2_TX + threadIdx.x, o1 = blockIdx.y * K2_TY + threadIdx.y;
   if (o1 >= a.vout.n[1] || o2 >= a.vout.n[2]) return;
   const int O0s = chunk * a.zchunk, O0e = min(a.vout.n[0], O0s + a.zchunk);
-  const S* in = static_cast<const S*>(a.in) + (int64_t)b * a.vin.sb;
-  S* out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)o1 * a.vout.s1 + o2;
-  const S* base = a.subtract ? static_cast<const S*>(a.base) + (int64_t)b * a.vbase.sb + (int64_t)o1 * a.vbase.s1 + o2
-                             : nullptr;
+  const S* __restrict__ in = static_cast<const S*>(a.in) + (int64_t)b * a.vin.sb;
+  S* __restrict__ out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)o1 * a.vout.s1 + o2;
+  const S* __restrict__ base =
+      a.subtract ? static_cast<const S*>(a.base) + (int64_t)b * a.vbase.sb + (int64_t)o1 * a.vbase.s1 + o2
+                 : nullptr;
   // per axis: o + skip0 = 2 i + e; coarse (unpadded) index u = i - pad0
   const int t1 = o1 + a.skip0[1], t2 = o2 + a.skip0[2];
   const int u1 = (t1 >> 1) - a.pad0[1], e1 = t1 & 1;
@@ -135,25 +137,25 @@ __global__ void __launch_bounds__(K2_TX* K2_TY) interpolate_k2_kernel(const Tran
     if (e2) z1 = i2h(z1, k2_ld(pl + off[1][1], v0 && ok[1][1]));
     return i2h(z0, z1);
   };
-  // march over fine planes; two consecutive outputs share a coarse plane
-  int ucur = INT_MIN;
-  S ya = S(0), yb = S(0);  // Y(ucur), Y(ucur + 1)
-  for (int o0 = O0s; o0 < O0e; ++o0) {
-    const int t0 = o0 + a.skip0[0];
-    const int u0 = (t0 >> 1) - a.pad0[0], e0 = t0 & 1;
-    if (u0 != ucur) {
-      if (u0 == ucur + 1) {
-        ya = yb;
-        yb = Y(u0 + 1);
-      } else {
-        ya = Y(u0);
-        yb = Y(u0 + 1);
-      }
-      ucur = u0;
+  // march over coarse planes u: fine outputs o = 2 (u + pad0) + e0 - skip0
+  // (e0 = 0: Y(u); e0 = 1: the midpoint of Y(u) and Y(u+1)); the loads of
+  // the next plane do not depend on this plane's stores, so they run ahead
+  const int us = ((O0s + a.skip0[0]) >> 1) - a.pad0[0];
+  const int ue = ((O0e - 1 + a.skip0[0]) >> 1) - a.pad0[0];
+  S ya = Y(us);
+#pragma unroll 2
+  for (int u = us; u <= ue; ++u) {
+    const S yb = Y(u + 1);
+    const int oe = 2 * (u + a.pad0[0]) - a.skip0[0];
+    if (oe >= O0s && oe < O0e) {
+      const int64_t q = (int64_t)oe * a.vout.s0;
+      out[q] = a.subtract ? base[(int64_t)oe * a.vbase.s0] - ya : ya;
     }
-    const S val = e0 ? i2h(ya, yb) : ya;
-    S* dst = out + (int64_t)o0 * a.vout.s0;
-    *dst = a.subtract ? base[(int64_t)o0 * a.vbase.s0] - val : val;
+    if (oe + 1 >= O0s && oe + 1 < O0e) {
+      const S mid = i2h(ya, yb);
+      out[(int64_t)(oe + 1) * a.vout.s0] = a.subtract ? base[(int64_t)(oe + 1) * a.vbase.s0] - mid : mid;
+    }
+    ya = yb;
   }
 }
 

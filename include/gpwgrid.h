@@ -205,6 +205,17 @@ int gpw_poisson_solve(gpw_poisson *ps, double *phi, const double *rho,
 int gpw_poisson_last_stats(const gpw_poisson *ps, int64_t *kernel_launches,
                            int64_t *graph_launches);
 
+/* Times one level-0 kernel of the engine on its own buffers (contents are
+ * overwritten; call between solves): `which` 0 = float64 Jacobi sweep,
+ * 1 = float64 residual + norm, 2 = float32 Jacobi sweep, 3 = float32 sweep
+ * adding into float64 phi (defect-correction update), 4 = float64 defect
+ * (float32 rhs + first sweep + norm).  `reps` launches between CUDA events
+ * on `stream`; writes the mean milliseconds per launch and the algorithmic
+ * bytes per launch (each compulsory read and write counted once).          */
+int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
+                            int reps, double *ms_per_launch,
+                            double *bytes_per_launch, gpw_stream stream);
+
 void gpw_poisson_free(gpw_poisson *ps);
 
 #ifdef __cplusplus
