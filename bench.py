@@ -86,55 +86,79 @@ def reduce_max(x, dist, device):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    """nvidia-smi clock / throttle-reason samples (100 ms period).
 
-    Q = ('index,clocks.sm,clocks.max.sm,power.draw,'
+    Started before the warm-up so that the sampler is running when the
+    timed region begins; ``window(t0, t1)`` keeps the samples whose host
+    timestamps fall inside the timed region.
+    """
+
+    Q = ('timestamp,index,clocks.sm,clocks.max.sm,power.draw,'
          'clocks_event_reasons.hw_slowdown,'
          'clocks_event_reasons.hw_thermal_slowdown,'
          'clocks_event_reasons.sw_thermal_slowdown,'
          'clocks_event_reasons.sw_power_cap')
+    NAMES = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+             'sw_power_cap']
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.lines = []
+        self.reader = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.Q,
-                 '--format=csv,noheader,nounits', '-lms', '200'],
+                 '--format=csv,noheader,nounits', '-lms', '100'],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        time.sleep(1.0)  # nvidia-smi start-up
 
-    def stop(self):
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line))
+
+    def stop(self, t0=None, t1=None):
         if self.proc is None:
-            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+            return {'sm_mhz': None, 'sm_max_mhz': None,
+                    'reasons': ['unsampled']}
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-            out = ''
-        sm, smax, reasons = [], [], set()
-        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
-                 'sw_power_cap']
-        for line in out.strip().splitlines():
+        if self.reader is not None:
+            self.reader.join(timeout=5)
+        rows = []
+        for ts, line in self.lines:
             f = [x.strip() for x in line.split(',')]
-            if len(f) < 8:
+            if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                rows.append((ts, float(f[2]), float(f[3]),
+                             [n for n, v in zip(self.NAMES, f[5:9])
+                              if v.lower() == 'active']))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[4:8]):
-                if v.lower() == 'active':
-                    reasons.add(nm)
-        if not sm:
-            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
-        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': max(smax),
-                'reasons': sorted(reasons), 'samples': len(sm)}
+        # a sample line is printed when it is taken: keep those stamped in
+        # the timed window (plus one period of slack on each side)
+        sel = [r for r in rows if t0 is None or t0 - 0.1 <= r[0] <= t1 + 0.1]
+        scope = 'timed region'
+        if not sel:
+            sel, scope = rows, 'whole run (timed region shorter than a sample)'
+        if not sel:
+            return {'sm_mhz': None, 'sm_max_mhz': None,
+                    'reasons': ['unsampled']}
+        reasons = sorted({n for r in sel for n in r[3]})
+        return {'sm_mhz': float(np.median([r[1] for r in sel])),
+                'sm_max_mhz': max(r[2] for r in sel), 'reasons': reasons,
+                'samples': len(sel), 'scope': scope}
 
 
 # ------------------------------------------------------------------ CPU side
@@ -188,7 +212,11 @@ def cpu_arm(rounds, warmup, seed0=10_000):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    r = cpu_arm(args.steps, args.warmup)
+    # one round (a solve per host core) takes ~10 s on a 16-core host: the
+    # sample is capped at 6 timed rounds and 1 warm-up round so that the
+    # reference arm ends within a couple of minutes whatever K and W are
+    rounds, warm = max(1, min(args.steps, 6)), min(args.warmup, 1)
+    r = cpu_arm(rounds, warm)
     v = float(np.mean(r['rates']))
     line = {'metric': METRIC, 'value': v, 'unit': 'solves/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup,
@@ -201,7 +229,8 @@ def run_reference(args, rank, world):
                              'sample': r['sample']},
             'e2e': {'value': v, 'unit': 'solves/s', 'h2d_bytes_per_step': 0,
                     'd2h_bytes_per_step': 0},
-            'vcycles_mean': r['vcycles_mean']}
+            'vcycles_mean': r['vcycles_mean'],
+            'rounds_timed': rounds, 'rounds_warmup': warm}
     print(json.dumps(line), flush=True)
 
 
@@ -259,15 +288,16 @@ def run_ours(args, rank, world, dist):
 
     # ---- device-resident throughput
     niters = None
+    clk = ClockSampler(dev.index)
+    clk.start()
     for _ in range(args.warmup):
         phi_d.zero_()
         niters = ps.solve_batch(phi_d, rho_d, eps=eps)
     barrier()
-    clk = ClockSampler(dev.index)
-    clk.start()
     launches = 0
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
     e0.record(stream)
     for _ in range(args.steps):
         phi_d.zero_()
@@ -275,7 +305,7 @@ def run_ours(args, rank, world, dist):
         launches += stats()[0]
     e1.record(stream)
     barrier()
-    clocks = clk.stop()
+    clocks = clk.stop(w0, time.time())
     t_dev = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
     value = world * B * args.steps / t_dev
 
@@ -631,7 +661,7 @@ def run_bands(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--batch', type=int, default=16)

@@ -29,7 +29,8 @@ EXPORTS = [
     'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
     'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_add_scalar',
     'gpw_poisson_new', 'gpw_poisson_solve', 'gpw_poisson_last_stats',
-    'gpw_poisson_time_level0', 'gpw_poisson_free',
+    'gpw_poisson_time_level0', 'gpw_poisson_set_inner_schedule',
+    'gpw_poisson_free',
 ]
 
 _c_i64p = ctypes.POINTER(ctypes.c_int64)
@@ -80,6 +81,8 @@ _SIGS = {
     'gpw_poisson_last_stats': (ctypes.c_int, [_vp, _vp, _vp]),
     'gpw_poisson_time_level0': (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int,
                                                ctypes.c_int, _vp, _vp, _vp]),
+    'gpw_poisson_set_inner_schedule': (ctypes.c_int, [_vp, _vp, _vp, _vp,
+                                                      ctypes.c_int]),
     'gpw_poisson_free': (None, [_vp]),
 }
 

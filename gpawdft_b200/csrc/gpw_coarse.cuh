@@ -1,0 +1,234 @@
+// The coarse end of the multigrid V-cycle in one CTA per solve.
+//
+// Below ~15^3 points a level is too small to fill the GPU: at 127^3 the
+// levels 15^3, 7^3, 3^3 and 1^3 of gpaw/poisson.py's hierarchy cost ~35
+// launches per V-cycle, each bound by launch latency.  This kernel runs the
+// recursive part of iterate2 (gpaw/poisson.py:331-356) from a level `lc`
+// down to the coarsest level and back for one batch member per CTA, with
+// every level's phi (two ping-pong buffers) and rho resident in shared
+// memory:
+//   for l = lc .. L-1:  pre-sweeps, r = A phi - rho, rho_{l+1} = R r,
+//                       phi_{l+1} = 0
+//   coarsest:           post-sweeps
+//   for l = L-1 .. lc:  phi_l -= I phi_{l+1}, post-sweeps
+// The input is rho_lc (written by the restriction from level lc-1), the
+// output phi_lc (read by the interpolation to level lc-1).
+//
+// Operators are the 7-point (nn=1) Laplacians of the coarse levels
+// (gpaw/poisson.py:118-130) with weighted-Jacobi sweeps, one weight per
+// sweep.  Restriction and interpolation are the K=2 transformers
+// (c/bmgs/restrict.c:37-39, c/bmgs/interpolate.c:31-33) evaluated with the
+// same expressions as gpw_transfer_k2.cuh; boundaries are zero or periodic
+// (real data, no Bloch phase).
+#pragma once
+#include "gpw_common.cuh"
+#include "gpw_transfer.cuh"
+#include "gpw_transfer_k2.cuh"
+
+namespace gpw {
+
+constexpr int CG_MAXL = 8;       // levels handled inside the kernel
+constexpr int CG_MAXW = 16;      // sweep weights per level (pre then post)
+constexpr int CG_THREADS = 512;  // threads per CTA
+
+struct CoarseLevel {
+  int n[3];
+  int periodic[3];
+  int pts;                // n0 * n1 * n2
+  int base;               // element offset of the level's buffers: phi0, phi1, rho
+  double cc;              // centre coefficient
+  double cm[3], cp[3];    // neighbour coefficients at offsets -1 / +1 per axis
+  int npre, npost;
+  double w[CG_MAXW];      // pre-sweep weights, then post-sweep weights
+  int rpad0[3];           // restriction to the next level: low padding
+  int ipad0[3], iskip0[3];  // interpolation from the next level
+};
+
+struct CoarseArgs {
+  int nl;                 // levels in the kernel (lc .. L)
+  CoarseLevel lv[CG_MAXL];
+  const void* rho;        // rho of level lc, engine layout
+  GridView vrho;
+  void* phi;              // phi of level lc (result)
+  GridView vphi;
+  const unsigned char* active;
+};
+
+__device__ __forceinline__ int cg_wrap(int i, int n, int periodic, bool& ok) {
+  ok = true;
+  if (i >= 0 && i < n) return i;
+  if (!periodic) {
+    ok = false;
+    return 0;
+  }
+  i %= n;
+  return i < 0 ? i + n : i;
+}
+
+template <typename S>
+__device__ __forceinline__ S cg_at(const S* buf, const CoarseLevel& L, int i0, int i1, int i2) {
+  bool o0, o1, o2;
+  i0 = cg_wrap(i0, L.n[0], L.periodic[0], o0);
+  i1 = cg_wrap(i1, L.n[1], L.periodic[1], o1);
+  i2 = cg_wrap(i2, L.n[2], L.periodic[2], o2);
+  return (o0 && o1 && o2) ? buf[(i0 * L.n[1] + i1) * L.n[2] + i2] : S(0);
+}
+
+__device__ __forceinline__ void cg_index(const CoarseLevel& L, int i, int& i0, int& i1, int& i2) {
+  i2 = i % L.n[2];
+  const int t = i / L.n[2];
+  i1 = t % L.n[1];
+  i0 = t / L.n[1];
+}
+
+// sum_{p != 0} c_p phi[x + o_p]
+template <typename S>
+__device__ __forceinline__ S cg_offdiag(const S* phi, const CoarseLevel& L, int i0, int i1, int i2) {
+  S av = (S)L.cm[2] * cg_at(phi, L, i0, i1, i2 - 1);
+  av = fmac((S)L.cp[2], cg_at(phi, L, i0, i1, i2 + 1), av);
+  av = fmac((S)L.cm[1], cg_at(phi, L, i0, i1 - 1, i2), av);
+  av = fmac((S)L.cp[1], cg_at(phi, L, i0, i1 + 1, i2), av);
+  av = fmac((S)L.cm[0], cg_at(phi, L, i0 - 1, i1, i2), av);
+  av = fmac((S)L.cp[0], cg_at(phi, L, i0 + 1, i1, i2), av);
+  return av;
+}
+
+// dst = (1 - w) src + (w / c0) (rho - sum_{p != 0} c_p src[x + o_p])   (c/bmgs/relax.c:62)
+template <typename S>
+__device__ __forceinline__ void cg_jacobi(const CoarseLevel& L, const S* src, S* dst, const S* rho, double wd) {
+  const S w = (S)wd, wc = w / (S)L.cc;
+  for (int i = threadIdx.x; i < L.pts; i += blockDim.x) {
+    int i0, i1, i2;
+    cg_index(L, i, i0, i1, i2);
+    const S av = cg_offdiag(src, L, i0, i1, i2);
+    dst[i] = (S(1) - w) * src[i] + wc * (rho[i] - av);
+  }
+  __syncthreads();
+}
+
+// r = A phi - rho
+template <typename S>
+__device__ __forceinline__ void cg_residual(const CoarseLevel& L, const S* phi, S* r, const S* rho) {
+  for (int i = threadIdx.x; i < L.pts; i += blockDim.x) {
+    int i0, i1, i2;
+    cg_index(L, i, i0, i1, i2);
+    const S av = cg_offdiag(phi, L, i0, i1, i2);
+    r[i] = fmac((S)L.cc, phi[i], av) - rho[i];
+  }
+  __syncthreads();
+}
+
+// rho_C = R r_F (K = 2) and phi_C = 0
+template <typename S>
+__device__ __forceinline__ void cg_restrict(const CoarseLevel& F, const S* r, const CoarseLevel& C, S* rho_c,
+                                            S* phi_c) {
+  for (int i = threadIdx.x; i < C.pts; i += blockDim.x) {
+    int I0, I1, I2;
+    cg_index(C, i, I0, I1, I2);
+    const int c0 = 1 + 2 * I0 - F.rpad0[0], c1 = 1 + 2 * I1 - F.rpad0[1], c2 = 1 + 2 * I2 - F.rpad0[2];
+    S y[3];
+#pragma unroll
+    for (int d0 = 0; d0 < 3; ++d0) {
+      S z[3];
+#pragma unroll
+      for (int d1 = 0; d1 < 3; ++d1)
+        z[d1] = r2(cg_at(r, F, c0 - 1 + d0, c1 - 1 + d1, c2 - 1), cg_at(r, F, c0 - 1 + d0, c1 - 1 + d1, c2),
+                   cg_at(r, F, c0 - 1 + d0, c1 - 1 + d1, c2 + 1));
+      y[d0] = r2(z[0], z[1], z[2]);
+    }
+    rho_c[i] = r2(y[0], y[1], y[2]);
+    phi_c[i] = S(0);
+  }
+  __syncthreads();
+}
+
+// dst = base - I e_C (K = 2)
+template <typename S>
+__device__ __forceinline__ S cg_interp_plane(const S* e, const CoarseLevel& C, int u0, int u1, int u2, int e1,
+                                             int e2) {
+  S z0 = cg_at(e, C, u0, u1, u2);
+  if (e2) z0 = i2h(z0, cg_at(e, C, u0, u1, u2 + 1));
+  if (!e1) return z0;
+  S z1 = cg_at(e, C, u0, u1 + 1, u2);
+  if (e2) z1 = i2h(z1, cg_at(e, C, u0, u1 + 1, u2 + 1));
+  return i2h(z0, z1);
+}
+
+template <typename S>
+__device__ __forceinline__ void cg_interp_sub(const CoarseLevel& F, const S* base, S* dst, const CoarseLevel& C,
+                                              const S* e) {
+  for (int i = threadIdx.x; i < F.pts; i += blockDim.x) {
+    int o0, o1, o2;
+    cg_index(F, i, o0, o1, o2);
+    const int t0 = o0 + F.iskip0[0], t1 = o1 + F.iskip0[1], t2 = o2 + F.iskip0[2];
+    const int u0 = (t0 >> 1) - F.ipad0[0], u1 = (t1 >> 1) - F.ipad0[1], u2 = (t2 >> 1) - F.ipad0[2];
+    S v = cg_interp_plane(e, C, u0, u1, u2, t1 & 1, t2 & 1);
+    if (t0 & 1) v = i2h(v, cg_interp_plane(e, C, u0 + 1, u1, u2, t1 & 1, t2 & 1));
+    dst[i] = base[i] - v;
+  }
+  __syncthreads();
+}
+
+template <typename S>
+__global__ void __launch_bounds__(CG_THREADS) coarse_vcycle_kernel(const CoarseArgs a) {
+  const int b = blockIdx.x;
+  if (a.active && !a.active[b]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sm = reinterpret_cast<S*>(smem_raw);
+  const int nl = a.nl;
+  int cur[CG_MAXL];
+  {
+    const CoarseLevel& L = a.lv[0];
+    S* phi = sm + L.base;
+    S* rho = sm + L.base + 2 * L.pts;
+    const S* g = static_cast<const S*>(a.rho) + (int64_t)b * a.vrho.sb;
+    for (int i = threadIdx.x; i < L.pts; i += blockDim.x) {
+      int i0, i1, i2;
+      cg_index(L, i, i0, i1, i2);
+      rho[i] = g[(int64_t)i0 * a.vrho.s0 + (int64_t)i1 * a.vrho.s1 + i2];
+      phi[i] = S(0);
+    }
+    __syncthreads();
+  }
+  // descend
+  for (int l = 0; l < nl; ++l) {
+    const CoarseLevel& L = a.lv[l];
+    S* P[2] = {sm + L.base, sm + L.base + L.pts};
+    const S* rho = sm + L.base + 2 * L.pts;
+    int c = 0;
+    if (l == nl - 1) {
+      for (int s = 0; s < L.npost; ++s, c = 1 - c) cg_jacobi(L, P[c], P[1 - c], rho, L.w[L.npre + s]);
+      cur[l] = c;
+      break;
+    }
+    for (int s = 0; s < L.npre; ++s, c = 1 - c) cg_jacobi(L, P[c], P[1 - c], rho, L.w[s]);
+    cur[l] = c;
+    cg_residual(L, P[c], P[1 - c], rho);
+    const CoarseLevel& C = a.lv[l + 1];
+    cg_restrict(L, P[1 - c], C, sm + C.base + 2 * C.pts, sm + C.base);
+  }
+  // ascend
+  for (int l = nl - 2; l >= 0; --l) {
+    const CoarseLevel& L = a.lv[l];
+    const CoarseLevel& C = a.lv[l + 1];
+    S* P[2] = {sm + L.base, sm + L.base + L.pts};
+    const S* rho = sm + L.base + 2 * L.pts;
+    int c = cur[l];
+    cg_interp_sub(L, P[c], P[1 - c], C, sm + C.base + cur[l + 1] * C.pts);
+    c = 1 - c;
+    for (int s = 0; s < L.npost; ++s, c = 1 - c) cg_jacobi(L, P[c], P[1 - c], rho, L.w[L.npre + s]);
+    cur[l] = c;
+  }
+  {
+    const CoarseLevel& L = a.lv[0];
+    const S* phi = sm + L.base + cur[0] * L.pts;
+    S* g = static_cast<S*>(a.phi) + (int64_t)b * a.vphi.sb;
+    for (int i = threadIdx.x; i < L.pts; i += blockDim.x) {
+      int i0, i1, i2;
+      cg_index(L, i, i0, i1, i2);
+      g[(int64_t)i0 * a.vphi.s0 + (int64_t)i1 * a.vphi.s1 + i2] = phi[i];
+    }
+  }
+}
+
+}  // namespace gpw

@@ -111,6 +111,12 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
                             const void* base, const GridView* vbase, const unsigned char* active,
                             cudaStream_t st);
 
+// ---------------------------------------------------------------- coarse levels
+// The coarse end of a V-cycle in one CTA per batch member (gpw_coarse.cuh);
+// smem = the levels' buffer bytes.
+struct CoarseArgs;
+cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatch, cudaStream_t st);
+
 // ---------------------------------------------------------------- blas
 cudaError_t launch_axpy(int dtype, int64_t n, double ar, double ai, const void* x, void* y, cudaStream_t st);
 cudaError_t launch_scal(int dtype, int64_t n, double ar, double ai, void* x, cudaStream_t st);

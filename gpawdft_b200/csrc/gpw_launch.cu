@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 
 #include "gpw_blas.cuh"
+#include "gpw_coarse.cuh"
 #include "gpw_internal.h"
 #include "gpw_star_tma.cuh"
 #include "gpw_stencil.cuh"
@@ -373,6 +374,46 @@ static cudaError_t dispatch_transfer(const TransferArgs& a, int k, bool interp, 
   return cudaErrorInvalidValue;
 }
 
+// ------------------------------------------------------------------ coarse levels
+cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatch, cudaStream_t st) {
+  if (a.nl < 1 || a.nl > CG_MAXL || nbatch < 1 || smem > 200 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e;
+  if (dtype == GPW_F64) {
+    static std::once_flag once;
+    static cudaError_t oe = cudaSuccess;
+    std::call_once(once, [] {
+      oe = cudaFuncSetAttribute(coarse_vcycle_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                200 * 1024);
+    });
+    if (oe != cudaSuccess) return oe;
+    coarse_vcycle_kernel<double><<<nbatch, CG_THREADS, smem, st>>>(a);
+  } else if (dtype == GPW_F32) {
+    static std::once_flag once;
+    static cudaError_t oe = cudaSuccess;
+    std::call_once(once, [] {
+      oe = cudaFuncSetAttribute(coarse_vcycle_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                200 * 1024);
+    });
+    if (oe != cudaSuccess) return oe;
+    coarse_vcycle_kernel<float><<<nbatch, CG_THREADS, smem, st>>>(a);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  e = cudaGetLastError();
+  return e;
+}
+
+// The vector interpolation needs 16-byte aligned rows / planes / batch
+// members of `out` (and `base`) and grids wide enough to fill the vectors.
+static bool k2_vec_ok(const TransferArgs& a) {
+  auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+  auto view_ok = [](const GridView& v) { return v.s1 % 4 == 0 && v.s0 % 4 == 0 && v.sb % 4 == 0; };
+  if (a.vout.n[2] < 8) return false;
+  if (!aligned(a.out) || !view_ok(a.vout)) return false;
+  if (a.subtract && (!aligned(a.base) || !view_ok(a.vbase))) return false;
+  return true;
+}
+
 cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const GridView& vin, void* out,
                             const GridView& vout, int nbatch, const Boundary& bc, int subtract,
                             const void* base, const GridView* vbase, const unsigned char* active,
@@ -392,6 +433,23 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
   a.base = base;
   if (vbase) a.vbase = *vbase;
   const bool interp = d.interpolate != 0;
+  if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32) && interp && k2_vec_ok(a)) {
+    dim3 grid((vout.n[2] + 4 * K2V_TX - 1) / (4 * K2V_TX), (vout.n[1] + K2V_TY - 1) / K2V_TY, 1);
+    // ~8 CTAs of 256 threads per SM; chunks of at least 8 output planes
+    const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
+    const int64_t want = 8LL * num_sms();
+    int64_t nc = std::max<int64_t>(1, (want + tiles - 1) / tiles);
+    nc = std::min<int64_t>(nc, std::max(1, vout.n[0] / 8));
+    a.zchunk = (int)((vout.n[0] + nc - 1) / nc);
+    a.nchunk = (vout.n[0] + a.zchunk - 1) / a.zchunk;
+    grid.z = a.nchunk * nbatch;
+    const dim3 blk(K2V_TX, K2V_TY);
+    if (dtype == GPW_F64)
+      interpolate_k2_vec_kernel<double><<<grid, blk, 0, st>>>(a);
+    else
+      interpolate_k2_vec_kernel<float><<<grid, blk, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32)) {
     dim3 grid((vout.n[2] + K2_TX - 1) / K2_TX, (vout.n[1] + K2_TY - 1) / K2_TY, 1);
     choose_chunks(vout.n[0], (int64_t)grid.x * grid.y * nbatch, 4, a.zchunk, a.nchunk);

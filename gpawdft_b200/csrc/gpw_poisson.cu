@@ -22,6 +22,7 @@
 #include <memory>
 #include <vector>
 
+#include "gpw_coarse.cuh"
 #include "gpw_internal.h"
 #include "gpw_relax_gs.cuh"
 
@@ -34,6 +35,8 @@ struct Level {
   GridView v;
   int pre = 0, post = 0;
   double w = 1.0;
+  // per-sweep Jacobi weights, [0] float64 method, [1] float32 inner cycles
+  std::vector<double> wpre[2], wpost[2];
   // float64 buffers (nbatch_max grids each)
   Workspace phi[2], rho, res;
   // float32 buffers for the defect-correction form
@@ -90,6 +93,11 @@ struct gpw_poisson {
   int relax_method = 2;
   double dv = 1.0;
   int64_t nbmax = 1;
+  // coarse end of the V-cycle in one CTA per solve (gpw_coarse.cuh): first
+  // level handled there per form ([0] float64, [1] float32; nlevels = off)
+  int lc[2] = {0, 0};
+  CoarseArgs cargs[2];
+  size_t csmem[2] = {0, 0};
   Workspace d_err, d_eps, d_niter, d_active, d_any, d_r64, d_gs_old, d_maxiter;
   SumScratch sums;
   int* h_any = nullptr;  // pinned
@@ -122,7 +130,7 @@ struct Rec {
 
 // Relax `n` sweeps on level l (dtype f64 or f32); returns the index of the
 // phi buffer holding the result.
-int rec_relax(Rec& r, int l, int cur, int nsweeps, bool f32) {
+int rec_relax(Rec& r, int l, int cur, const double* ws, int nsweeps, bool f32) {
   Level& L = r.ps->lv[l];
   const int dt = f32 ? GPW_F32 : GPW_F64;
   Boundary bc = make_boundary(L.op->periodic, dt, nullptr);
@@ -138,7 +146,7 @@ int rec_relax(Rec& r, int l, int cur, int nsweeps, bool f32) {
     return cur;
   }
   for (int s = 0; s < nsweeps; ++s) {
-    r.ok(launch_stencil(*L.op, dt, MODE_JACOBI, phi[cur].ptr, L.v, phi[1 - cur].ptr, L.v, rho, L.v, r.nb, bc, L.w,
+    r.ok(launch_stencil(*L.op, dt, MODE_JACOBI, phi[cur].ptr, L.v, phi[1 - cur].ptr, L.v, rho, L.v, r.nb, bc, ws[s],
                         r.active, gs, r.st));
     cur = 1 - cur;
   }
@@ -156,22 +164,36 @@ int rec_vcycle(Rec& r, int l, int cur, bool f32) {
   Workspace& rho = f32 ? L.rho32 : L.rho;
   Workspace& res = f32 ? L.res32 : L.res;
   Boundary bc = make_boundary(L.op->periodic, dt, nullptr);
+  const int p = f32 ? 1 : 0;
   if (l < nl - 1) {
     Level& C = ps->lv[l + 1];
     Workspace* cphi = f32 ? C.phi32 : C.phi;
     Workspace& crho = f32 ? C.rho32 : C.rho;
-    cur = rec_relax(r, l, cur, L.pre, f32);
+    cur = rec_relax(r, l, cur, L.wpre[p].data(), (int)L.wpre[p].size(), f32);
     r.ok(launch_stencil(*L.op, dt, MODE_RESIDUAL, phi[cur].ptr, L.v, res.ptr, L.v, rho.ptr, L.v, r.nb, bc, 1.0,
                         r.active, ps->sums.gs(), r.st));
     r.ok(launch_transfer(*L.restr, dt, res.ptr, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st));
-    r.ok(launch_zero(dt, C.v, cphi[0].ptr, r.nb, r.active, r.st));
-    int ccur = rec_vcycle(r, l + 1, 0, f32);
+    int ccur;
+    if (l + 1 == ps->lc[p]) {
+      // levels l+1 .. L in one CTA per solve: rho_{l+1} in, phi_{l+1} out
+      CoarseArgs ca = ps->cargs[p];
+      ca.rho = crho.ptr;
+      ca.vrho = C.v;
+      ca.phi = cphi[0].ptr;
+      ca.vphi = C.v;
+      ca.active = r.active;
+      r.ok(launch_coarse(dt, ca, ps->csmem[p], r.nb, r.st));
+      ccur = 0;
+    } else {
+      r.ok(launch_zero(dt, C.v, cphi[0].ptr, r.nb, r.active, r.st));
+      ccur = rec_vcycle(r, l + 1, 0, f32);
+    }
     Boundary cbc = make_boundary(C.op->periodic, dt, nullptr);
     r.ok(launch_transfer(*L.interp, dt, cphi[ccur].ptr, C.v, phi[1 - cur].ptr, L.v, r.nb, cbc, 1, phi[cur].ptr, &L.v,
                          r.active, r.st));
     cur = 1 - cur;
   }
-  cur = rec_relax(r, l, cur, L.post, f32);
+  cur = rec_relax(r, l, cur, L.wpost[p].data(), (int)L.wpost[p].size(), f32);
   return cur;
 }
 
@@ -195,6 +217,68 @@ const OpDesc* operator_desc(const gpw_operator* op);
 const TrDesc* transformer_desc(const gpw_transformer* tr);
 }  // namespace gpw
 
+// Choose the first level of the coarse one-CTA kernel for form p (0 float64,
+// 1 float32) and fill its arguments: the deepest suffix of levels (never
+// level 0) that are real 7-point star Laplacians relaxed by Jacobi and whose
+// buffers (two phi + rho per level) fit the shared-memory budget.
+static void setup_coarse(gpw_poisson* ps, int p) {
+  const int nl = (int)ps->lv.size();
+  const size_t es = p ? 4 : 8;
+  const size_t budget = 160 * 1024;
+  ps->lc[p] = nl;
+  ps->csmem[p] = 0;
+  if (ps->relax_method != 2) return;
+  size_t bytes = 0;
+  int lc = nl;
+  for (int l = nl - 1; l >= 1 && nl - l <= CG_MAXL; --l) {
+    const Level& L = ps->lv[l];
+    const OpDesc& d = *L.op;
+    if (!d.real || !d.star_jacobi || d.R != 1) break;
+    if ((int)(L.wpre[p].size() + L.wpost[p].size()) > CG_MAXW) break;
+    const size_t b = 3 * (size_t)view_points(L.v) * es;
+    if (bytes + b > budget) break;
+    bytes += b;
+    lc = l;
+  }
+  if (lc >= nl) return;
+  CoarseArgs& ca = ps->cargs[p];
+  ca = CoarseArgs{};
+  ca.nl = nl - lc;
+  int base = 0;
+  for (int k = 0; k < ca.nl; ++k) {
+    const Level& L = ps->lv[lc + k];
+    const OpDesc& d = *L.op;
+    CoarseLevel& c = ca.lv[k];
+    for (int a = 0; a < 3; ++a) {
+      c.n[a] = L.v.n[a];
+      c.periodic[a] = d.periodic[a];
+    }
+    c.pts = (int)view_points(L.v);
+    c.base = base;
+    base += 3 * c.pts;
+    c.cc = d.sc.cc;
+    c.cm[0] = d.sc.cx[0];
+    c.cp[0] = d.sc.cx[2];
+    c.cm[1] = d.sc.cy[0];
+    c.cp[1] = d.sc.cy[2];
+    c.cm[2] = d.sc.cz[0];
+    c.cp[2] = d.sc.cz[2];
+    c.npre = (int)L.wpre[p].size();
+    c.npost = (int)L.wpost[p].size();
+    for (int i = 0; i < c.npre; ++i) c.w[i] = L.wpre[p][i];
+    for (int i = 0; i < c.npost; ++i) c.w[c.npre + i] = L.wpost[p][i];
+    if (lc + k + 1 < nl) {
+      for (int a = 0; a < 3; ++a) {
+        c.rpad0[a] = L.restr->pad[a][0];
+        c.ipad0[a] = L.interp->pad[a][0];
+        c.iskip0[a] = L.interp->skip[a][0];
+      }
+    }
+  }
+  ps->lc[p] = lc;
+  ps->csmem[p] = bytes;
+}
+
 int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer* const* restrictors,
                     gpw_transformer* const* interpolators, const int* presmooths, const int* postsmooths,
                     const double* weights, int relax_method, double dv, int64_t nbatch_max, gpw_poisson** out) {
@@ -216,6 +300,12 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
     L.pre = presmooths[l];
     L.post = postsmooths[l];
     L.w = weights[l];
+    if (L.pre < 0 || L.post < 0 || L.pre > CG_MAXW || L.post > CG_MAXW || L.pre + L.post > CG_MAXW)
+      return fail(GPW_EINVAL, "poisson: smoothing counts out of range");
+    for (int p = 0; p < 2; ++p) {
+      L.wpre[p].assign(l + 1 < nlevels ? L.pre : 0, L.w);
+      L.wpost[p].assign(L.post, L.w);
+    }
     if (l < nlevels - 1) {
       if (!restrictors[l] || !interpolators[l]) return fail(GPW_EINVAL, "poisson: null transformer");
       L.restr = transformer_desc(restrictors[l]);
@@ -238,6 +328,8 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
           A.interp->nout[c] != A.v.n[c])
         return fail(GPW_EINVAL, "poisson: level shapes do not chain");
   }
+  setup_coarse(ps.get(), 0);
+  setup_coarse(ps.get(), 1);
   int rc;
   if ((rc = ps->d_err.ensure(nbatch_max * 8)) || (rc = ps->d_eps.ensure(nbatch_max * 8)) ||
       (rc = ps->d_niter.ensure(nbatch_max * 4)) || (rc = ps->d_active.ensure(nbatch_max)) ||
@@ -347,7 +439,8 @@ static int ensure_f32(gpw_poisson* ps) {
 // Laplacians with at least one pre- and one post-sweep on level 0.
 static bool fused_dc(const gpw_poisson* ps) {
   const Level& L0 = ps->lv[0];
-  return ps->relax_method == 2 && ps->lv.size() >= 2 && L0.pre >= 1 && L0.post >= 1 && dc_fusable(*L0.op);
+  return ps->relax_method == 2 && ps->lv.size() >= 2 && !L0.wpre[1].empty() && !L0.wpost[1].empty() &&
+         dc_fusable(*L0.op);
 }
 
 static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, int maxiter_unused, cudaStream_t st) {
@@ -369,24 +462,38 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, int maxit
     // level-0 post-sweep adds e into float64 phi; then the fused residual
     // writes the next rhs / first sweep and the norm.
     Level& C = ps->lv[1];
-    int cur = rec_relax(r, 0, 0, L0.pre - 1, true);
+    const std::vector<double>& wpre = L0.wpre[1];
+    const std::vector<double>& wpost = L0.wpost[1];
+    int cur = rec_relax(r, 0, 0, wpre.data() + 1, (int)wpre.size() - 1, true);
     Boundary bc32 = make_boundary(L0.op->periodic, GPW_F32, nullptr);
     r.ok(launch_stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[cur].ptr, L0.v, L0.res32.ptr, L0.v, L0.rho32.ptr,
                         L0.v, nb, bc32, 1.0, r.active, ps->sums.gs(), st));
     r.ok(launch_transfer(*L0.restr, GPW_F32, L0.res32.ptr, L0.v, C.rho32.ptr, C.v, nb, bc32, 0, nullptr, nullptr,
                          r.active, st));
-    r.ok(launch_zero(GPW_F32, C.v, C.phi32[0].ptr, nb, r.active, st));
-    const int ccur = rec_vcycle(r, 1, 0, true);
+    int ccur;
+    if (ps->lc[1] == 1) {
+      CoarseArgs ca = ps->cargs[1];
+      ca.rho = C.rho32.ptr;
+      ca.vrho = C.v;
+      ca.phi = C.phi32[0].ptr;
+      ca.vphi = C.v;
+      ca.active = r.active;
+      r.ok(launch_coarse(GPW_F32, ca, ps->csmem[1], nb, st));
+      ccur = 0;
+    } else {
+      r.ok(launch_zero(GPW_F32, C.v, C.phi32[0].ptr, nb, r.active, st));
+      ccur = rec_vcycle(r, 1, 0, true);
+    }
     Boundary cbc = make_boundary(C.op->periodic, GPW_F32, nullptr);
     r.ok(launch_transfer(*L0.interp, GPW_F32, C.phi32[ccur].ptr, C.v, L0.phi32[1 - cur].ptr, L0.v, nb, cbc, 1,
                          L0.phi32[cur].ptr, &L0.v, r.active, st));
     cur = 1 - cur;
-    cur = rec_relax(r, 0, cur, L0.post - 1, true);
+    cur = rec_relax(r, 0, cur, wpost.data(), (int)wpost.size() - 1, true);
     GridSum none{};
     r.ok(launch_stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[cur].ptr, L0.v, nullptr, L0.phi[0].ptr,
-                           L0.rho32.ptr, nb, L0.w, 0.0, r.active, none, st));
+                           L0.rho32.ptr, nb, wpost.back(), 0.0, r.active, none, st));
     r.ok(launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr,
-                           nb, 1.0, L0.w, r.active, ps->sums.gs(), st));
+                           nb, 1.0, wpre[0], r.active, ps->sums.gs(), st));
     converge_update_kernel<<<1, 256, 0, st>>>(nb, ps->sums.gs().result, ps->dv, (const double*)ps->d_eps.ptr,
                                               (const int*)ps->d_maxiter.ptr, (double*)ps->d_err.ptr,
                                               (int*)ps->d_niter.ptr, (unsigned char*)ps->d_active.ptr,
@@ -445,7 +552,7 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
   if (precision == 1 && fused_dc(ps)) {
     // initial defect: float32 rhs and first level-0 sweep, fused
     e = launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr, nb,
-                          1.0, L0.w, (const unsigned char*)ps->d_active.ptr, ps->sums.gs(), st);
+                          1.0, L0.wpre[1][0], (const unsigned char*)ps->d_active.ptr, ps->sums.gs(), st);
     if (e != cudaSuccess) return cuda_fail(e, "poisson initial defect");
   } else if (precision == 1) {
     // initial residual for the first defect-correction step
@@ -508,5 +615,48 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
     return cuda_fail(e, "poisson result copies");
   for (int b = 0; b < nb; ++b)
     if (niter[b] >= maxiter) return fail(GPW_ECONV, "Poisson solver did not converge in maxiter iterations");
+  return GPW_OK;
+}
+
+// Float32 inner V-cycle schedule of the defect-correction form (precision 1):
+// per level npre[l] / npost[l] Jacobi sweeps with their own weights, listed
+// level by level in `weights` (npre[l] pre-sweep weights, then npost[l]
+// post-sweep weights; nweights = the total).  The coarsest level runs only
+// its post-sweeps (its pre-sweep weights are skipped).  The float64 method
+// keeps the reference schedule.  Captured graphs of the float32 form are
+// discarded.
+extern "C" int gpw_poisson_set_inner_schedule(gpw_poisson* ps, const int* npre, const int* npost,
+                                              const double* weights, int nweights) {
+  if (!ps || !npre || !npost || !weights) return fail(GPW_EINVAL, "null argument");
+  const int nl = (int)ps->lv.size();
+  int total = 0;
+  for (int l = 0; l < nl; ++l) {
+    const int pre = (l + 1 < nl) ? npre[l] : 0;
+    if (npre[l] < 0 || npost[l] < 0 || pre + npost[l] > CG_MAXW)
+      return fail(GPW_EINVAL, "inner schedule: sweep counts out of range");
+    if (l == 0 && nl > 1 && (pre < 1 || npost[l] < 1))
+      return fail(GPW_EINVAL, "inner schedule: level 0 needs at least one pre- and one post-sweep");
+    total += npre[l] + npost[l];
+  }
+  if (total != nweights) return fail(GPW_EINVAL, "inner schedule: weight count does not match the sweep counts");
+  int k = 0;
+  for (int l = 0; l < nl; ++l) {
+    Level& L = ps->lv[l];
+    const int pre = (l + 1 < nl) ? npre[l] : 0;
+    L.wpre[1].assign(weights + k, weights + k + pre);
+    k += npre[l];
+    L.wpost[1].assign(weights + k, weights + k + npost[l]);
+    k += npost[l];
+  }
+  setup_coarse(ps, 1);
+  for (auto it = ps->graphs.begin(); it != ps->graphs.end();) {
+    if (it->first.prec == 1) {
+      cudaGraphExecDestroy(it->second);
+      ps->graph_kernels.erase(it->first);
+      it = ps->graphs.erase(it);
+    } else {
+      ++it;
+    }
+  }
   return GPW_OK;
 }

@@ -159,4 +159,136 @@ __global__ void __launch_bounds__(K2_TX* K2_TY) interpolate_k2_kernel(const Tran
   }
 }
 
+// ------------------------------------------------------------------ vector form
+// Interpolation with each thread owning 4 adjacent axis-2 outputs (16-byte
+// loads of `base` and stores of `out` for float32; two 16-byte accesses for
+// float64) and axis 0 split into chunks: the scalar kernel above keeps too
+// few bytes in flight per thread to reach HBM bandwidth on 127^3 grids.
+// Same expressions per output as interpolate_k2_kernel (bit-identical).
+// Needs out / base rows, planes and batch members 16-byte aligned; outputs
+// past the row end are never written.
+constexpr int K2V_TX = 32, K2V_TY = 8;
+
+template <typename S>
+__device__ __forceinline__ void ld4(const S* p, S (&v)[4], int nvalid) {
+  if (nvalid == 4) {
+    if constexpr (sizeof(S) == 4) {
+      const float4 t = *reinterpret_cast<const float4*>(p);
+      v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else {
+      const double2 t0 = reinterpret_cast<const double2*>(p)[0];
+      const double2 t1 = reinterpret_cast<const double2*>(p)[1];
+      v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = (k < nvalid) ? p[k] : S(0);
+  }
+}
+
+template <typename S>
+__device__ __forceinline__ void st4(S* p, const S (&v)[4], int nvalid) {
+  if (nvalid == 4) {
+    if constexpr (sizeof(S) == 4) {
+      *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+      reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+      reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < nvalid) p[k] = v[k];
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(K2V_TX* K2V_TY) interpolate_k2_vec_kernel(const TransferArgs a) {
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int o2 = 4 * (blockIdx.x * K2V_TX + threadIdx.x), o1 = blockIdx.y * K2V_TY + threadIdx.y;
+  if (o1 >= a.vout.n[1] || o2 >= a.vout.n[2]) return;
+  const int nvalid = min(4, a.vout.n[2] - o2);
+  const int O0s = chunk * a.zchunk, O0e = min(a.vout.n[0], O0s + a.zchunk);
+  const S* __restrict__ in = static_cast<const S*>(a.in) + (int64_t)b * a.vin.sb;
+  S* __restrict__ out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)o1 * a.vout.s1 + o2;
+  const S* __restrict__ base =
+      a.subtract ? static_cast<const S*>(a.base) + (int64_t)b * a.vbase.sb + (int64_t)o1 * a.vbase.s1 + o2
+                 : nullptr;
+  const int t1 = o1 + a.skip0[1], t2 = o2 + a.skip0[2];
+  const int u1 = (t1 >> 1) - a.pad0[1], e1 = t1 & 1;
+  const int u2 = (t2 >> 1) - a.pad0[2], e2 = t2 & 1;
+  // the 4 outputs need coarse axis-2 points u2 .. u2+2 on rows u1 (and u1+1)
+  int64_t off[2][3];
+  bool ok[2][3];
+#pragma unroll
+  for (int d1 = 0; d1 < 2; ++d1) {
+    int64_t q1, q2;
+    const bool v1 = k2_axis(u1 + d1, a.vin.n[1], a.bc.periodic[1], a.vin.s1, q1);
+#pragma unroll
+    for (int d2 = 0; d2 < 3; ++d2) {
+      const bool v2 = k2_axis(u2 + d2, a.vin.n[2], a.bc.periodic[2], 1, q2);
+      off[d1][d2] = q1 + q2;
+      ok[d1][d2] = v1 && v2;
+    }
+  }
+  auto Y = [&](int u0, S (&y)[4]) {
+    int64_t q0;
+    const bool v0 = k2_axis(u0, a.vin.n[0], a.bc.periodic[0], a.vin.s0, q0);
+    const S* pl = in + q0;
+    S c[2][3];
+#pragma unroll
+    for (int d2 = 0; d2 < 3; ++d2) {
+      c[0][d2] = k2_ld(pl + off[0][d2], v0 && ok[0][d2]);
+      c[1][d2] = e1 ? k2_ld(pl + off[1][d2], v0 && ok[1][d2]) : S(0);
+    }
+    // axis-2 pass per row: output k takes coarse point (e2 + k) / 2, or the
+    // midpoint with the next one when e2 + k is odd
+    S z[2][4];
+#pragma unroll
+    for (int d1 = 0; d1 < 2; ++d1) {
+      const S m01 = i2h(c[d1][0], c[d1][1]), m12 = i2h(c[d1][1], c[d1][2]);
+      z[d1][0] = e2 ? m01 : c[d1][0];
+      z[d1][1] = e2 ? c[d1][1] : m01;
+      z[d1][2] = e2 ? m12 : c[d1][1];
+      z[d1][3] = e2 ? c[d1][2] : m12;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) y[k] = e1 ? i2h(z[0][k], z[1][k]) : z[0][k];
+  };
+  const int us = ((O0s + a.skip0[0]) >> 1) - a.pad0[0];
+  const int ue = ((O0e - 1 + a.skip0[0]) >> 1) - a.pad0[0];
+  S ya[4], yb[4], v[4], bv[4];
+  Y(us, ya);
+#pragma unroll 2
+  for (int u = us; u <= ue; ++u) {
+    Y(u + 1, yb);
+    const int oe = 2 * (u + a.pad0[0]) - a.skip0[0];
+    if (oe >= O0s && oe < O0e) {
+      if (a.subtract) {
+        ld4(base + (int64_t)oe * a.vbase.s0, bv, nvalid);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = bv[k] - ya[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = ya[k];
+      }
+      st4(out + (int64_t)oe * a.vout.s0, v, nvalid);
+    }
+    if (oe + 1 >= O0s && oe + 1 < O0e) {
+      if (a.subtract) {
+        ld4(base + (int64_t)(oe + 1) * a.vbase.s0, bv, nvalid);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = bv[k] - i2h(ya[k], yb[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = i2h(ya[k], yb[k]);
+      }
+      st4(out + (int64_t)(oe + 1) * a.vout.s0, v, nvalid);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ya[k] = yb[k];
+  }
+}
+
 }  // namespace gpw

@@ -11,6 +11,9 @@ convergence loop run on the device in libgpwgrid.so (``gpw_poisson_*``).
 Two options go beyond the reference:
   precision='fp32'  float32 V-cycles inside a float64 defect-correction loop
                     (float64 residual, update, charge integral and norms);
+                    the inner cycles use Chebyshev-weighted Jacobi smoothing
+                    (``inner='chebyshev'``, see ``inner_schedule``) or the
+                    reference's schedule (``inner='reference'``);
   solve_batch()     many independent same-grid solves in one batched launch
                     sequence, each with its own convergence test.
 """
@@ -49,10 +52,81 @@ def PoissonSolver(dipolelayer=None, **kwargs):
 _PREC = {'fp64': 0, 'fp32': 1}
 
 
+def jacobi_spectrum(op, lowest=False):
+    """Extreme eigenvalue of D^-1 A for a constant-coefficient stencil.
+
+    The symbol of the stencil, sum_p c_p cos(o_p . theta), divided by the
+    centre coefficient, sampled on the grid's own Fourier modes (zero
+    boundary: theta = pi k / (n + 1), k = 1..n; periodic: 2 pi k / n).
+    Returns the largest value, or with ``lowest`` the smallest non-zero one.
+    """
+    n_c = op.gd.n_c
+    axes = []
+    for c in range(3):
+        n = int(n_c[c])
+        if op.gd.pbc_c[c]:
+            axes.append(2 * np.pi * np.arange(n) / n)
+        else:
+            axes.append(np.pi * np.arange(1, n + 1) / (n + 1))
+    # the symbol is a sum of per-axis terms for star stencils; sample at
+    # most 64 modes per axis (it is smooth in theta)
+    axes = [a if len(a) <= 64 else
+            np.unique(np.concatenate([a[::max(1, len(a) // 64)], a[-1:],
+                                      a[:1]])) for a in axes]
+    t0, t1, t2 = np.meshgrid(*axes, indexing='ij')
+    c0 = None
+    sym = 0.0
+    for coef, o in zip(op.coef_p, op.offset_pc):
+        if not o.any():
+            c0 = coef if c0 is None else c0 + coef
+        sym = sym + coef * np.cos(o[0] * t0 + o[1] * t1 + o[2] * t2)
+    lam = sym / c0
+    if lowest:
+        nz = lam[lam > 1e-12 * lam.max()]
+        return float(nz.min())
+    return float(lam.max())
+
+
+def chebyshev_weights(k, lo, hi):
+    """Jacobi weights whose product of (1 - w_i lambda) is the degree-k
+    Chebyshev polynomial of [lo, hi], smallest weight first."""
+    return [2.0 / ((hi + lo) + (hi - lo) * np.cos((2 * i - 1) * np.pi /
+                                                   (2 * k)))
+            for i in range(1, k + 1)]
+
+
+def inner_schedule(operators, fine=(2, 6.0), coarse=(3, 4.0), coarsest=8):
+    """Float32 inner V-cycle schedule of the defect-correction form.
+
+    Level 0: ``fine[0]`` pre- and post-sweeps with Chebyshev weights damping
+    the modes with lambda(D^-1 A) in [lambda_max / fine[1], lambda_max];
+    coarse levels likewise with ``coarse``; the coarsest level ``coarsest``
+    post-sweeps over its whole non-zero spectrum.  Returns (npre, npost,
+    weights) in the layout of gpw_poisson_set_inner_schedule.
+    """
+    npre, npost, weights = [], [], []
+    L = len(operators)
+    for l, op in enumerate(operators):
+        hi = jacobi_spectrum(op)
+        if l == L - 1:
+            lo = min(jacobi_spectrum(op, lowest=True), hi)
+            w = chebyshev_weights(coarsest, lo, hi)
+            npre.append(0)
+            npost.append(coarsest)
+            weights.extend(w)
+            continue
+        k, ratio = fine if l == 0 else coarse
+        w = chebyshev_weights(k, hi / ratio, hi)
+        npre.append(k)
+        npost.append(k)
+        weights.extend(w + w[::-1])
+    return npre, npost, weights
+
+
 class FDPoissonSolver:
     def __init__(self, nn=3, relax='J', eps=2e-10, maxiter=1000,
                  remove_moment=None, use_charge_center=False,
-                 precision='fp64', batch=1):
+                 precision='fp64', batch=1, inner='chebyshev'):
         self.relax = relax
         self.nn = nn
         self.eps = eps
@@ -69,6 +143,9 @@ class FDPoissonSolver:
         if precision not in _PREC:
             raise ValueError("precision must be 'fp64' or 'fp32'")
         self.precision = precision
+        if inner not in ('chebyshev', 'reference'):
+            raise ValueError("inner must be 'chebyshev' or 'reference'")
+        self.inner = inner
         self.batch = int(batch)
         self.description = None
         self._engine = None
@@ -170,6 +247,14 @@ class FDPoissonSolver:
                                        int(nbatch), ctypes.byref(h)))
         self._engine = (h, int(nbatch))
         self._lib = lib
+        if (self.precision == 'fp32' and self.inner == 'chebyshev' and
+                self.relax_method == 2 and L > 1):
+            npre, npost, ws = inner_schedule(self.operators)
+            a_pre = (ctypes.c_int * L)(*npre)
+            a_post = (ctypes.c_int * L)(*npost)
+            a_w = (ctypes.c_double * len(ws))(*ws)
+            _lib.check(lib.gpw_poisson_set_inner_schedule(h, a_pre, a_post,
+                                                          a_w, len(ws)))
 
     def _free_engine(self):
         if self._engine is not None:

@@ -216,6 +216,19 @@ int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
                             int reps, double *ms_per_launch,
                             double *bytes_per_launch, gpw_stream stream);
 
+/* Inner V-cycle schedule of the float32 defect-correction form
+ * (precision 1; no counterpart in the reference, whose only schedule is the
+ * float64 one of gpaw/poisson.py:111-128, 191-192, which precision 0 keeps).
+ * Level l runs npre[l] pre- and npost[l] post-smoothing weighted-Jacobi
+ * sweeps, each with its own weight: `weights` lists, level by level,
+ * npre[l] pre-sweep weights then npost[l] post-sweep weights (nweights =
+ * the total).  The coarsest level runs only its post-sweeps.  Level 0 needs
+ * at least one sweep of each kind; at most 16 sweeps per level.  Default
+ * (never called): the reference schedule.                                   */
+int gpw_poisson_set_inner_schedule(gpw_poisson *ps, const int *npre,
+                                   const int *npost, const double *weights,
+                                   int nweights);
+
 void gpw_poisson_free(gpw_poisson *ps);
 
 #ifdef __cplusplus

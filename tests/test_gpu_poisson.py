@@ -147,3 +147,50 @@ def test_fp32_defect_correction(cuda):
     e32 = hartree(ogd, phi32, rho)
     assert abs(e64 - e32) < 1e-8
     assert n32 < 200
+
+
+def test_fp32_inner_schedules(cuda):
+    """Chebyshev-weighted inner cycles vs the reference schedule (float32
+    inner, float64 outer): both reach relative residual 1e-10 with E_H
+    within 1e-8 Ha of the float64 method; the Chebyshev schedule needs at
+    most about half the outer iterations."""
+    N = 64
+    rho, L = gaussian_density(N, 0.2, 8, 1)
+    gd, ogd, ps, ops = solvers(N, L, 0, nn=3, maxiter=200)
+    eps = 1e-20 * float(np.dot(rho.ravel(), rho.ravel())) * gd.dv
+    phi64 = gd.zeros()
+    n64 = ps.solve(phi64, rho, eps=eps)
+    e64 = hartree(ogd, phi64, rho)
+    counts = {}
+    for inner in ('chebyshev', 'reference'):
+        p = type(ps)(nn=3, maxiter=200, precision='fp32', inner=inner)
+        p.set_grid_descriptor(gd)
+        p.initialize()
+        phi = gd.zeros()
+        counts[inner] = p.solve(phi, rho, eps=eps)
+        assert p.last_errors[0] <= eps
+        assert abs(hartree(ogd, phi, rho) - e64) < 1e-8
+    assert abs(counts['reference'] - n64) <= 1
+    assert counts['chebyshev'] <= (n64 + 1) // 2 + 1, (counts, n64)
+
+
+def test_fp32_batch_equals_single(cuda):
+    N = 32
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    rhos = []
+    for s in range(3):
+        rho, L = gaussian_density(N, 0.2, 4 + 4 * s, 40 + s)
+        rhos.append(rho)
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    ps = PoissonSolver(nn=3, batch=3, precision='fp32', maxiter=100)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    eps = [1e-20 * float(np.dot(r.ravel(), r.ravel())) * gd.dv for r in rhos]
+    phib = np.zeros((3,) + tuple(gd.n_c))
+    nb = ps.solve_batch(phib, np.array(rhos), eps=eps)
+    for s in range(3):
+        phi = gd.zeros()
+        n = ps.solve_neutral(phi, rhos[s], eps=eps[s])
+        assert n == nb[s]
+        assert np.array_equal(phi, phib[s])

@@ -89,3 +89,35 @@ def test_interpolator_too_small_raises():
     gd = GridDescriptor((12, 8, 16), (3, 2, 4), 0)
     with pytest.raises(ValueError):
         Transformer(gd.coarsen(), gd, 3)
+
+
+def test_inner_schedule_layout():
+    """Float32 inner schedule: Chebyshev-weighted Jacobi sweeps whose error
+    polynomial prod(1 - w_i lambda) equals 1 / T_k on the damped range."""
+    from gpawdft_b200.poisson import (PoissonSolver, chebyshev_weights,
+                                      inner_schedule, jacobi_spectrum)
+    N = 64
+    gd = GridDescriptor((N,) * 3, (N * 0.4,) * 3, 0)
+    ps = PoissonSolver(nn=3, precision='fp32')
+    ps.set_grid_descriptor(gd)
+    npre, npost, ws = inner_schedule(ps.operators)
+    L = len(ps.operators)
+    assert npre == [2] + [3] * (L - 2) + [0]
+    assert npost == [2] + [3] * (L - 2) + [8]
+    assert len(ws) == sum(npre) + sum(npost)
+    assert all(w > 0 for w in ws)
+    # level 0: 19-point sixth-order Laplacian, lambda_max(D^-1 A) -> 2.2204
+    hi = jacobi_spectrum(ps.operators[0])
+    assert 2.21 < hi < 2.2205
+    # pre-sweeps smallest weight first, post-sweeps reversed
+    assert ws[:2] == sorted(ws[:2]) and ws[2:4] == ws[:2][::-1]
+    for k, ratio in ((2, 6.0), (3, 4.0)):
+        lo = hi / ratio
+        w = chebyshev_weights(k, lo, hi)
+        lam = np.linspace(lo, hi, 2001)
+        p = np.prod([1 - wi * lam for wi in w], axis=0)
+        x0 = (hi + lo) / (hi - lo)
+        tk = np.cosh(k * np.arccosh(x0))
+        assert np.abs(p).max() <= 1 / tk * (1 + 1e-9)
+    # the 1^3 coarsest grid: one exact sweep (D^-1 A = 1)
+    assert jacobi_spectrum(ps.operators[-1]) == pytest.approx(1.0)
