@@ -14,7 +14,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libgpwgrid.so')
-SOURCES = ['gpw_api.cu', 'gpw_launch.cu', 'gpw_poisson.cu', 'gpw_noalloc.cu']
+SOURCES = ['gpw_api.cu', 'gpw_launch.cu', 'gpw_poisson.cu', 'gpw_noalloc.cu',
+           'gpw_tma_f64.cu', 'gpw_tma_f32.cu']
 
 
 def nvcc_path():

@@ -34,7 +34,7 @@ constexpr int CG_THREADS = 512;  // threads per CTA
 struct CoarseLevel {
   int n[3];
   int periodic[3];
-  int pts;                // n0 * n1 * n2
+  int pts;                // elements per buffer: n0 n1 n2 (padded form: (n0+2)(n1+2)(n2+2))
   int base;               // element offset of the level's buffers: phi0, phi1, rho
   double cc;              // centre coefficient
   double cm[3], cp[3];    // neighbour coefficients at offsets -1 / +1 per axis
@@ -46,6 +46,7 @@ struct CoarseLevel {
 
 struct CoarseArgs {
   int nl;                 // levels in the kernel (lc .. L)
+  int padded;             // zero boundaries everywhere: padded layout (see below)
   CoarseLevel lv[CG_MAXL];
   const void* rho;        // rho of level lc, engine layout
   GridView vrho;
@@ -169,12 +170,197 @@ __device__ __forceinline__ void cg_interp_sub(const CoarseLevel& F, const S* bas
   __syncthreads();
 }
 
+// ---------------------------------------------------------------- padded form
+// When every level has zero boundaries, each level buffer is stored with a
+// one-point zero halo ((n0+2)(n1+2)(n2+2) elements, the halo never written):
+// neighbours sit at fixed offsets and need no bounds checks, and each thread
+// walks whole axis-0 columns by adding the plane stride, so no point pays an
+// index division.  `pts` then counts the padded elements.  The transfers
+// assume the zero-boundary K=2 tables: restriction pad 0 (fine centre
+// 2I + 1), interpolation pad 1 and skip 1 on every axis.
+struct PadGeom {
+  int n0, n1, n2;
+  int sy, sz;  // padded row and plane strides
+  __device__ __forceinline__ explicit PadGeom(const CoarseLevel& L)
+      : n0(L.n[0]), n1(L.n[1]), n2(L.n[2]), sy(L.n[2] + 2), sz((L.n[1] + 2) * (L.n[2] + 2)) {}
+  __device__ __forceinline__ int at(int i0, int i1, int i2) const { return (i0 + 1) * sz + (i1 + 1) * sy + i2 + 1; }
+};
+
 template <typename S>
-__global__ void __launch_bounds__(CG_THREADS) coarse_vcycle_kernel(const CoarseArgs a) {
+__device__ __forceinline__ void pg_jacobi(const CoarseLevel& L, const S* src, S* dst, const S* rho, double wd) {
+  const PadGeom g(L);
+  const S w = (S)wd, wc = w / (S)L.cc;
+  const S c0m = (S)L.cm[0], c0p = (S)L.cp[0], c1m = (S)L.cm[1], c1p = (S)L.cp[1], c2m = (S)L.cm[2],
+          c2p = (S)L.cp[2];
+  for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
+    const int i1 = c / g.n2, i2 = c - i1 * g.n2;
+    int k = g.at(0, i1, i2);
+    for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) {
+      S av = c2m * src[k - 1];
+      av = fmac(c2p, src[k + 1], av);
+      av = fmac(c1m, src[k - g.sy], av);
+      av = fmac(c1p, src[k + g.sy], av);
+      av = fmac(c0m, src[k - g.sz], av);
+      av = fmac(c0p, src[k + g.sz], av);
+      dst[k] = (S(1) - w) * src[k] + wc * (rho[k] - av);
+    }
+  }
+  __syncthreads();
+}
+
+template <typename S>
+__device__ __forceinline__ void pg_residual(const CoarseLevel& L, const S* phi, S* r, const S* rho) {
+  const PadGeom g(L);
+  const S c0m = (S)L.cm[0], c0p = (S)L.cp[0], c1m = (S)L.cm[1], c1p = (S)L.cp[1], c2m = (S)L.cm[2],
+          c2p = (S)L.cp[2], cc = (S)L.cc;
+  for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
+    const int i1 = c / g.n2, i2 = c - i1 * g.n2;
+    int k = g.at(0, i1, i2);
+    for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) {
+      S av = c2m * phi[k - 1];
+      av = fmac(c2p, phi[k + 1], av);
+      av = fmac(c1m, phi[k - g.sy], av);
+      av = fmac(c1p, phi[k + g.sy], av);
+      av = fmac(c0m, phi[k - g.sz], av);
+      av = fmac(c0p, phi[k + g.sz], av);
+      r[k] = fmac(cc, phi[k], av) - rho[k];
+    }
+  }
+  __syncthreads();
+}
+
+// rho_C = R r_F and phi_C = 0 (zero boundaries: fine centre 2I + 1)
+template <typename S>
+__device__ __forceinline__ void pg_restrict(const CoarseLevel& F, const S* r, const CoarseLevel& C, S* rho_c,
+                                            S* phi_c) {
+  const PadGeom f(F), g(C);
+  for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
+    const int I1 = c / g.n2, I2 = c - I1 * g.n2;
+    int k = g.at(0, I1, I2);
+    int kf = f.at(1, 2 * I1 + 1, 2 * I2 + 1);  // fine centre of I0 = 0
+    for (int I0 = 0; I0 < g.n0; ++I0, k += g.sz, kf += 2 * f.sz) {
+      S y[3];
+#pragma unroll
+      for (int d0 = 0; d0 < 3; ++d0) {
+        S z[3];
+#pragma unroll
+        for (int d1 = 0; d1 < 3; ++d1) {
+          const int q = kf + (d0 - 1) * f.sz + (d1 - 1) * f.sy;
+          z[d1] = r2(r[q - 1], r[q], r[q + 1]);
+        }
+        y[d0] = r2(z[0], z[1], z[2]);
+      }
+      rho_c[k] = r2(y[0], y[1], y[2]);
+      phi_c[k] = S(0);
+    }
+  }
+  __syncthreads();
+}
+
+// dst = base - I e_C (zero boundaries: skip0 = 1, pad0 = 1 on every axis)
+template <typename S>
+__device__ __forceinline__ S pg_interp_plane(const S* e, const PadGeom& g, int q, int e1, int e2) {
+  S z0 = e[q];
+  if (e2) z0 = i2h(z0, e[q + 1]);
+  if (!e1) return z0;
+  S z1 = e[q + g.sy];
+  if (e2) z1 = i2h(z1, e[q + g.sy + 1]);
+  return i2h(z0, z1);
+}
+
+template <typename S>
+__device__ __forceinline__ void pg_interp_sub(const CoarseLevel& F, const S* base, S* dst, const CoarseLevel& C,
+                                              const S* e) {
+  const PadGeom f(F), g(C);
+  for (int c = threadIdx.x; c < f.n1 * f.n2; c += blockDim.x) {
+    const int o1 = c / f.n2, o2 = c - o1 * f.n2;
+    // t = o + 1; coarse u = t / 2 - 1 (padded index u + 1 = t / 2), e = t & 1
+    const int t1 = o1 + 1, t2 = o2 + 1;
+    const int e1 = t1 & 1, e2 = t2 & 1;
+    const int qc = (t1 >> 1) * g.sy + (t2 >> 1);  // padded in-plane coarse index
+    int k = f.at(0, o1, o2);
+    for (int o0 = 0; o0 < f.n0; ++o0, k += f.sz) {
+      const int t0 = o0 + 1;
+      const int q = (t0 >> 1) * g.sz + qc;
+      S v = pg_interp_plane(e, g, q, e1, e2);
+      if (t0 & 1) v = i2h(v, pg_interp_plane(e, g, q + g.sz, e1, e2));
+      dst[k] = base[k] - v;
+    }
+  }
+  __syncthreads();
+}
+
+template <typename S>
+__device__ void coarse_vcycle_padded(const CoarseArgs& a, S* sm, int b) {
+  const int nl = a.nl;
+  int cur[CG_MAXL];
+  // zero every buffer once (the halos stay zero), then load rho of level 0
+  int total = 0;
+  for (int l = 0; l < nl; ++l) total = max(total, a.lv[l].base + 3 * a.lv[l].pts);
+  for (int i = threadIdx.x; i < total; i += blockDim.x) sm[i] = S(0);
+  __syncthreads();
+  {
+    const CoarseLevel& L = a.lv[0];
+    const PadGeom g(L);
+    S* rho = sm + L.base + 2 * L.pts;
+    const S* gr = static_cast<const S*>(a.rho) + (int64_t)b * a.vrho.sb;
+    for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
+      const int i1 = c / g.n2, i2 = c - i1 * g.n2;
+      int k = g.at(0, i1, i2);
+      for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) rho[k] = gr[(int64_t)i0 * a.vrho.s0 + (int64_t)i1 * a.vrho.s1 + i2];
+    }
+    __syncthreads();
+  }
+  for (int l = 0; l < nl; ++l) {
+    const CoarseLevel& L = a.lv[l];
+    S* P[2] = {sm + L.base, sm + L.base + L.pts};
+    const S* rho = sm + L.base + 2 * L.pts;
+    int c = 0;
+    if (l == nl - 1) {
+      for (int s = 0; s < L.npost; ++s, c = 1 - c) pg_jacobi(L, P[c], P[1 - c], rho, L.w[L.npre + s]);
+      cur[l] = c;
+      break;
+    }
+    for (int s = 0; s < L.npre; ++s, c = 1 - c) pg_jacobi(L, P[c], P[1 - c], rho, L.w[s]);
+    cur[l] = c;
+    pg_residual(L, P[c], P[1 - c], rho);
+    const CoarseLevel& C = a.lv[l + 1];
+    pg_restrict(L, P[1 - c], C, sm + C.base + 2 * C.pts, sm + C.base);
+  }
+  for (int l = nl - 2; l >= 0; --l) {
+    const CoarseLevel& L = a.lv[l];
+    const CoarseLevel& C = a.lv[l + 1];
+    S* P[2] = {sm + L.base, sm + L.base + L.pts};
+    const S* rho = sm + L.base + 2 * L.pts;
+    int c = cur[l];
+    pg_interp_sub(L, P[c], P[1 - c], C, sm + C.base + cur[l + 1] * C.pts);
+    c = 1 - c;
+    for (int s = 0; s < L.npost; ++s, c = 1 - c) pg_jacobi(L, P[c], P[1 - c], rho, L.w[L.npre + s]);
+    cur[l] = c;
+  }
+  {
+    const CoarseLevel& L = a.lv[0];
+    const PadGeom g(L);
+    const S* phi = sm + L.base + cur[0] * L.pts;
+    S* gp = static_cast<S*>(a.phi) + (int64_t)b * a.vphi.sb;
+    for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
+      const int i1 = c / g.n2, i2 = c - i1 * g.n2;
+      int k = g.at(0, i1, i2);
+      for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) gp[(int64_t)i0 * a.vphi.s0 + (int64_t)i1 * a.vphi.s1 + i2] = phi[k];
+    }
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(CG_THREADS, 1) coarse_vcycle_kernel(const CoarseArgs a) {
   const int b = blockIdx.x;
   if (a.active && !a.active[b]) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S* sm = reinterpret_cast<S*>(smem_raw);
+  if (a.padded) {
+    coarse_vcycle_padded(a, sm, b);
+    return;
+  }
   const int nl = a.nl;
   int cur[CG_MAXL];
   {

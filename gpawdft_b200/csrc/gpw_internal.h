@@ -1,6 +1,8 @@
 // Host-side internal interfaces shared by the C ABI (gpw_api.cu), the kernel
 // launchers (gpw_launch.cu) and the multigrid engine (gpw_poisson.cu).
 #pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -106,10 +108,50 @@ struct TrDesc {
 };
 
 // subtract != 0 (interpolation only): out = base - I(in); base may alias out.
+// sweep (K=2 real restriction only, see restrict_sweep_ok): also write the
+// first weighted-Jacobi sweep of the coarse level from phi = 0,
+// sweep->phi = (w / c0) out.
+struct RestrictSweep {
+  void* phi;
+  double w, c0;
+};
+bool restrict_sweep_ok(const TrDesc& d, int dtype);
 cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const GridView& vin, void* out,
                             const GridView& vout, int nbatch, const Boundary& bc, int subtract,
                             const void* base, const GridView* vbase, const unsigned char* active,
-                            cudaStream_t st);
+                            cudaStream_t st, const RestrictSweep* sweep = nullptr);
+
+// ---------------------------------------------------------------- TMA stencils
+// The TMA star-stencil path (gpw_star_tma.cuh): real zero-boundary star
+// stencils on 16-byte aligned, 16-byte pitched grids.  Launches pick a tile
+// variant and an axis-0 chunk count from the autotuner's cache (defaults
+// when the shape was never tuned).
+struct TmaChoice {
+  int var;     // tile variant (gpw_star_tma.cuh)
+  int nchunk;  // axis-0 chunks; <= 0: wave model
+};
+cudaError_t tma_stencil_f64(int mode, int R, int var, const StencilArgs& a, int nbatch, const StarCoefs& sc,
+                            int nchunk, cudaStream_t st);
+cudaError_t tma_stencil_f32(int mode, int R, int var, const StencilArgs& a, int nbatch, const StarCoefs& sc,
+                            int nchunk, cudaStream_t st);
+// Time the candidate (variant, chunking) choices of one stencil launch on
+// the given buffers (their contents are overwritten) and keep the fastest
+// for every later launch of the same shape.  Not allowed during capture.
+// mode MODE_RESID_DC / MODE_JACOBI_ADD64 take the launch_stencil_dc arguments.
+cudaError_t tune_stencil(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, void* out,
+                         const GridView& vout, const void* rho, const GridView& vrho, void* out2, int nbatch,
+                         double w, const GridSum& gs, cudaStream_t st);
+// Number of stencil choices tuned so far (the cache size).
+int tuned_stencil_count();
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
+// Dynamic shared memory above 48 KB needs a one-time opt-in per kernel.
+template <typename F>
+inline cudaError_t smem_optin_bytes(F* kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 
 // ---------------------------------------------------------------- coarse levels
 // The coarse end of a V-cycle in one CTA per batch member (gpw_coarse.cuh);

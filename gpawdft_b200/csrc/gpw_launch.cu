@@ -1,6 +1,7 @@
 // Kernel launchers: dtype / radius / tap-count dispatch, launch geometry and
 // shared-memory opt-in for every device kernel of the library.
 #include <algorithm>
+#include <map>
 #include <mutex>
 
 #include <cudaTypedefs.h>
@@ -8,7 +9,6 @@
 #include "gpw_blas.cuh"
 #include "gpw_coarse.cuh"
 #include "gpw_internal.h"
-#include "gpw_star_tma.cuh"
 #include "gpw_stencil.cuh"
 #include "gpw_transfer.cuh"
 #include "gpw_transfer_k2.cuh"
@@ -127,18 +127,16 @@ int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& v, int 
   int zc, nc;
   choose_chunks(v.n[0], (int64_t)gx * gy * nbatch, minz, zc, nc);
   int nblk = gx * gy * nc;
-  if (use_star) {  // the TMA tile (64 x 16, 4R+4 minimum chunk) may be chosen instead
-    // smallest TMA tile of any epilogue: an upper bound on the CTA count
-    constexpr int TTY = TmaCfg<double, 1, MODE_APPLY>::TY, TTZ = TmaCfg<double, 1, MODE_APPLY>::TZ;
-    const int tx2 = (v.n[2] + TTZ - 1) / TTZ, ty2 = (v.n[1] + TTY - 1) / TTY;
-    choose_chunks(v.n[0], (int64_t)tx2 * ty2 * nbatch, 4 * d.R + 4, zc, nc);
-    nblk = std::max(nblk, tx2 * ty2 * nc);
+  if (use_star) {  // a TMA tile variant may be chosen instead: bound its CTA count
+    // (tiles of at least 64 x 8 points, at most n0 / (2R + 2) axis-0 chunks)
+    const int tx2 = (v.n[2] + 63) / 64, ty2 = (v.n[1] + 7) / 8;
+    nblk = std::max(nblk, tx2 * ty2 * std::max(1, v.n[0] / (2 * d.R + 2)));
   }
   return nblk;
 }
 
 // ------------------------------------------------------------------ TMA path
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
   std::call_once(once, [] {
@@ -172,48 +170,45 @@ static bool view_tma_ok(const GridView& v, size_t es, int nbatch) {
   return true;
 }
 
-template <typename S, int R, int MODE>
-static cudaError_t run_star_tma(const StencilArgs& a0, int nbatch, const StarCoefs& sc, cudaStream_t st) {
-  using C = TmaCfg<S, R, MODE>;
-  auto enc = tensor_map_encoder();
-  if (!enc) return cudaErrorNotSupported;
-  StencilArgs a = a0;
-  const GridView& vi = a.vin;
-  CUtensorMap map;
-  cuuint64_t dims[4] = {(cuuint64_t)vi.n[2], (cuuint64_t)vi.n[1], (cuuint64_t)vi.n[0], (cuuint64_t)nbatch};
-  cuuint64_t strides[3] = {(cuuint64_t)(vi.s1 * sizeof(S)), (cuuint64_t)(vi.s0 * sizeof(S)),
-                           (cuuint64_t)(std::max<int64_t>(vi.sb, vi.s0 * vi.n[0]) * sizeof(S))};
-  cuuint32_t box[4] = {(cuuint32_t)C::W, (cuuint32_t)C::H, 1, 1};
-  cuuint32_t estr[4] = {1, 1, 1, 1};
-  CUresult r = enc(&map, sizeof(S) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
-                   const_cast<void*>(a.in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
-  const GridView& v = a.vout;
-  dim3 grid((v.n[2] + C::TZ - 1) / C::TZ, (v.n[1] + C::TY - 1) / C::TY, 1);
-  choose_chunks(v.n[0], (int64_t)grid.x * grid.y * nbatch, 4 * R + 4, a.zchunk, a.nchunk);
-  grid.z = a.nchunk * nbatch;
-  a.nblk_seg = grid.x * grid.y * a.nchunk;
-  TmaArgs ta{a, device_status_word()};
-  auto kern = star_tma_kernel<S, R, MODE>;
-  static std::once_flag once;
-  cudaError_t e = cudaSuccess;
-  std::call_once(once, [&] { e = smem_optin(kern, C::smem); });
-  if (e != cudaSuccess) return e;
-  kern<<<grid, dim3(C::NTX, C::NTY), C::smem, st>>>(map, ta, sc);
-  return cudaGetLastError();
+// ------------------------------------------------------------------ TMA autotuner
+// Per launch shape (dtype, radius, epilogue, grid extent, batch) the tile
+// variant and axis-0 chunking that ran fastest when the shape was tuned;
+// untuned shapes use variant 2 and the wave model.
+namespace {
+struct TuneKey {
+  int dtype, R, mode, n0, n1, n2, nbatch;
+  bool operator<(const TuneKey& o) const {
+    const int a[7] = {dtype, R, mode, n0, n1, n2, nbatch}, b[7] = {o.dtype, o.R, o.mode, o.n0, o.n1, o.n2, o.nbatch};
+    for (int i = 0; i < 7; ++i)
+      if (a[i] != b[i]) return a[i] < b[i];
+    return false;
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TmaChoice> g_tune;
+}  // namespace
+
+static TmaChoice tma_choice(int dtype, int R, int mode, const GridView& v, int nbatch) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tune.find(TuneKey{dtype, R, mode, v.n[0], v.n[1], v.n[2], nbatch});
+  if (it != g_tune.end()) return it->second;
+  return TmaChoice{R == 4 ? 1 : 2, 0};
 }
 
-template <typename S, int MODE>
-static cudaError_t dispatch_star_tma(const StencilArgs& a, const OpDesc& d, int nbatch, cudaStream_t st) {
-  switch (d.R) {
-    case 1: return run_star_tma<S, 1, MODE>(a, nbatch, d.sc, st);
-    case 2: return run_star_tma<S, 2, MODE>(a, nbatch, d.sc, st);
-    case 3: return run_star_tma<S, 3, MODE>(a, nbatch, d.sc, st);
-    case 4: return run_star_tma<S, 4, MODE>(a, nbatch, d.sc, st);
-  }
-  return cudaErrorInvalidValue;
+static bool tma_tuned(int dtype, int R, int mode, const GridView& v, int nbatch) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  return g_tune.count(TuneKey{dtype, R, mode, v.n[0], v.n[1], v.n[2], nbatch}) != 0;
+}
+
+static cudaError_t tma_launch(int dtype, int mode, int R, const TmaChoice& ch, const StencilArgs& a, int nbatch,
+                              const StarCoefs& sc, cudaStream_t st) {
+  if (dtype == GPW_F64) return tma_stencil_f64(mode, R, ch.var, a, nbatch, sc, ch.nchunk, st);
+  return tma_stencil_f32(mode, R, ch.var, a, nbatch, sc, ch.nchunk, st);
+}
+
+int tuned_stencil_count() {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  return (int)g_tune.size();
 }
 
 // The TMA path serves real zero-boundary star stencils whose arrays are
@@ -250,19 +245,18 @@ cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in,
   a.active = active;
   a.gsum = gs;
   if (tma_path_ok(d, dtype, mode, in, vin, out, vout, rho, vrho, nbatch)) {
-    if (dtype == GPW_F64) {
-      switch (mode) {
-        case MODE_APPLY: return dispatch_star_tma<double, MODE_APPLY>(a, d, nbatch, st);
-        case MODE_RESIDUAL: return dispatch_star_tma<double, MODE_RESIDUAL>(a, d, nbatch, st);
-        case MODE_JACOBI: return dispatch_star_tma<double, MODE_JACOBI>(a, d, nbatch, st);
-      }
-    } else {
-      switch (mode) {
-        case MODE_APPLY: return dispatch_star_tma<float, MODE_APPLY>(a, d, nbatch, st);
-        case MODE_RESIDUAL: return dispatch_star_tma<float, MODE_RESIDUAL>(a, d, nbatch, st);
-        case MODE_JACOBI: return dispatch_star_tma<float, MODE_JACOBI>(a, d, nbatch, st);
+    // first launch of an untuned shape outside stream capture: tune it now
+    // (apply / residual / Jacobi recompute their output from inputs they do
+    // not overwrite, so the timed repetitions leave the same result)
+    if (!active && out != rho && !tma_tuned(dtype, d.R, mode, vout, nbatch)) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+        cudaError_t te = tune_stencil(d, dtype, mode, in, vin, out, vout, rho, vrho, nullptr, nbatch, w, gs, st);
+        if (te != cudaSuccess) return te;
       }
     }
+    const TmaChoice ch = tma_choice(dtype, d.R, mode, vout, nbatch);
+    return tma_launch(dtype, mode, d.R, ch, a, nbatch, d.sc, st);
   }
   OpDesc dd = d;
   if (!star_radius_ok(dd.R)) {
@@ -318,9 +312,81 @@ cudaError_t launch_stencil_dc(const OpDesc& d, int mode, const void* in, const G
   a.c0 = d.coefs[0];
   a.active = active;
   a.gsum = gs;
-  if (mode == MODE_RESID_DC) return dispatch_star_tma<double, MODE_RESID_DC>(a, d, nbatch, st);
-  if (mode == MODE_JACOBI_ADD64) return dispatch_star_tma<float, MODE_JACOBI_ADD64>(a, d, nbatch, st);
-  return cudaErrorInvalidValue;
+  if (mode != MODE_RESID_DC && mode != MODE_JACOBI_ADD64) return cudaErrorInvalidValue;
+  const int dtype = (mode == MODE_RESID_DC) ? GPW_F64 : GPW_F32;
+  const TmaChoice ch = tma_choice(dtype, d.R, mode, v, nbatch);
+  return tma_launch(dtype, mode, d.R, ch, a, nbatch, d.sc, st);
+}
+
+cudaError_t tune_stencil(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, void* out,
+                         const GridView& vout, const void* rho, const GridView& vrho, void* out2, int nbatch,
+                         double w, const GridSum& gs, cudaStream_t st) {
+  StencilArgs a{};
+  a.in = in;
+  a.out = out;
+  a.out2 = out2;
+  a.rho = rho;
+  a.vin = vin;
+  a.vout = vout;
+  a.vrho = vrho;
+  a.w = w;
+  a.w2 = w;
+  a.c0 = d.coefs.empty() ? 1.0 : d.coefs[0];
+  a.gsum = gs;
+  int ldtype = dtype;
+  if (mode == MODE_RESID_DC || mode == MODE_JACOBI_ADD64) {
+    const size_t es_in = (mode == MODE_RESID_DC) ? 8 : 4;
+    if (!dc_fusable(d) || !aligned16(in) || !aligned16(rho) || !aligned16(out2) || (out && !aligned16(out)) ||
+        !view_tma_ok(vout, es_in, nbatch) || !view_tma_ok(vout, 4, nbatch))
+      return cudaSuccess;
+    ldtype = (mode == MODE_RESID_DC) ? GPW_F64 : GPW_F32;
+    a.vin = a.vrho = vout;
+  } else if (!tma_path_ok(d, dtype, mode, in, vin, out, vout, rho, vrho, nbatch)) {
+    return cudaSuccess;  // not the TMA path: nothing to tune
+  }
+  const TuneKey key{ldtype, d.R, mode, vout.n[0], vout.n[1], vout.n[2], nbatch};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    if (g_tune.count(key)) return cudaSuccess;
+  }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return cudaGetLastError();
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cudaGetLastError();
+  }
+  TmaChoice best{d.R == 4 ? 1 : 2, 0};
+  float best_ms = 1e30f;
+  for (int var = 0; var < TMA_NVARIANT; ++var) {
+    for (int nc : {0, -2}) {
+      const TmaChoice ch{var, nc};
+      cudaError_t e = tma_launch(ldtype, mode, d.R, ch, a, nbatch, d.sc, st);
+      if (e != cudaSuccess) {
+        cudaGetLastError();  // a variant this shape cannot launch: skip it
+        continue;
+      }
+      const int reps = 3;
+      cudaEventRecord(e0, st);
+      for (int i = 0; i < reps && e == cudaSuccess; ++i) e = tma_launch(ldtype, mode, d.R, ch, a, nbatch, d.sc, st);
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess || e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return e != cudaSuccess ? e : cudaGetLastError();
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = ch;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune[key] = best;
+  return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ transfers
@@ -408,16 +474,35 @@ cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatc
 static bool k2_vec_ok(const TransferArgs& a) {
   auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
   auto view_ok = [](const GridView& v) { return v.s1 % 4 == 0 && v.s0 % 4 == 0 && v.sb % 4 == 0; };
-  if (a.vout.n[2] < 8) return false;
+  // a warp covers 128 outputs: narrower rows leave lanes idle
+  if (a.vout.n[2] < 96) return false;
   if (!aligned(a.out) || !view_ok(a.vout)) return false;
   if (a.subtract && (!aligned(a.base) || !view_ok(a.vbase))) return false;
+  return true;
+}
+
+bool restrict_sweep_ok(const TrDesc& d, int dtype) {
+  return d.k == 2 && !d.interpolate && (dtype == GPW_F64 || dtype == GPW_F32);
+}
+
+// The vector restriction needs zero boundaries and pad 0 along axis 2 (fine
+// taps 2 I2 .. 2 I2 + 8 start 16-byte aligned) and aligned input rows.
+static bool k2r_vec_ok(const TransferArgs& a) {
+  auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+  auto view_ok = [](const GridView& v) { return v.s1 % 4 == 0 && v.s0 % 4 == 0 && v.sb % 4 == 0; };
+  // a warp covers 64 outputs: narrower rows leave lanes idle (the scalar
+  // kernel's 32-wide rows serve them better)
+  if (a.bc.periodic[2] || a.pad0[2] != 0 || a.vout.n[2] < 48) return false;
+  if (!aligned(a.in) || !view_ok(a.vin)) return false;
+  if (!aligned(a.out) || !view_ok(a.vout)) return false;
+  if (a.out2 && !aligned(a.out2)) return false;
   return true;
 }
 
 cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const GridView& vin, void* out,
                             const GridView& vout, int nbatch, const Boundary& bc, int subtract,
                             const void* base, const GridView* vbase, const unsigned char* active,
-                            cudaStream_t st) {
+                            cudaStream_t st, const RestrictSweep* sweep) {
   TransferArgs a{};
   a.in = in;
   a.out = out;
@@ -433,6 +518,29 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
   a.base = base;
   if (vbase) a.vbase = *vbase;
   const bool interp = d.interpolate != 0;
+  if (sweep) {
+    if (!restrict_sweep_ok(d, dtype)) return cudaErrorInvalidValue;
+    a.out2 = sweep->phi;
+    a.w2 = sweep->w;
+    a.c02 = sweep->c0;
+  }
+  if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32) && !interp && k2r_vec_ok(a)) {
+    dim3 grid((vout.n[2] + 2 * K2V_TX - 1) / (2 * K2V_TX), (vout.n[1] + K2V_TY - 1) / K2V_TY, 1);
+    // ~8 CTAs of 256 threads per SM; chunks of at least 4 output planes
+    const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
+    const int64_t want = 8LL * num_sms();
+    int64_t nc = std::max<int64_t>(1, (want + tiles - 1) / tiles);
+    nc = std::min<int64_t>(nc, std::max(1, vout.n[0] / 4));
+    a.zchunk = (int)((vout.n[0] + nc - 1) / nc);
+    a.nchunk = (vout.n[0] + a.zchunk - 1) / a.zchunk;
+    grid.z = a.nchunk * nbatch;
+    const dim3 blk(K2V_TX, K2V_TY);
+    if (dtype == GPW_F64)
+      restrict_k2_vec_kernel<double><<<grid, blk, 0, st>>>(a);
+    else
+      restrict_k2_vec_kernel<float><<<grid, blk, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32) && interp && k2_vec_ok(a)) {
     dim3 grid((vout.n[2] + 4 * K2V_TX - 1) / (4 * K2V_TX), (vout.n[1] + K2V_TY - 1) / K2V_TY, 1);
     // ~8 CTAs of 256 threads per SM; chunks of at least 8 output planes

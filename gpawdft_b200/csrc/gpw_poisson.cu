@@ -122,9 +122,28 @@ struct Rec {
   int nb;
   cudaStream_t st;
   const unsigned char* active;
+  bool tune = false;  // tuning pass: time the stencil launches' variants, launch nothing else
   cudaError_t err = cudaSuccess;
   void ok(cudaError_t e) {
     if (err == cudaSuccess && e != cudaSuccess) err = e;
+  }
+  // one star / general stencil launch (or, in the tuning pass, its tuning)
+  void stencil(const OpDesc& d, int dt, int mode, const void* in, void* out, const void* rho, const GridView& v,
+               double w, const GridSum& gs) {
+    if (tune)
+      ok(tune_stencil(d, dt, mode, in, v, out, v, rho, v, nullptr, nb, w, gs, st));
+    else
+      ok(launch_stencil(d, dt, mode, in, v, out, v, rho, v, nb, make_boundary(d.periodic, dt, nullptr), w, active,
+                        gs, st));
+  }
+  // one fused defect-correction stencil launch (or its tuning)
+  void stencil_dc(const OpDesc& d, int mode, const void* in, const GridView& v, void* out, void* out2,
+                  const void* rho, double w, double w2, const GridSum& gs) {
+    if (tune)
+      ok(tune_stencil(d, mode == MODE_RESID_DC ? GPW_F64 : GPW_F32, mode, in, v, out, v, rho, v, out2, nb,
+                      mode == MODE_RESID_DC ? w2 : w, gs, st));
+    else
+      ok(launch_stencil_dc(d, mode, in, v, out, out2, rho, nb, w, w2, active, gs, st));
   }
 };
 
@@ -133,11 +152,11 @@ struct Rec {
 int rec_relax(Rec& r, int l, int cur, const double* ws, int nsweeps, bool f32) {
   Level& L = r.ps->lv[l];
   const int dt = f32 ? GPW_F32 : GPW_F64;
-  Boundary bc = make_boundary(L.op->periodic, dt, nullptr);
-  GridSum gs{};
   Workspace* phi = f32 ? L.phi32 : L.phi;
   const void* rho = f32 ? L.rho32.ptr : L.rho.ptr;
   if (r.ps->relax_method == 1) {
+    if (r.tune) return cur;
+    Boundary bc = make_boundary(L.op->periodic, dt, nullptr);
     for (int b = 0; b < r.nb; ++b) {
       const size_t es = elt_size(dt) * (size_t)L.v.sb;
       r.ok(launch_relax_gs_ws(*L.op, dt, (char*)phi[cur].ptr + b * es, L.v, (const char*)rho + b * es, L.v,
@@ -146,36 +165,32 @@ int rec_relax(Rec& r, int l, int cur, const double* ws, int nsweeps, bool f32) {
     return cur;
   }
   for (int s = 0; s < nsweeps; ++s) {
-    r.ok(launch_stencil(*L.op, dt, MODE_JACOBI, phi[cur].ptr, L.v, phi[1 - cur].ptr, L.v, rho, L.v, r.nb, bc, ws[s],
-                        r.active, gs, r.st));
+    r.stencil(*L.op, dt, MODE_JACOBI, phi[cur].ptr, phi[1 - cur].ptr, rho, L.v, ws[s], GridSum{});
     cur = 1 - cur;
   }
   return cur;
 }
 
-// Records iterate2(level l) starting from phi buffer `cur`; returns the buffer
-// holding phi_l afterwards.
-int rec_vcycle(Rec& r, int l, int cur, bool f32) {
+// Levels l+1 .. L of form p, from the level-l residual `res`: restriction
+// into rho_{l+1}, then the coarse one-CTA kernel when l+1 is its first level,
+// else the recursive V-cycle from phi_{l+1} = 0, whose first weighted-Jacobi
+// sweep ((w / c0) rho_{l+1}, exactly) the restriction writes alongside.
+// Returns the buffer holding phi_{l+1}.
+int rec_vcycle(Rec& r, int l, int cur, bool f32, bool first_done = false);
+int rec_lower(Rec& r, int l, const void* res, bool f32) {
   gpw_poisson* ps = r.ps;
   const int nl = (int)ps->lv.size();
-  Level& L = ps->lv[l];
-  const int dt = f32 ? GPW_F32 : GPW_F64;
-  Workspace* phi = f32 ? L.phi32 : L.phi;
-  Workspace& rho = f32 ? L.rho32 : L.rho;
-  Workspace& res = f32 ? L.res32 : L.res;
-  Boundary bc = make_boundary(L.op->periodic, dt, nullptr);
   const int p = f32 ? 1 : 0;
-  if (l < nl - 1) {
-    Level& C = ps->lv[l + 1];
-    Workspace* cphi = f32 ? C.phi32 : C.phi;
-    Workspace& crho = f32 ? C.rho32 : C.rho;
-    cur = rec_relax(r, l, cur, L.wpre[p].data(), (int)L.wpre[p].size(), f32);
-    r.ok(launch_stencil(*L.op, dt, MODE_RESIDUAL, phi[cur].ptr, L.v, res.ptr, L.v, rho.ptr, L.v, r.nb, bc, 1.0,
-                        r.active, ps->sums.gs(), r.st));
-    r.ok(launch_transfer(*L.restr, dt, res.ptr, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st));
-    int ccur;
-    if (l + 1 == ps->lc[p]) {
-      // levels l+1 .. L in one CTA per solve: rho_{l+1} in, phi_{l+1} out
+  const int dt = f32 ? GPW_F32 : GPW_F64;
+  Level& L = ps->lv[l];
+  Level& C = ps->lv[l + 1];
+  Workspace* cphi = f32 ? C.phi32 : C.phi;
+  Workspace& crho = f32 ? C.rho32 : C.rho;
+  Boundary bc = make_boundary(L.op->periodic, dt, nullptr);
+  if (l + 1 == ps->lc[p]) {
+    // levels l+1 .. L in one CTA per solve: rho_{l+1} in, phi_{l+1} out
+    if (!r.tune) {
+      r.ok(launch_transfer(*L.restr, dt, res, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st));
       CoarseArgs ca = ps->cargs[p];
       ca.rho = crho.ptr;
       ca.vrho = C.v;
@@ -183,18 +198,59 @@ int rec_vcycle(Rec& r, int l, int cur, bool f32) {
       ca.vphi = C.v;
       ca.active = r.active;
       r.ok(launch_coarse(dt, ca, ps->csmem[p], r.nb, r.st));
-      ccur = 0;
-    } else {
-      r.ok(launch_zero(dt, C.v, cphi[0].ptr, r.nb, r.active, r.st));
-      ccur = rec_vcycle(r, l + 1, 0, f32);
     }
-    Boundary cbc = make_boundary(C.op->periodic, dt, nullptr);
-    r.ok(launch_transfer(*L.interp, dt, cphi[ccur].ptr, C.v, phi[1 - cur].ptr, L.v, r.nb, cbc, 1, phi[cur].ptr, &L.v,
-                         r.active, r.st));
-    cur = 1 - cur;
+    return 0;
   }
-  cur = rec_relax(r, l, cur, L.wpost[p].data(), (int)L.wpost[p].size(), f32);
-  return cur;
+  const bool coarsest = (l + 2 == nl);
+  const std::vector<double>& first = coarsest ? C.wpost[p] : C.wpre[p];
+  const bool fuse = ps->relax_method == 2 && !first.empty() && restrict_sweep_ok(*L.restr, dt) &&
+                    !C.op->coefs.empty();
+  if (!r.tune) {
+    if (fuse) {
+      const RestrictSweep sw{cphi[0].ptr, first[0], C.op->coefs[0]};
+      r.ok(launch_transfer(*L.restr, dt, res, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st,
+                           &sw));
+    } else {
+      r.ok(launch_transfer(*L.restr, dt, res, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st));
+      r.ok(launch_zero(dt, C.v, cphi[0].ptr, r.nb, r.active, r.st));
+    }
+  }
+  // the fused first sweep wrote buffer 0 as the result of sweep 1: the
+  // V-cycle continues from there (ping-pong parity counts that sweep)
+  if (fuse) return rec_vcycle(r, l + 1, 0, f32, true);
+  return rec_vcycle(r, l + 1, 0, f32);
+}
+
+// Records iterate2(level l) starting from phi buffer `cur`; returns the buffer
+// holding phi_l afterwards.  first_done: the first sweep of this level (its
+// first pre-sweep, or on the coarsest level its first post-sweep) has already
+// been written into buffer `cur`.
+int rec_vcycle(Rec& r, int l, int cur, bool f32, bool first_done) {
+  gpw_poisson* ps = r.ps;
+  const int nl = (int)ps->lv.size();
+  Level& L = ps->lv[l];
+  const int dt = f32 ? GPW_F32 : GPW_F64;
+  Workspace* phi = f32 ? L.phi32 : L.phi;
+  Workspace& rho = f32 ? L.rho32 : L.rho;
+  Workspace& res = f32 ? L.res32 : L.res;
+  const int p = f32 ? 1 : 0;
+  if (l < nl - 1) {
+    Level& C = ps->lv[l + 1];
+    Workspace* cphi = f32 ? C.phi32 : C.phi;
+    const int skip = first_done ? 1 : 0;
+    cur = rec_relax(r, l, cur, L.wpre[p].data() + skip, (int)L.wpre[p].size() - skip, f32);
+    // the residual's norm is not needed below level 0's convergence test
+    r.stencil(*L.op, dt, MODE_RESIDUAL, phi[cur].ptr, res.ptr, rho.ptr, L.v, 1.0, GridSum{});
+    const int ccur = rec_lower(r, l, res.ptr, f32);
+    Boundary cbc = make_boundary(C.op->periodic, dt, nullptr);
+    if (!r.tune)
+      r.ok(launch_transfer(*L.interp, dt, cphi[ccur].ptr, C.v, phi[1 - cur].ptr, L.v, r.nb, cbc, 1, phi[cur].ptr,
+                           &L.v, r.active, r.st));
+    cur = 1 - cur;
+    return rec_relax(r, l, cur, L.wpost[p].data(), (int)L.wpost[p].size(), f32);
+  }
+  const int skip = first_done ? 1 : 0;
+  return rec_relax(r, l, cur, L.wpost[p].data() + skip, (int)L.wpost[p].size() - skip, f32);
 }
 
 }  // namespace
@@ -228,6 +284,21 @@ static void setup_coarse(gpw_poisson* ps, int p) {
   ps->lc[p] = nl;
   ps->csmem[p] = 0;
   if (ps->relax_method != 2) return;
+  // padded layout (zero halo) when no level of the hierarchy is periodic
+  // and the transfers have the zero-boundary K=2 tables
+  bool padded = true;
+  for (int l = 0; l < nl; ++l) {
+    const Level& L = ps->lv[l];
+    for (int a = 0; a < 3; ++a) {
+      if (L.op->periodic[a]) padded = false;
+      if (l + 1 < nl && (L.restr->k != 2 || L.restr->pad[a][0] != 0 || L.interp->k != 2 ||
+                         L.interp->pad[a][0] != 1 || L.interp->skip[a][0] != 1))
+        padded = false;
+    }
+  }
+  auto buf_pts = [&](const Level& L) -> size_t {
+    return padded ? (size_t)(L.v.n[0] + 2) * (L.v.n[1] + 2) * (L.v.n[2] + 2) : (size_t)view_points(L.v);
+  };
   size_t bytes = 0;
   int lc = nl;
   for (int l = nl - 1; l >= 1 && nl - l <= CG_MAXL; --l) {
@@ -235,7 +306,7 @@ static void setup_coarse(gpw_poisson* ps, int p) {
     const OpDesc& d = *L.op;
     if (!d.real || !d.star_jacobi || d.R != 1) break;
     if ((int)(L.wpre[p].size() + L.wpost[p].size()) > CG_MAXW) break;
-    const size_t b = 3 * (size_t)view_points(L.v) * es;
+    const size_t b = 3 * buf_pts(L) * es;
     if (bytes + b > budget) break;
     bytes += b;
     lc = l;
@@ -244,6 +315,7 @@ static void setup_coarse(gpw_poisson* ps, int p) {
   CoarseArgs& ca = ps->cargs[p];
   ca = CoarseArgs{};
   ca.nl = nl - lc;
+  ca.padded = padded ? 1 : 0;
   int base = 0;
   for (int k = 0; k < ca.nl; ++k) {
     const Level& L = ps->lv[lc + k];
@@ -253,7 +325,7 @@ static void setup_coarse(gpw_poisson* ps, int p) {
       c.n[a] = L.v.n[a];
       c.periodic[a] = d.periodic[a];
     }
-    c.pts = (int)view_points(L.v);
+    c.pts = (int)buf_pts(L);
     c.base = base;
     base += 3 * c.pts;
     c.cc = d.sc.cc;
@@ -361,7 +433,7 @@ static bool fused_dc(const gpw_poisson* ps);
 extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int which, int reps, double* ms_per_launch,
                                        double* bytes_per_launch, gpw_stream stream) {
   if (!ps || !ms_per_launch || !bytes_per_launch) return fail(GPW_EINVAL, "null argument");
-  if (nbatch < 1 || nbatch > ps->nbmax || reps < 1 || which < 0 || which > 4)
+  if (nbatch < 1 || nbatch > ps->nbmax || reps < 1 || which < 0 || which > 5)
     return fail(GPW_EINVAL, "time_level0: bad arguments");
   if (which >= 2) {
     int rc = ensure_f32(ps);
@@ -388,12 +460,16 @@ extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int whic
       case 3:
         return launch_stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[0].ptr, L0.v, nullptr, L0.phi[1].ptr,
                                  L0.rho32.ptr, nb, L0.w, 0.0, act, GridSum{}, st);
-      default:
+      case 4:
         return launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[1].ptr,
                                  L0.rho.ptr, nb, 1.0, L0.w, act, ps->sums.gs(), st);
+      default:
+        return launch_stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[0].ptr, L0.v, L0.res32.ptr, L0.v,
+                              L0.rho32.ptr, L0.v, nb, make_boundary(L0.op->periodic, GPW_F32, nullptr), 1.0, act,
+                              GridSum{}, st);
     }
   };
-  static const double bytes_pp[5] = {24.0, 16.0, 12.0, 24.0, 24.0};
+  static const double bytes_pp[6] = {24.0, 16.0, 12.0, 24.0, 24.0, 12.0};
   cudaError_t e = launch();  // warm-up (and lazy kernel setup)
   if (e != cudaSuccess) return cuda_fail(e, "time_level0 launch");
   cudaEvent_t e0, e1;
@@ -443,18 +519,28 @@ static bool fused_dc(const gpw_poisson* ps) {
          dc_fusable(*L0.op);
 }
 
-static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, int maxiter_unused, cudaStream_t st) {
-  (void)maxiter_unused;
+// tune = true: the autotuner's pass over the same stencil launches (before
+// capture, on the engine's buffers); nothing else is launched.
+static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStream_t st, bool tune = false) {
   Rec r{ps, nb, st, (const unsigned char*)ps->d_active.ptr};
+  r.tune = tune;
   Level& L0 = ps->lv[0];
-  Boundary bc = make_boundary(L0.op->periodic, GPW_F64, nullptr);
   const int64_t per = L0.v.sb;
   const int64_t n = per * nb;
   const int thr = 256;
   const int blocks = (int)std::min<int64_t>((n + thr - 1) / thr, 4LL * num_sms());
+  auto converge = [&]() {
+    if (tune) return;
+    converge_update_kernel<<<1, 256, 0, st>>>(nb, ps->sums.gs().result, ps->dv, (const double*)ps->d_eps.ptr,
+                                              (const int*)ps->d_maxiter.ptr, (double*)ps->d_err.ptr,
+                                              (int*)ps->d_niter.ptr, (unsigned char*)ps->d_active.ptr,
+                                              (int*)ps->d_any.ptr);
+    r.ok(cudaGetLastError());
+  };
   if (prec == 0) {
     const int cur = rec_vcycle(r, 0, 0, false);
-    if (cur != 0) r.ok(cudaMemcpyAsync(L0.phi[0].ptr, L0.phi[1].ptr, n * 8, cudaMemcpyDeviceToDevice, st));
+    if (cur != 0 && !tune)
+      r.ok(cudaMemcpyAsync(L0.phi[0].ptr, L0.phi[1].ptr, n * 8, cudaMemcpyDeviceToDevice, st));
   } else if (fused_dc(ps)) {
     // Fused defect correction.  On entry L0.rho32 holds rhs = -(A phi - rho)
     // and L0.phi32[0] the first level-0 sweep from zero (both written by the
@@ -465,61 +551,41 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, int maxit
     const std::vector<double>& wpre = L0.wpre[1];
     const std::vector<double>& wpost = L0.wpost[1];
     int cur = rec_relax(r, 0, 0, wpre.data() + 1, (int)wpre.size() - 1, true);
-    Boundary bc32 = make_boundary(L0.op->periodic, GPW_F32, nullptr);
-    r.ok(launch_stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[cur].ptr, L0.v, L0.res32.ptr, L0.v, L0.rho32.ptr,
-                        L0.v, nb, bc32, 1.0, r.active, ps->sums.gs(), st));
-    r.ok(launch_transfer(*L0.restr, GPW_F32, L0.res32.ptr, L0.v, C.rho32.ptr, C.v, nb, bc32, 0, nullptr, nullptr,
-                         r.active, st));
-    int ccur;
-    if (ps->lc[1] == 1) {
-      CoarseArgs ca = ps->cargs[1];
-      ca.rho = C.rho32.ptr;
-      ca.vrho = C.v;
-      ca.phi = C.phi32[0].ptr;
-      ca.vphi = C.v;
-      ca.active = r.active;
-      r.ok(launch_coarse(GPW_F32, ca, ps->csmem[1], nb, st));
-      ccur = 0;
-    } else {
-      r.ok(launch_zero(GPW_F32, C.v, C.phi32[0].ptr, nb, r.active, st));
-      ccur = rec_vcycle(r, 1, 0, true);
-    }
+    r.stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[cur].ptr, L0.res32.ptr, L0.rho32.ptr, L0.v, 1.0, GridSum{});
+    const int ccur = rec_lower(r, 0, L0.res32.ptr, true);
     Boundary cbc = make_boundary(C.op->periodic, GPW_F32, nullptr);
-    r.ok(launch_transfer(*L0.interp, GPW_F32, C.phi32[ccur].ptr, C.v, L0.phi32[1 - cur].ptr, L0.v, nb, cbc, 1,
-                         L0.phi32[cur].ptr, &L0.v, r.active, st));
+    if (!tune)
+      r.ok(launch_transfer(*L0.interp, GPW_F32, C.phi32[ccur].ptr, C.v, L0.phi32[1 - cur].ptr, L0.v, nb, cbc, 1,
+                           L0.phi32[cur].ptr, &L0.v, r.active, st));
     cur = 1 - cur;
     cur = rec_relax(r, 0, cur, wpost.data(), (int)wpost.size() - 1, true);
-    GridSum none{};
-    r.ok(launch_stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[cur].ptr, L0.v, nullptr, L0.phi[0].ptr,
-                           L0.rho32.ptr, nb, wpost.back(), 0.0, r.active, none, st));
-    r.ok(launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr,
-                           nb, 1.0, wpre[0], r.active, ps->sums.gs(), st));
-    converge_update_kernel<<<1, 256, 0, st>>>(nb, ps->sums.gs().result, ps->dv, (const double*)ps->d_eps.ptr,
-                                              (const int*)ps->d_maxiter.ptr, (double*)ps->d_err.ptr,
-                                              (int*)ps->d_niter.ptr, (unsigned char*)ps->d_active.ptr,
-                                              (int*)ps->d_any.ptr);
-    r.ok(cudaGetLastError());
+    r.stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[cur].ptr, L0.v, nullptr, L0.phi[0].ptr, L0.rho32.ptr,
+                 wpost.back(), 0.0, GridSum{});
+    r.stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr, 1.0,
+                 wpre[0], ps->sums.gs());
+    converge();
     return r.err;
   } else {
     // defect correction: rhs32 = -(A phi - rho) (residual computed at the end
     // of the previous iteration into d_r64), e = FP32 V-cycle(rhs32), phi += e
-    to_f32_neg_kernel<<<blocks, thr, 0, st>>>(n, (const double*)ps->d_r64.ptr, (float*)L0.rho32.ptr, r.active, per);
-    r.ok(cudaGetLastError());
-    r.ok(launch_zero(GPW_F32, L0.v, L0.phi32[0].ptr, nb, r.active, st));
+    if (!tune) {
+      to_f32_neg_kernel<<<blocks, thr, 0, st>>>(n, (const double*)ps->d_r64.ptr, (float*)L0.rho32.ptr, r.active,
+                                                per);
+      r.ok(cudaGetLastError());
+      r.ok(launch_zero(GPW_F32, L0.v, L0.phi32[0].ptr, nb, r.active, st));
+    }
     const int cur = rec_vcycle(r, 0, 0, true);
-    add_f32_kernel<<<blocks, thr, 0, st>>>(n, (const float*)L0.phi32[cur].ptr, (double*)L0.phi[0].ptr, r.active, per);
-    r.ok(cudaGetLastError());
+    if (!tune) {
+      add_f32_kernel<<<blocks, thr, 0, st>>>(n, (const float*)L0.phi32[cur].ptr, (double*)L0.phi[0].ptr, r.active,
+                                             per);
+      r.ok(cudaGetLastError());
+    }
   }
   // error = sum(r^2) dv on level 0 after post-smoothing (gpaw/poisson.py:357-361)
   // (the float64 residual itself is kept only as the next defect-correction right-hand side)
-  r.ok(launch_stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, L0.v, prec == 1 ? ps->d_r64.ptr : nullptr, L0.v,
-                      L0.rho.ptr, L0.v, nb,
-                      bc, 1.0, r.active, ps->sums.gs(), st));
-  converge_update_kernel<<<1, 256, 0, st>>>(nb, ps->sums.gs().result, ps->dv, (const double*)ps->d_eps.ptr,
-                                            (const int*)ps->d_maxiter.ptr,
-                                            (double*)ps->d_err.ptr, (int*)ps->d_niter.ptr,
-                                            (unsigned char*)ps->d_active.ptr, (int*)ps->d_any.ptr);
-  r.ok(cudaGetLastError());
+  r.stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, prec == 1 ? ps->d_r64.ptr : nullptr, L0.rho.ptr, L0.v,
+            1.0, ps->sums.gs());
+  converge();
   return r.err;
 }
 
@@ -533,10 +599,47 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
   cudaStream_t st = (cudaStream_t)stream;
   Level& L0 = ps->lv[0];
   const int nb = (int)nbatch;
-  const size_t bytes = (size_t)L0.v.sb * nb * 8;
   int rc;
   if (precision == 1 && (rc = ensure_f32(ps))) return rc;
   cudaError_t e;
+  // get (or capture) the graph of one iteration for this batch size
+  gpw_poisson::GraphKey key{nbatch, precision};
+  auto it = ps->graphs.find(key);
+  if (it == ps->graphs.end()) {
+    // autotune the stencil launches of the iteration on the engine's own
+    // buffers (before the inputs are copied in), then capture it
+    cudaError_t te = record_iteration(ps, nb, precision, st, true);
+    if (te == cudaSuccess) te = cudaStreamSynchronize(st);
+    if (te != cudaSuccess) return cuda_fail(te, "stencil autotuning");
+    cudaGraph_t g;
+    cudaStream_t cs;
+    if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e, "stream");
+    if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+      cudaStreamDestroy(cs);
+      return cuda_fail(e, "begin capture");
+    }
+    cudaError_t re = record_iteration(ps, nb, precision, cs);
+    e = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (re != cudaSuccess) return cuda_fail(re, "record V-cycle");
+    if (e != cudaSuccess) return cuda_fail(e, "end capture");
+    size_t nnodes = 0;
+    int64_t nkern = 0;
+    if (cudaGraphGetNodes(g, nullptr, &nnodes) == cudaSuccess && nnodes) {
+      std::vector<cudaGraphNode_t> nodes(nnodes);
+      if (cudaGraphGetNodes(g, nodes.data(), &nnodes) == cudaSuccess)
+        for (auto n : nodes) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(n, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nkern;
+        }
+    }
+    cudaGraphExec_t ge;
+    e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+    it = ps->graphs.emplace(key, ge).first;
+    ps->graph_kernels[key] = nkern;
+  }
   // state: eps, niter = 1, active = 1
   std::vector<int> ones(nb, 1);
   std::vector<unsigned char> act(nb, 1);
@@ -560,40 +663,6 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
     e = launch_stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, L0.v, ps->d_r64.ptr, L0.v, L0.rho.ptr, L0.v, nb,
                        bc, 1.0, (const unsigned char*)ps->d_active.ptr, ps->sums.gs(), st);
     if (e != cudaSuccess) return cuda_fail(e, "poisson initial residual");
-  }
-  // get (or capture) the graph of one iteration for this batch size
-  gpw_poisson::GraphKey key{nbatch, precision};
-  auto it = ps->graphs.find(key);
-  if (it == ps->graphs.end()) {
-    // eager warm-up run of the launch sequence is avoided: capture directly
-    cudaGraph_t g;
-    cudaStream_t cs;
-    if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e, "stream");
-    if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
-      cudaStreamDestroy(cs);
-      return cuda_fail(e, "begin capture");
-    }
-    cudaError_t re = record_iteration(ps, nb, precision, maxiter, cs);
-    e = cudaStreamEndCapture(cs, &g);
-    cudaStreamDestroy(cs);
-    if (re != cudaSuccess) return cuda_fail(re, "record V-cycle");
-    if (e != cudaSuccess) return cuda_fail(e, "end capture");
-    size_t nnodes = 0;
-    int64_t nkern = 0;
-    if (cudaGraphGetNodes(g, nullptr, &nnodes) == cudaSuccess && nnodes) {
-      std::vector<cudaGraphNode_t> nodes(nnodes);
-      if (cudaGraphGetNodes(g, nodes.data(), &nnodes) == cudaSuccess)
-        for (auto n : nodes) {
-          cudaGraphNodeType t;
-          if (cudaGraphNodeGetType(n, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nkern;
-        }
-    }
-    cudaGraphExec_t ge;
-    e = cudaGraphInstantiate(&ge, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
-    it = ps->graphs.emplace(key, ge).first;
-    ps->graph_kernels[key] = nkern;
   }
   ps->last_kernels = (precision == 1) ? 1 : 0;
   ps->last_graphs = 0;

@@ -24,36 +24,52 @@
 
 namespace gpw {
 
-// Tile shapes measured on B200 (127^3 x 16 grids, float64): the sweep /
-// residual epilogues run best with 8 x 32 threads, one plane of prefetch and
-// two CTAs per SM; the plain apply with 4 x 32 threads and two planes of
-// prefetch (less register pressure, more CTAs).
-template <int MODE> struct TmaShape {
-  static constexpr int NTY = 8, D = 1, MINB = 2;
+// Tile-shape variants (the launcher's autotuner times them per grid, dtype,
+// radius and epilogue and keeps the fastest): NTY thread rows of 32 threads,
+// PY axis-1 rows per thread, D planes of TMA prefetch beyond the current one,
+// MINB CTAs per SM the register allocation must allow.
+template <int NTY_, int PY_, int D_, int MINB_>
+struct TmaShape {
+  static constexpr int NTY = NTY_, PY = PY_, D = D_, MINB = MINB_;
 };
-template <> struct TmaShape<MODE_APPLY> {
-  static constexpr int NTY = 4, D = 2, MINB = 1;
-};
+template <int V> struct TmaVariant;
+template <> struct TmaVariant<0> { using T = TmaShape<8, 2, 1, 2>; };  // 64 x 16 tile, 1 plane ahead
+template <> struct TmaVariant<1> { using T = TmaShape<4, 2, 2, 1>; };  // 64 x 8 tile, 2 planes ahead
+template <> struct TmaVariant<2> { using T = TmaShape<8, 2, 2, 2>; };  // 64 x 16 tile, 2 planes ahead
+template <> struct TmaVariant<3> { using T = TmaShape<4, 4, 2, 2>; };  // 64 x 16 tile, 4 rows per thread
+template <> struct TmaVariant<4> { using T = TmaShape<8, 2, 3, 2>; };  // 64 x 16 tile, 3 planes ahead
 
-template <typename S, int R, int MODE = MODE_JACOBI>
+constexpr int tma_align128(int b) { return (b + 127) / 128 * 128; }
+
+template <typename S, int R, int MODE, int V = 0>
 struct TmaCfg {
+  using Sh = typename TmaVariant<V>::T;
   static constexpr int VEC = 2;                        // points per thread along axis 2
   static constexpr int NTX = 32;                       // threads along axis 2
   static constexpr int TZ = NTX * VEC;                 // tile width (points)
-  static constexpr int PY = 2;                         // axis-1 rows per thread
-  static constexpr int NTY = TmaShape<MODE>::NTY;      // threads along axis 1
-  static constexpr int MINB = TmaShape<MODE>::MINB;    // CTAs per SM the registers must allow
+  static constexpr int PY = Sh::PY;                    // axis-1 rows per thread
+  static constexpr int NTY = Sh::NTY;                  // threads along axis 1
+  static constexpr int MINB = Sh::MINB;                // CTAs per SM the registers must allow
   static constexpr int TY = NTY * PY;                  // tile height
   static constexpr int NT = NTX * NTY;                 // threads per CTA
   static constexpr int ALIGN = 16 / (int)sizeof(S);    // elements per 16 bytes
   static constexpr int XL = ((R + ALIGN - 1) / ALIGN) * ALIGN;  // left halo, 16-byte aligned start
   static constexpr int W = TZ + 2 * XL;                // box width (elements)
   static constexpr int H = TY + 2 * R;                 // box height
-  static constexpr int D = TmaShape<MODE>::D;          // planes prefetched beyond the current one
+  static constexpr int D = Sh::D;                      // planes prefetched beyond the current one
   static constexpr int NS = R + D + 1;                 // ring stages
-  static constexpr int STAGE_BYTES = ((H * W * (int)sizeof(S) + 127) / 128) * 128;
+  // per stage: the input plane (with halo), the rho plane of the output
+  // completed at that step, and (JACOBI_ADD64) the float64 phi plane
+  static constexpr bool HAS_RHO = MODE != MODE_APPLY;
+  static constexpr bool HAS_AUX = MODE == MODE_JACOBI_ADD64;
+  static constexpr int IN_BYTES = H * W * (int)sizeof(S);
+  static constexpr int RHO_BYTES = HAS_RHO ? TY * TZ * (int)sizeof(S) : 0;
+  static constexpr int AUX_BYTES = HAS_AUX ? TY * TZ * 8 : 0;
+  static constexpr int STAGE_BYTES = tma_align128(IN_BYTES) + tma_align128(RHO_BYTES) + tma_align128(AUX_BYTES);
+  static constexpr int RHO_OFF = tma_align128(IN_BYTES);
+  static constexpr int AUX_OFF = RHO_OFF + tma_align128(RHO_BYTES);
   static constexpr int NR = 2 * R + 1;
-  static constexpr size_t smem = (size_t)NS * STAGE_BYTES + 128;
+  static constexpr size_t smem = (size_t)NS * STAGE_BYTES + (size_t)NS * 8 + 128;
 };
 
 struct TmaArgs {
@@ -97,15 +113,16 @@ template <typename S> struct Vec2;
 template <> struct Vec2<double> { using T = double2; };
 template <> struct Vec2<float> { using T = float2; };
 
-template <typename S, int R, int MODE>
-__global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MINB)
-    star_tma_kernel(const __grid_constant__ CUtensorMap tmap, const TmaArgs ta, const StarCoefs k) {
-  using C = TmaCfg<S, R, MODE>;
+template <typename S, int R, int MODE, int VAR>
+__global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE, VAR>::MINB)
+    star_tma_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_rho,
+                    const __grid_constant__ CUtensorMap tmap_aux, const TmaArgs ta, const StarCoefs k) {
+  using C = TmaCfg<S, R, MODE, VAR>;
   using V = typename Vec2<S>::T;
   constexpr int W = C::W, NS = C::NS, NR = C::NR, PY = C::PY, D = C::D;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  // 128-byte aligned ring (TMA destination), then the mbarriers; the launch
-  // reserves 128 spare bytes for the alignment shift
+  // 128-byte aligned ring of stages (TMA destinations), then the mbarriers;
+  // the launch reserves 128 bytes for the alignment shift
   unsigned char* ring = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + NS * C::STAGE_BYTES);
   __shared__ double red[32];
@@ -115,8 +132,9 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
   if (a.active && !a.active[b]) return;
   const int x0 = blockIdx.x * C::TZ, y0 = blockIdx.y * C::TY;
   const int n0 = a.vout.n[0];
-  const int z0 = chunk * a.zchunk;
-  const int z1 = min(n0, z0 + a.zchunk);
+  // balanced chunks of axis 0 (lengths differ by at most one plane)
+  const int z0 = (int)((int64_t)chunk * n0 / a.nchunk);
+  const int z1 = (int)((int64_t)(chunk + 1) * n0 / a.nchunk);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + C::NTX * ty;
   const int xl = C::XL + C::VEC * tx;     // local column of this thread's first point
@@ -134,14 +152,24 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
 
   if (z0 < z1) {
     const int pfirst = z0 - R;
-    const int nsteps = (z1 - 1 + R) - pfirst + 1;
-    if (tid == 0) {
-      for (int i = 0; i <= D && i < nsteps; ++i) {
-        const unsigned bar = mbar_u32(&bars[i % NS]);
-        mbar_expect_tx(bar, (unsigned)(C::H * W * sizeof(S)));
-        tma_load_4d(smem_u32(ring + (i % NS) * C::STAGE_BYTES), &tmap, x0 - C::XL, y0 - R, pfirst + i, b, bar);
+    const int nsteps = z1 - z0 + 2 * R;
+    // step i brings input plane pfirst + i and, once it completes an output
+    // plane o = z0 - 2R + i of this chunk, that plane's rho (and float64 phi)
+    auto issue = [&](int i) {
+      unsigned char* st = ring + (i % NS) * C::STAGE_BYTES;
+      const unsigned bar = mbar_u32(&bars[i % NS]);
+      const int o = z0 - 2 * R + i;
+      const bool with_out = C::HAS_RHO && o >= z0;
+      const unsigned bytes = C::IN_BYTES + (with_out ? C::RHO_BYTES + C::AUX_BYTES : 0);
+      mbar_expect_tx(bar, bytes);
+      tma_load_4d(smem_u32(st), &tmap, x0 - C::XL, y0 - R, pfirst + i, b, bar);
+      if (with_out) {
+        tma_load_4d(smem_u32(st + C::RHO_OFF), &tmap_rho, x0, y0, o, b, bar);
+        if constexpr (C::HAS_AUX) tma_load_4d(smem_u32(st + C::AUX_OFF), &tmap_aux, x0, y0, o, b, bar);
       }
-    }
+    };
+    if (tid == 0)
+      for (int i = 0; i <= D && i < nsteps; ++i) issue(i);
     V acc[PY][NR];
 #pragma unroll
     for (int j = 0; j < PY; ++j)
@@ -154,42 +182,9 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
         const int s = sb + ph;
         if (s >= nsteps) break;
         const int slot = s % NS;
-        const S* sl = reinterpret_cast<const S*>(ring + slot * C::STAGE_BYTES);
+        const unsigned char* stg = ring + slot * C::STAGE_BYTES;
+        const S* sl = reinterpret_cast<const S*>(stg);
         const int o = pfirst + s - R;  // output plane completed by this step
-        // prefetch rho for the completed plane
-        V rho[PY];
-        if constexpr (MODE != MODE_APPLY) {
-#pragma unroll
-          for (int j = 0; j < PY; ++j) {
-            rho[j] = V{S(0), S(0)};
-            const int y = y0 + yb + j;
-            if (o >= z0 && y < a.vout.n[1] && xin0) {
-              const S* rp = static_cast<const S*>(a.rho) + (int64_t)b * a.vrho.sb + (int64_t)o * a.vrho.s0 +
-                            (int64_t)y * a.vrho.s1 + x;
-              if (xin1)
-                rho[j] = *reinterpret_cast<const V*>(rp);
-              else
-                rho[j].x = rp[0];
-            }
-          }
-        }
-        // JACOBI_ADD64: prefetch the float64 phi that receives this plane's update
-        double2 phi64[PY];
-        if constexpr (MODE == MODE_JACOBI_ADD64) {
-#pragma unroll
-          for (int j = 0; j < PY; ++j) {
-            phi64[j] = make_double2(0.0, 0.0);
-            const int y = y0 + yb + j;
-            if (o >= z0 && y < a.vout.n[1] && xin0) {
-              const double* pp = static_cast<const double*>(a.out2) + (int64_t)b * a.vout.sb +
-                                 (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
-              if (xin1)
-                phi64[j] = *reinterpret_cast<const double2*>(pp);
-              else
-                phi64[j].x = pp[0];
-            }
-          }
-        }
         if (!mbar_wait_bounded(mbar_u32(&bars[slot]), (unsigned)((s / NS) & 1))) timed_out = true;
 
         // column of PY + 2R rows (2 points each) at this thread's columns
@@ -243,25 +238,29 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
         // output plane o is complete: logical slot 0 = physical ph
         if (o >= z0) {
           const S* osl = reinterpret_cast<const S*>(ring + ((s + NS - R) % NS) * C::STAGE_BYTES);
+          const S* rsl = reinterpret_cast<const S*>(stg + C::RHO_OFF);
+          const double* asl = reinterpret_cast<const double*>(stg + C::AUX_OFF);
 #pragma unroll
           for (int j = 0; j < PY; ++j) {
             const int y = y0 + yb + j;
             if (y < a.vout.n[1] && xin0) {
               V av = acc[j][ph];
               V res;
+              V rho = V{S(0), S(0)};
+              if constexpr (C::HAS_RHO) rho = *reinterpret_cast<const V*>(rsl + (yb + j) * C::TZ + C::VEC * tx);
               const int64_t oidx =
                   (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
               if constexpr (MODE == MODE_APPLY) {
                 res = av;
               } else if constexpr (MODE == MODE_RESIDUAL || MODE == MODE_RESID_DC) {
-                res.x = av.x - rho[j].x;
-                res.y = av.y - rho[j].y;
+                res.x = av.x - rho.x;
+                res.y = av.y - rho.y;
                 sumsq += (double)res.x * res.x + (xin1 ? (double)res.y * res.y : 0.0);
               } else {
                 const V cur = *reinterpret_cast<const V*>(osl + (yb + j + R) * W + xl);
                 const S w = (S)a.w, wc = w / (S)a.c0;
-                res.x = (S(1) - w) * cur.x + wc * (rho[j].x - av.x);
-                res.y = (S(1) - w) * cur.y + wc * (rho[j].y - av.y);
+                res.x = (S(1) - w) * cur.x + wc * (rho.x - av.x);
+                res.y = (S(1) - w) * cur.y + wc * (rho.y - av.y);
               }
               if constexpr (MODE == MODE_RESID_DC) {
                 // float32 defect and first inner Jacobi iterate from zero
@@ -280,7 +279,7 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
               } else if constexpr (MODE == MODE_JACOBI_ADD64) {
                 // phi64 += e (the inner correction), e never stored
                 double* pp = static_cast<double*>(a.out2) + oidx;
-                double2 pv = phi64[j];
+                double2 pv = *reinterpret_cast<const double2*>(asl + (yb + j) * C::TZ + C::VEC * tx);
                 pv.x += (double)res.x;
                 pv.y += (double)res.y;
                 if (xin1)
@@ -288,8 +287,7 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
                 else
                   pp[0] = pv.x;
               } else if (MODE != MODE_RESIDUAL || a.out) {
-                S* op = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 +
-                        (int64_t)y * a.vout.s1 + x;
+                S* op = static_cast<S*>(a.out) + oidx;
                 if (xin1)
                   *reinterpret_cast<V*>(op) = res;
                 else
@@ -301,20 +299,17 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE>::NT, TmaCfg<S, R, MODE>::MI
 #pragma unroll
         for (int j = 0; j < PY; ++j) acc[j][ph] = V{S(0), S(0)};
         __syncthreads();  // every thread is done with plane s - R (its slot is refilled next)
-        if (tid == 0 && s + D + 1 < nsteps) {
-          const int sn = s + D + 1;
-          const unsigned bar = mbar_u32(&bars[sn % NS]);
-          mbar_expect_tx(bar, (unsigned)(C::H * W * sizeof(S)));
-          tma_load_4d(smem_u32(ring + (sn % NS) * C::STAGE_BYTES), &tmap, x0 - C::XL, y0 - R, pfirst + sn, b, bar);
-        }
+        if (tid == 0 && s + D + 1 < nsteps) issue(s + D + 1);
       }
     }
   }
   if (timed_out && ta.status) atomicExch(ta.status, GPW_ETIMEDOUT);
   if constexpr (MODE == MODE_RESIDUAL || MODE == MODE_RESID_DC) {
-    double tot = block_sum(sumsq, red);
-    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
-    grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);
+    if (a.gsum.partial) {
+      double tot = block_sum(sumsq, red);
+      const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
+      grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);
+    }
   }
 }
 

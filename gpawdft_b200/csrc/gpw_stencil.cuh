@@ -38,6 +38,9 @@ namespace gpw {
 // array `out2` (phi += e) instead of being stored.
 enum StencilMode { MODE_APPLY = 0, MODE_RESIDUAL = 1, MODE_JACOBI = 2, MODE_RESID_DC = 3, MODE_JACOBI_ADD64 = 4 };
 
+// Number of tile-shape variants of the TMA star kernel (gpw_star_tma.cuh).
+constexpr int TMA_NVARIANT = 5;
+
 constexpr int PMAX = 80;  // GUC n<=6 with 6 directions needs 73
 
 struct StencilArgs {
@@ -191,6 +194,7 @@ __global__ void __launch_bounds__(GEN_TZ* GEN_TY)
     }
   }
   if constexpr (MODE == MODE_RESIDUAL) {
+    if (!a.gsum.partial) return;  // residual without its norm
     double tot = block_sum(sumsq, red);
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
     grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);
@@ -426,6 +430,7 @@ __global__ void __launch_bounds__(StarCfg<R, T>::NT)
     }
   }
   if constexpr (MODE == MODE_RESIDUAL) {
+    if (!a.gsum.partial) return;  // residual without its norm
     double tot = block_sum(sumsq, red);
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
     grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);

@@ -1,0 +1,18 @@
+// TMA star-stencil launches for float32 grids (apply, residual, Jacobi and
+// the Jacobi sweep that adds its result into float64 phi).
+#include "gpw_tma_launch.cuh"
+
+namespace gpw {
+
+cudaError_t tma_stencil_f32(int mode, int R, int var, const StencilArgs& a, int nbatch, const StarCoefs& sc,
+                            int nchunk, cudaStream_t st) {
+  switch (mode) {
+    case MODE_APPLY: return tma_run_radius<float, MODE_APPLY>(R, var, a, nbatch, sc, nchunk, st);
+    case MODE_RESIDUAL: return tma_run_radius<float, MODE_RESIDUAL>(R, var, a, nbatch, sc, nchunk, st);
+    case MODE_JACOBI: return tma_run_radius<float, MODE_JACOBI>(R, var, a, nbatch, sc, nchunk, st);
+    case MODE_JACOBI_ADD64: return tma_run_radius<float, MODE_JACOBI_ADD64>(R, var, a, nbatch, sc, nchunk, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace gpw

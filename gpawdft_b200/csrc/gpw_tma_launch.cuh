@@ -1,0 +1,142 @@
+// Launch of the TMA star-stencil kernel (gpw_star_tma.cuh) for one element
+// type: tensor maps, axis-0 chunking and the (radius, epilogue, tile
+// variant) dispatch.  Included by gpw_tma_f64.cu and gpw_tma_f32.cu, which
+// compile the two element types in parallel.
+#pragma once
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "gpw_internal.h"
+#include "gpw_star_tma.cuh"
+
+namespace gpw {
+
+// Every variant is compiled for radius 1 (coarse multigrid levels) and 3
+// (the nn=3 Laplacian of level 0); radius 2 uses variant 2 only and radius 4
+// variant 1 (128 threads: its float64 accumulators do not fit the register
+// share of two 256-thread CTAs per SM).
+__host__ __device__ constexpr int tma_default_variant(int R) { return R == 4 ? 1 : 2; }
+__host__ __device__ constexpr bool tma_variant_compiled(int R, int v) {
+  return (R == 1 || R == 3) ? (v >= 0 && v < TMA_NVARIANT) : v == tma_default_variant(R);
+}
+
+// 4D tensor map (axis 2, axis 1, axis 0, batch) over a grid view with a
+// box of bw x bh elements of one plane.
+inline bool encode_grid_map(CUtensorMap* map, size_t es, const void* base, const GridView& v, int nbatch, int bw,
+                            int bh) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  cuuint64_t dims[4] = {(cuuint64_t)v.n[2], (cuuint64_t)v.n[1], (cuuint64_t)v.n[0], (cuuint64_t)nbatch};
+  cuuint64_t strides[3] = {(cuuint64_t)(v.s1 * es), (cuuint64_t)(v.s0 * es),
+                           (cuuint64_t)(std::max<int64_t>(v.sb, v.s0 * v.n[0]) * es)};
+  cuuint32_t box[4] = {(cuuint32_t)bw, (cuuint32_t)bh, 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(map, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// Axis-0 chunk count from a wave model: CTAs run in waves of `slots`
+// (CTAs per SM x SMs); a wave costs its CTAs' planes, each chunk re-reading
+// a 2R-plane warm-up.  Chunks keep at least 2R + 2 planes.
+inline int tma_model_chunks(int n0, int64_t tiles, int R, int64_t slots) {
+  const int maxc = std::max(1, n0 / (2 * R + 2));
+  int best = 1;
+  double bestc = 1e300;
+  for (int nc = 1; nc <= maxc; ++nc) {
+    const int64_t ctas = tiles * nc;
+    const int64_t waves = (ctas + slots - 1) / slots;
+    const double cost = (double)waves * ((n0 + nc - 1) / nc + 2 * R);
+    if (cost < bestc * (1 - 1e-9)) {
+      best = nc;
+      bestc = cost;
+    }
+  }
+  return best;
+}
+
+inline int tma_max_chunks(int n0, int R) { return std::max(1, n0 / (2 * R + 2)); }
+
+template <typename S, int R, int MODE, int VAR>
+struct TmaKernel {
+  using C = TmaCfg<S, R, MODE, VAR>;
+  static int slots_per_sm() {
+    static int n = -1;
+    static std::once_flag once;
+    std::call_once(once, [] {
+      if (smem_optin_bytes(star_tma_kernel<S, R, MODE, VAR>, C::smem) != cudaSuccess) {
+        n = 0;
+        return;
+      }
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, star_tma_kernel<S, R, MODE, VAR>, C::NT, C::smem) !=
+          cudaSuccess)
+        b = 0;
+      n = b;
+    });
+    return n;
+  }
+  // nchunk == 0: from the wave model; nchunk < 0: the model's count times -nchunk
+  static cudaError_t run(const StencilArgs& a0, int nbatch, const StarCoefs& sc, int nchunk, cudaStream_t st) {
+    const int spm = slots_per_sm();
+    if (spm <= 0) return cudaErrorInvalidConfiguration;
+    StencilArgs a = a0;
+    CUtensorMap map_in, map_rho, map_aux;
+    std::memset(&map_rho, 0, sizeof(map_rho));
+    std::memset(&map_aux, 0, sizeof(map_aux));
+    if (!encode_grid_map(&map_in, sizeof(S), a.in, a.vin, nbatch, C::W, C::H)) return cudaErrorInvalidValue;
+    if (C::HAS_RHO && !encode_grid_map(&map_rho, sizeof(S), a.rho, a.vrho, nbatch, C::TZ, C::TY))
+      return cudaErrorInvalidValue;
+    if (C::HAS_AUX && !encode_grid_map(&map_aux, 8, a.out2, a.vout, nbatch, C::TZ, C::TY))
+      return cudaErrorInvalidValue;
+    const GridView& v = a.vout;
+    dim3 grid((v.n[2] + C::TZ - 1) / C::TZ, (v.n[1] + C::TY - 1) / C::TY, 1);
+    const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
+    int nc = nchunk > 0 ? nchunk
+                        : tma_model_chunks(v.n[0], tiles, R, (int64_t)spm * num_sms()) * std::max(1, -nchunk);
+    nc = std::max(1, std::min(nc, tma_max_chunks(v.n[0], R)));
+    a.nchunk = nc;
+    a.zchunk = (v.n[0] + nc - 1) / nc;
+    grid.z = nc * nbatch;
+    a.nblk_seg = grid.x * grid.y * nc;
+    TmaArgs ta{a, device_status_word()};
+    star_tma_kernel<S, R, MODE, VAR><<<grid, dim3(C::NTX, C::NTY), C::smem, st>>>(map_in, map_rho, map_aux, ta, sc);
+    return cudaGetLastError();
+  }
+};
+
+template <typename S, int R, int MODE>
+cudaError_t tma_run_variant(int var, const StencilArgs& a, int nbatch, const StarCoefs& sc, int nchunk,
+                            cudaStream_t st) {
+  if (!tma_variant_compiled(R, var)) return cudaErrorInvalidValue;
+  if constexpr (R == 1 || R == 3) {
+    switch (var) {
+      case 0: return TmaKernel<S, R, MODE, 0>::run(a, nbatch, sc, nchunk, st);
+      case 1: return TmaKernel<S, R, MODE, 1>::run(a, nbatch, sc, nchunk, st);
+      case 2: return TmaKernel<S, R, MODE, 2>::run(a, nbatch, sc, nchunk, st);
+      case 3: return TmaKernel<S, R, MODE, 3>::run(a, nbatch, sc, nchunk, st);
+      case 4: return TmaKernel<S, R, MODE, 4>::run(a, nbatch, sc, nchunk, st);
+    }
+    return cudaErrorInvalidValue;
+  } else {
+    return TmaKernel<S, R, MODE, tma_default_variant(R)>::run(a, nbatch, sc, nchunk, st);
+  }
+}
+
+template <typename S, int MODE>
+cudaError_t tma_run_radius(int R, int var, const StencilArgs& a, int nbatch, const StarCoefs& sc, int nchunk,
+                           cudaStream_t st) {
+  switch (R) {
+    case 1: return tma_run_variant<S, 1, MODE>(var, a, nbatch, sc, nchunk, st);
+    case 2: return tma_run_variant<S, 2, MODE>(var, a, nbatch, sc, nchunk, st);
+    case 3: return tma_run_variant<S, 3, MODE>(var, a, nbatch, sc, nchunk, st);
+    case 4: return tma_run_variant<S, 4, MODE>(var, a, nbatch, sc, nchunk, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace gpw

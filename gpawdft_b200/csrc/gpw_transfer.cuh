@@ -37,6 +37,10 @@ struct TransferArgs {
   int subtract;       // interpolation: out = base - I(in) instead of out = I(in)
   const void* base;   // (the reference's phi -= I(e) into another buffer; must not alias out)
   GridView vbase;
+  // K=2 restriction into a multigrid level: also write the level's first
+  // weighted-Jacobi sweep from phi = 0, out2 = (w2 / c02) out (same view)
+  void* out2;
+  double w2, c02;
 };
 
 // Load plane p of the box rows [ys, ys+H) x cols [xs, xs+W) (unpadded input

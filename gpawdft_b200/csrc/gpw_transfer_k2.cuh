@@ -87,12 +87,17 @@ __global__ void __launch_bounds__(K2_TX* K2_TY) restrict_k2_kernel(const Transfe
                  k2_ld(pl + off[d1][2], v0 && ok[d1][2]));
     return r2(z[0], z[1], z[2]);
   };
+  S* __restrict__ out2 =
+      a.out2 ? static_cast<S*>(a.out2) + (int64_t)b * a.vout.sb + (int64_t)I1 * a.vout.s1 + I2 : nullptr;
+  const S wc = (S)a.w2 / (S)a.c02;
   S ylo = Y(1 + 2 * I0s - a.pad0[0] - 1);
 #pragma unroll 2
   for (int I0 = I0s; I0 < I0e; ++I0) {
     const int c0 = 1 + 2 * I0 - a.pad0[0];
     const S ym = Y(c0), yp = Y(c0 + 1);
-    out[(int64_t)I0 * a.vout.s0] = r2(ylo, ym, yp);
+    const S v = r2(ylo, ym, yp);
+    out[(int64_t)I0 * a.vout.s0] = v;
+    if (out2) out2[(int64_t)I0 * a.vout.s0] = wc * v;
     ylo = yp;
   }
 }
@@ -288,6 +293,103 @@ __global__ void __launch_bounds__(K2V_TX* K2V_TY) interpolate_k2_vec_kernel(cons
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) ya[k] = yb[k];
+  }
+}
+
+// ------------------------------------------------------------------ vector restriction
+// Restriction with each thread owning 2 adjacent axis-2 outputs I2, I2+1
+// (a warp covers a 64-point output row): per (axis-0, axis-1) tap row the 5
+// fine inputs 2 I2 .. 2 I2 + 4 come from one 16-byte load (two for float64)
+// plus one scalar.  Zero-boundary grids with pad 0 on axis 2 (fine centre
+// 2I + 1), 16-byte aligned rows; a thread whose taps would pass the row end
+// falls back to checked scalar loads.  Same expressions per output as
+// restrict_k2_kernel (bit-identical).
+template <typename S>
+__device__ __forceinline__ void ld5(const S* p, S (&v)[5]) {
+  if constexpr (sizeof(S) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  } else {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+  v[4] = p[4];
+}
+
+template <typename S>
+__device__ __forceinline__ void st2(S* p, S v0, S v1, int nvalid) {
+  if (nvalid == 2) {
+    if constexpr (sizeof(S) == 4)
+      *reinterpret_cast<float2*>(p) = make_float2(v0, v1);
+    else
+      *reinterpret_cast<double2*>(p) = make_double2(v0, v1);
+  } else {
+    p[0] = v0;
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(K2V_TX* K2V_TY) restrict_k2_vec_kernel(const TransferArgs a) {
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int I2 = 2 * (blockIdx.x * K2V_TX + threadIdx.x), I1 = blockIdx.y * K2V_TY + threadIdx.y;
+  if (I1 >= a.vout.n[1] || I2 >= a.vout.n[2]) return;
+  const int nvalid = min(2, a.vout.n[2] - I2);
+  const int I0s = chunk * a.zchunk, I0e = min(a.vout.n[0], I0s + a.zchunk);
+  const S* __restrict__ in = static_cast<const S*>(a.in) + (int64_t)b * a.vin.sb;
+  S* __restrict__ out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)I1 * a.vout.s1 + I2;
+  S* __restrict__ out2 =
+      a.out2 ? static_cast<S*>(a.out2) + (int64_t)b * a.vout.sb + (int64_t)I1 * a.vout.s1 + I2 : nullptr;
+  const S wc = (S)a.w2 / (S)a.c02;
+  const int c1 = 1 + 2 * I1 - a.pad0[1];
+  const int f2 = 2 * I2 - a.pad0[2];  // first fine tap along axis 2 (c2 - 1 of output I2)
+  const bool full = f2 >= 0 && f2 + 4 < a.vin.n[2];
+  int64_t o1[3];
+  bool v1[3];
+#pragma unroll
+  for (int d1 = 0; d1 < 3; ++d1) v1[d1] = k2_axis(c1 - 1 + d1, a.vin.n[1], a.bc.periodic[1], a.vin.s1, o1[d1]);
+  // the axis-2 and axis-1 passes of both outputs on fine plane f0
+  auto Y = [&](int f0, S& y0, S& y1) {
+    int64_t o0;
+    const bool v0 = k2_axis(f0, a.vin.n[0], a.bc.periodic[0], a.vin.s0, o0);
+    S z0[3], z1[3];
+#pragma unroll
+    for (int d1 = 0; d1 < 3; ++d1) {
+      S r[5];
+      if (v0 && v1[d1]) {
+        const S* row = in + o0 + o1[d1];
+        if (full) {
+          ld5(row + f2, r);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 5; ++q) {
+            const int f = f2 + q;
+            r[q] = (f >= 0 && f < a.vin.n[2]) ? row[f] : S(0);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) r[q] = S(0);
+      }
+      z0[d1] = r2(r[0], r[1], r[2]);
+      z1[d1] = r2(r[2], r[3], r[4]);
+    }
+    y0 = r2(z0[0], z0[1], z0[2]);
+    y1 = r2(z1[0], z1[1], z1[2]);
+  };
+  S l0, l1, m0, m1, p0, p1;
+  Y(1 + 2 * I0s - a.pad0[0] - 1, l0, l1);
+#pragma unroll 2
+  for (int I0 = I0s; I0 < I0e; ++I0) {
+    const int c0 = 1 + 2 * I0 - a.pad0[0];
+    Y(c0, m0, m1);
+    Y(c0 + 1, p0, p1);
+    const S v0 = r2(l0, m0, p0), v1v = r2(l1, m1, p1);
+    l0 = p0;
+    l1 = p1;
+    st2(out + (int64_t)I0 * a.vout.s0, v0, v1v, nvalid);
+    if (out2) st2(out2 + (int64_t)I0 * a.vout.s0, wc * v0, wc * v1v, nvalid);
   }
 }
 

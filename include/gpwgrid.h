@@ -209,7 +209,7 @@ int gpw_poisson_last_stats(const gpw_poisson *ps, int64_t *kernel_launches,
  * overwritten; call between solves): `which` 0 = float64 Jacobi sweep,
  * 1 = float64 residual + norm, 2 = float32 Jacobi sweep, 3 = float32 sweep
  * adding into float64 phi (defect-correction update), 4 = float64 defect
- * (float32 rhs + first sweep + norm).  `reps` launches between CUDA events
+ * (float32 rhs + first sweep + norm), 5 = float32 residual (no norm).  `reps` launches between CUDA events
  * on `stream`; writes the mean milliseconds per launch and the algorithmic
  * bytes per launch (each compulsory read and write counted once).          */
 int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,

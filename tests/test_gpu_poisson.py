@@ -194,3 +194,31 @@ def test_fp32_batch_equals_single(cuda):
         n = ps.solve_neutral(phi, rhos[s], eps=eps[s])
         assert n == nb[s]
         assert np.array_equal(phi, phib[s])
+
+
+def test_full_size_127_trajectory(cuda):
+    """127^3 (the benchmark grid): the engine's vector transfers, TMA
+    stencil variants and one-CTA coarse levels reproduce the reference's
+    V-cycle count and potential (oracle: the compiled reference C when it is
+    built, else the NumPy restatement)."""
+    from oracle import ref
+    N = 128
+    rho, L = gaussian_density(N, 0.2, 8, 11)
+    backend = 'ref' if ref.available() else 'numpy'
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    ogd = OGD((N,) * 3, (L,) * 3, 0)
+    ps = PoissonSolver(nn=3, relax='J', eps=2e-10)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    ops = ol.PoissonSolver(nn=3, relax='J', eps=2e-10, backend=backend)
+    ops.set_grid_descriptor(ogd)
+    ops.initialize()
+    phi = gd.zeros()
+    n = ps.solve(phi, rho)
+    ophi = ogd.zeros()
+    on = ops.solve(ophi, rho)
+    assert n == on
+    assert np.abs(phi - ophi).max() < 1e-11 * np.abs(ophi).max()
+    assert abs(hartree(ogd, phi, rho) - hartree(ogd, ophi, rho)) < 1e-8
