@@ -382,6 +382,10 @@ def run_ours(args, rank, world, dist):
                       'unit': 'solves/s', 'vcycles_mean': float(np.mean(n64))}
         del ps64
 
+    # ---- live per-launch breakdown of one outer iteration (eager launches)
+    breakdown = [{'launch': n, 'ms': t}
+                 for n, t in ps.profile_iteration(B, reps=5)]
+
     # ---- secondary: config (a) Laplace apply, 32 x 48^3 float64, zero BC
     stencil = stencil_config_a(dev, stream)
 
@@ -407,6 +411,7 @@ def run_ours(args, rank, world, dist):
            'gpu_launches': int(launches),
            'clocks': clocks,
            'vcycles': [int(x) for x in niters],
+           'iteration_breakdown': breakdown,
            'stencil_config_a': stencil}
     if rank == 0 and world == 1 and not args.no_cpu:
         r = cpu_arm(1, 0)
@@ -520,13 +525,14 @@ def run_uneven(args):
     """512 independent solves, cubic N_c log-uniform in [32, 128] rounded to
     multiples of 8 (seed 5), each density 4-32 neutral Gaussians (h = 0.2 A),
     relative residual 1e-10, float32 inner / float64 outer.  Solves of one
-    size form one batched engine (one captured graph per iteration); the size
-    groups run concurrently on separate streams.  Reports solves/s and p50/p99
-    per-solve latency (completion of its group, from the common start)."""
-    import threading
+    size form one batched engine (its stencil variants autotuned); all the
+    engines' convergence loops run on the device in ONE graph launch
+    (gpw_poisson_solve_many), as concurrent branches.  Reports solves/s and
+    the p50/p99 per-solve latency (device time from the launch to the end of
+    the iteration in which the solve converged)."""
     import torch
     from gpawdft_b200.grid_descriptor import GridDescriptor
-    from gpawdft_b200.poisson import PoissonSolver
+    from gpawdft_b200.poisson import PoissonSolver, solve_many
     from gpawdft_b200.workloads import gaussian_density
     rng = np.random.default_rng(5)
     NS = 512
@@ -536,69 +542,60 @@ def run_uneven(args):
     groups = {}
     for i, (N, ng) in enumerate(zip(Ns, ngs)):
         groups.setdefault(int(N), []).append((i, int(ng)))
-    work = []
+    solvers, phis, rhos, epss, sizes = [], [], [], [], []
     for N, members in sorted(groups.items()):
-        rhos, L = [], None
+        rl, L = [], None
         for i, ng in members:
             r, L = gaussian_density(N, 0.2, ng, 5000 + i)
-            rhos.append(r)
+            rl.append(r)
         gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
-        eps = [eps_for(r, gd.dv) for r in rhos]
-        ps = PoissonSolver(nn=3, relax='J', maxiter=1000, precision='fp32',
-                           batch=len(rhos))
+        ps = PoissonSolver(nn=3, relax='J', maxiter=1000,
+                           precision=args.precision, batch=len(rl))
         ps.set_grid_descriptor(gd)
         ps.initialize()
-        rho_d = torch.from_numpy(np.array(rhos)).cuda()
-        work.append(dict(N=N, n=len(rhos), ps=ps, rho=rho_d, eps=eps,
-                         phi=torch.zeros_like(rho_d),
-                         stream=torch.cuda.Stream()))
+        solvers.append(ps)
+        rhos.append(torch.from_numpy(np.array(rl)).cuda())
+        phis.append(torch.zeros_like(rhos[-1]))
+        epss.append([eps_for(r, gd.dv) for r in rl])
+        sizes.append((N, len(rl)))
 
-    def run_all(record):
-        start = torch.cuda.Event(enable_timing=True)
-        start.record()
-        ends = []
+    def step():
+        for p in phis:
+            p.zero_()
+        return solve_many(solvers, phis, rhos, epss)
 
-        def worker(w):
-            with torch.cuda.stream(w['stream']):
-                w['stream'].wait_event(start)
-                w['phi'].zero_()
-                w['niter'] = w['ps'].solve_batch(w['phi'], w['rho'],
-                                                 eps=w['eps'])
-                ev = torch.cuda.Event(enable_timing=True)
-                ev.record()
-                w['end'] = ev
-        ths = [threading.Thread(target=worker, args=(w,)) for w in work]
-        for t in ths:
-            t.start()
-        for t in ths:
-            t.join()
-        torch.cuda.synchronize()
-        lat = []
-        for w in work:
-            t = start.elapsed_time(w['end']) / 1e3
-            lat.extend([t] * w['n'])
-        return max(lat), lat
-
-    for _ in range(max(1, args.warmup)):
-        run_all(False)
-    tots, lats = [], []
+    for _ in range(max(3, args.warmup)):
+        nits = step()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    ts, lats = [], []
+    e0.record()
     for _ in range(args.steps):
-        t, lat = run_all(True)
-        tots.append(t)
-        lats.extend(lat)
-    T = float(np.median(tots))
+        s0, s1 = _events()
+        s0.record()
+        nits = step()
+        s1.record()
+        torch.cuda.synchronize()
+        ts.append(s0.elapsed_time(s1) / 1e3)
+        for ps, (N, nb) in zip(solvers, sizes):
+            lats.extend(ps.last_latency(nb) / 1e3)
+    e1.record()
+    torch.cuda.synchronize()
+    T = e0.elapsed_time(e1) / 1e3 / args.steps
     line = {'metric': 'batched_uneven_poisson_solves_per_s', 'value': NS / T,
             'unit': 'solves/s', 'higher_is_better': True, 'n_gpus': 1,
-            'steps': args.steps, 'warmup': args.warmup, 'dtype': 'f32+f64',
+            'steps': args.steps, 'warmup': args.warmup,
+            'dtype': 'f32+f64' if args.precision == 'fp32' else 'f64',
             'data': 'synthetic',
             'config': {'workload': '512 solves, N_c log-uniform 32-128 (x8), '
-                                   '4-32 Gaussians, rel 1e-10, fp32 inner',
-                       'sizes': {str(w['N']): w['n'] for w in work}},
+                                   '4-32 Gaussians, rel 1e-10, %s, one graph '
+                                   'launch' % args.precision,
+                       'sizes': {str(N): nb for N, nb in sizes}},
             'p50_latency_s': float(np.percentile(lats, 50)),
             'p99_latency_s': float(np.percentile(lats, 99)),
             'ms_per_step': 1e3 * T,
-            'vcycles_mean': float(np.mean(np.concatenate(
-                [w['niter'] for w in work])))}
+            'step_ms_min': 1e3 * min(ts),
+            'vcycles_mean': float(np.mean(np.concatenate(nits)))}
     print(json.dumps(line), flush=True)
 
 

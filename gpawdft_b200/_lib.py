@@ -30,7 +30,8 @@ EXPORTS = [
     'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_add_scalar',
     'gpw_poisson_new', 'gpw_poisson_solve', 'gpw_poisson_last_stats',
     'gpw_poisson_time_level0', 'gpw_poisson_set_inner_schedule',
-    'gpw_poisson_free',
+    'gpw_poisson_solve_many', 'gpw_poisson_last_latency',
+    'gpw_poisson_profile_iteration', 'gpw_poisson_free',
 ]
 
 _c_i64p = ctypes.POINTER(ctypes.c_int64)
@@ -83,6 +84,14 @@ _SIGS = {
                                                ctypes.c_int, _vp, _vp, _vp]),
     'gpw_poisson_set_inner_schedule': (ctypes.c_int, [_vp, _vp, _vp, _vp,
                                                       ctypes.c_int]),
+    'gpw_poisson_solve_many': (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp,
+                                              _vp, ctypes.c_int, ctypes.c_int,
+                                              _vp, _vp, _vp]),
+    'gpw_poisson_last_latency': (ctypes.c_int, [_vp, ctypes.c_int64, _vp, _vp]),
+    'gpw_poisson_profile_iteration': (ctypes.c_int, [_vp, ctypes.c_int64,
+                                                     ctypes.c_int, ctypes.c_int,
+                                                     _vp, ctypes.c_int, _vp,
+                                                     ctypes.c_int, _vp, _vp]),
     'gpw_poisson_free': (None, [_vp]),
 }
 

@@ -474,8 +474,9 @@ cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatc
 static bool k2_vec_ok(const TransferArgs& a) {
   auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
   auto view_ok = [](const GridView& v) { return v.s1 % 4 == 0 && v.s0 % 4 == 0 && v.sb % 4 == 0; };
-  // a warp covers 128 outputs: narrower rows leave lanes idle
-  if (a.vout.n[2] < 96) return false;
+  // a warp covers 128 outputs; rows down to ~32 points still run faster
+  // than the scalar kernel's one-point-per-thread form
+  if (a.vout.n[2] < 32) return false;
   if (!aligned(a.out) || !view_ok(a.vout)) return false;
   if (a.subtract && (!aligned(a.base) || !view_ok(a.vbase))) return false;
   return true;

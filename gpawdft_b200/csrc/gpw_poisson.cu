@@ -17,9 +17,12 @@
 // batched through every kernel (grid z = chunks x batch); a per-solve
 // `active` mask freezes solves that have converged, so each solve's result
 // and iteration count equal those of solving it alone.
+#include <algorithm>
 #include <cstring>
+#include <string>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "gpw_coarse.cuh"
@@ -43,11 +46,21 @@ struct Level {
   Workspace phi32[2], rho32, res32;
 };
 
+__device__ __forceinline__ int64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return (int64_t)t;
+}
+
+// The convergence test of solve_neutral after each iteration.  A solve that
+// stops records the device clock in tdone[b]; with a conditional handle the
+// kernel also sets the condition of the graph's device-side while loop.
 __global__ void converge_update_kernel(int nbatch, const double* __restrict__ sumsq, double dv,
                                        const double* __restrict__ eps, const int* __restrict__ maxiter_p,
                                        double* __restrict__ err,
                                        int* __restrict__ niter, unsigned char* __restrict__ active,
-                                       int* __restrict__ any_active) {
+                                       int* __restrict__ any_active, int64_t* __restrict__ tdone,
+                                       cudaGraphConditionalHandle cond, int use_cond) {
   __shared__ int any;
   const int maxiter = *maxiter_p;
   if (threadIdx.x == 0) any = 0;
@@ -62,10 +75,22 @@ __global__ void converge_update_kernel(int nbatch, const double* __restrict__ su
       atomicOr(&any, 1);
     } else {
       active[b] = 0;
+      if (tdone) tdone[b] = global_ns();
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0) *any_active = any;
+  if (threadIdx.x == 0) {
+    *any_active = any;
+    if (use_cond) cudaGraphSetConditional(cond, any ? 1u : 0u);
+  }
+}
+
+__global__ void stamp_kernel(int64_t* t) { *t = global_ns(); }
+
+template <typename T>
+__global__ void copy_kernel(int64_t n, const T* __restrict__ x, T* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = x[i];
 }
 
 __global__ void to_f32_neg_kernel(int64_t n, const double* __restrict__ x, float* __restrict__ y,
@@ -98,7 +123,7 @@ struct gpw_poisson {
   int lc[2] = {0, 0};
   CoarseArgs cargs[2];
   size_t csmem[2] = {0, 0};
-  Workspace d_err, d_eps, d_niter, d_active, d_any, d_r64, d_gs_old, d_maxiter;
+  Workspace d_err, d_eps, d_niter, d_active, d_any, d_r64, d_gs_old, d_maxiter, d_tdone, d_t0;
   SumScratch sums;
   int* h_any = nullptr;  // pinned
   struct GraphKey {
@@ -108,9 +133,15 @@ struct gpw_poisson {
   };
   std::map<GraphKey, cudaGraphExec_t> graphs;
   std::map<GraphKey, int64_t> graph_kernels;  // kernel nodes per graph
+  // the whole convergence loop as one graph: a conditional while node whose
+  // body is one iteration (null where conditional nodes are unavailable)
+  std::map<GraphKey, cudaGraphExec_t> loops;
   int64_t last_kernels = 0, last_graphs = 0;
+  bool device_loop = true;  // use the device-side loop when it can be built
   ~gpw_poisson() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : loops)
+      if (kv.second) cudaGraphExecDestroy(kv.second);
     if (h_any) cudaFreeHost(h_any);
   }
 };
@@ -123,9 +154,18 @@ struct Rec {
   cudaStream_t st;
   const unsigned char* active;
   bool tune = false;  // tuning pass: time the stencil launches' variants, launch nothing else
+  // profiling pass (eager launches): an event after every launch, labelled
+  std::vector<std::pair<std::string, cudaEvent_t>>* prof = nullptr;
   cudaError_t err = cudaSuccess;
   void ok(cudaError_t e) {
     if (err == cudaSuccess && e != cudaSuccess) err = e;
+  }
+  void tick(const std::string& label) {
+    if (!prof || tune) return;
+    cudaEvent_t ev;
+    if (cudaEventCreate(&ev) != cudaSuccess) return;
+    cudaEventRecord(ev, st);
+    prof->emplace_back(label, ev);
   }
   // one star / general stencil launch (or, in the tuning pass, its tuning)
   void stencil(const OpDesc& d, int dt, int mode, const void* in, void* out, const void* rho, const GridView& v,
@@ -166,6 +206,7 @@ int rec_relax(Rec& r, int l, int cur, const double* ws, int nsweeps, bool f32) {
   }
   for (int s = 0; s < nsweeps; ++s) {
     r.stencil(*L.op, dt, MODE_JACOBI, phi[cur].ptr, phi[1 - cur].ptr, rho, L.v, ws[s], GridSum{});
+    r.tick("L" + std::to_string(l) + (f32 ? " f32" : " f64") + " jacobi");
     cur = 1 - cur;
   }
   return cur;
@@ -191,6 +232,7 @@ int rec_lower(Rec& r, int l, const void* res, bool f32) {
     // levels l+1 .. L in one CTA per solve: rho_{l+1} in, phi_{l+1} out
     if (!r.tune) {
       r.ok(launch_transfer(*L.restr, dt, res, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st));
+      r.tick("L" + std::to_string(l) + " restrict");
       CoarseArgs ca = ps->cargs[p];
       ca.rho = crho.ptr;
       ca.vrho = C.v;
@@ -198,6 +240,7 @@ int rec_lower(Rec& r, int l, const void* res, bool f32) {
       ca.vphi = C.v;
       ca.active = r.active;
       r.ok(launch_coarse(dt, ca, ps->csmem[p], r.nb, r.st));
+      r.tick("L" + std::to_string(l + 1) + "+ coarse kernel");
     }
     return 0;
   }
@@ -210,9 +253,11 @@ int rec_lower(Rec& r, int l, const void* res, bool f32) {
       const RestrictSweep sw{cphi[0].ptr, first[0], C.op->coefs[0]};
       r.ok(launch_transfer(*L.restr, dt, res, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st,
                            &sw));
+      r.tick("L" + std::to_string(l) + " restrict+sweep");
     } else {
       r.ok(launch_transfer(*L.restr, dt, res, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st));
       r.ok(launch_zero(dt, C.v, cphi[0].ptr, r.nb, r.active, r.st));
+      r.tick("L" + std::to_string(l) + " restrict+zero");
     }
   }
   // the fused first sweep wrote buffer 0 as the result of sweep 1: the
@@ -241,11 +286,14 @@ int rec_vcycle(Rec& r, int l, int cur, bool f32, bool first_done) {
     cur = rec_relax(r, l, cur, L.wpre[p].data() + skip, (int)L.wpre[p].size() - skip, f32);
     // the residual's norm is not needed below level 0's convergence test
     r.stencil(*L.op, dt, MODE_RESIDUAL, phi[cur].ptr, res.ptr, rho.ptr, L.v, 1.0, GridSum{});
+    r.tick("L" + std::to_string(l) + (f32 ? " f32" : " f64") + " residual");
     const int ccur = rec_lower(r, l, res.ptr, f32);
     Boundary cbc = make_boundary(C.op->periodic, dt, nullptr);
-    if (!r.tune)
+    if (!r.tune) {
       r.ok(launch_transfer(*L.interp, dt, cphi[ccur].ptr, C.v, phi[1 - cur].ptr, L.v, r.nb, cbc, 1, phi[cur].ptr,
                            &L.v, r.active, r.st));
+      r.tick("L" + std::to_string(l) + " interpolate-subtract");
+    }
     cur = 1 - cur;
     return rec_relax(r, l, cur, L.wpost[p].data(), (int)L.wpost[p].size(), f32);
   }
@@ -405,6 +453,7 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
   int rc;
   if ((rc = ps->d_err.ensure(nbatch_max * 8)) || (rc = ps->d_eps.ensure(nbatch_max * 8)) ||
       (rc = ps->d_niter.ensure(nbatch_max * 4)) || (rc = ps->d_active.ensure(nbatch_max)) ||
+      (rc = ps->d_tdone.ensure(nbatch_max * 8)) || (rc = ps->d_t0.ensure(8)) ||
       (rc = ps->d_any.ensure(16)) || (rc = ps->d_maxiter.ensure(16)) || (rc = ps->d_r64.ensure((size_t)ps->lv[0].v.sb * nbatch_max * 8)))
     return rc;
   if (relax_method == 1) {
@@ -521,9 +570,12 @@ static bool fused_dc(const gpw_poisson* ps) {
 
 // tune = true: the autotuner's pass over the same stencil launches (before
 // capture, on the engine's buffers); nothing else is launched.
-static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStream_t st, bool tune = false) {
+static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStream_t st, bool tune = false,
+                                    const cudaGraphConditionalHandle* cond = nullptr,
+                                    std::vector<std::pair<std::string, cudaEvent_t>>* prof = nullptr) {
   Rec r{ps, nb, st, (const unsigned char*)ps->d_active.ptr};
   r.tune = tune;
+  r.prof = prof;
   Level& L0 = ps->lv[0];
   const int64_t per = L0.v.sb;
   const int64_t n = per * nb;
@@ -534,13 +586,17 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStrea
     converge_update_kernel<<<1, 256, 0, st>>>(nb, ps->sums.gs().result, ps->dv, (const double*)ps->d_eps.ptr,
                                               (const int*)ps->d_maxiter.ptr, (double*)ps->d_err.ptr,
                                               (int*)ps->d_niter.ptr, (unsigned char*)ps->d_active.ptr,
-                                              (int*)ps->d_any.ptr);
+                                              (int*)ps->d_any.ptr, (int64_t*)ps->d_tdone.ptr,
+                                              cond ? *cond : cudaGraphConditionalHandle{}, cond ? 1 : 0);
     r.ok(cudaGetLastError());
+    r.tick("convergence update");
   };
   if (prec == 0) {
     const int cur = rec_vcycle(r, 0, 0, false);
-    if (cur != 0 && !tune)
-      r.ok(cudaMemcpyAsync(L0.phi[0].ptr, L0.phi[1].ptr, n * 8, cudaMemcpyDeviceToDevice, st));
+    if (cur != 0 && !tune) {  // odd ping-pong parity: the iterate goes back to buffer 0
+      copy_kernel<double><<<blocks, thr, 0, st>>>(n, (const double*)L0.phi[1].ptr, (double*)L0.phi[0].ptr);
+      r.ok(cudaGetLastError());
+    }
   } else if (fused_dc(ps)) {
     // Fused defect correction.  On entry L0.rho32 holds rhs = -(A phi - rho)
     // and L0.phi32[0] the first level-0 sweep from zero (both written by the
@@ -552,17 +608,22 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStrea
     const std::vector<double>& wpost = L0.wpost[1];
     int cur = rec_relax(r, 0, 0, wpre.data() + 1, (int)wpre.size() - 1, true);
     r.stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[cur].ptr, L0.res32.ptr, L0.rho32.ptr, L0.v, 1.0, GridSum{});
+    r.tick("L0 f32 residual");
     const int ccur = rec_lower(r, 0, L0.res32.ptr, true);
     Boundary cbc = make_boundary(C.op->periodic, GPW_F32, nullptr);
-    if (!tune)
+    if (!tune) {
       r.ok(launch_transfer(*L0.interp, GPW_F32, C.phi32[ccur].ptr, C.v, L0.phi32[1 - cur].ptr, L0.v, nb, cbc, 1,
                            L0.phi32[cur].ptr, &L0.v, r.active, st));
+      r.tick("L0 interpolate-subtract");
+    }
     cur = 1 - cur;
     cur = rec_relax(r, 0, cur, wpost.data(), (int)wpost.size() - 1, true);
     r.stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[cur].ptr, L0.v, nullptr, L0.phi[0].ptr, L0.rho32.ptr,
                  wpost.back(), 0.0, GridSum{});
+    r.tick("L0 f32 jacobi + phi64 update");
     r.stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr, 1.0,
                  wpre[0], ps->sums.gs());
+    r.tick("L0 f64 defect + first sweep");
     converge();
     return r.err;
   } else {
@@ -585,64 +646,128 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStrea
   // (the float64 residual itself is kept only as the next defect-correction right-hand side)
   r.stencil(*L0.op, GPW_F64, MODE_RESIDUAL, L0.phi[0].ptr, prec == 1 ? ps->d_r64.ptr : nullptr, L0.rho.ptr, L0.v,
             1.0, ps->sums.gs());
+  r.tick("L0 f64 residual + norm");
   converge();
   return r.err;
 }
 
-int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t nbatch, const double* eps, int maxiter,
-                      int precision, int* niter, double* error, gpw_stream stream) {
-  if (!ps || !phi || !rho || !eps || !niter || !error) return fail(GPW_EINVAL, "null argument");
-  if (nbatch < 1 || nbatch > ps->nbmax) return fail(GPW_EINVAL, "poisson: nbatch out of range");
-  if (precision != 0 && precision != 1) return fail(GPW_EINVAL, "poisson: precision must be 0 or 1");
-  if (precision == 1 && ps->relax_method != 2) return fail(GPW_ENOTSUP, "poisson: float32 form needs Jacobi");
-  if (maxiter < 1) return fail(GPW_EINVAL, "poisson: maxiter < 1");
-  cudaStream_t st = (cudaStream_t)stream;
-  Level& L0 = ps->lv[0];
-  const int nb = (int)nbatch;
-  int rc;
-  if (precision == 1 && (rc = ensure_f32(ps))) return rc;
-  cudaError_t e;
-  // get (or capture) the graph of one iteration for this batch size
-  gpw_poisson::GraphKey key{nbatch, precision};
-  auto it = ps->graphs.find(key);
-  if (it == ps->graphs.end()) {
-    // autotune the stencil launches of the iteration on the engine's own
-    // buffers (before the inputs are copied in), then capture it
-    cudaError_t te = record_iteration(ps, nb, precision, st, true);
-    if (te == cudaSuccess) te = cudaStreamSynchronize(st);
-    if (te != cudaSuccess) return cuda_fail(te, "stencil autotuning");
-    cudaGraph_t g;
-    cudaStream_t cs;
-    if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e, "stream");
-    if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
-      cudaStreamDestroy(cs);
-      return cuda_fail(e, "begin capture");
-    }
-    cudaError_t re = record_iteration(ps, nb, precision, cs);
-    e = cudaStreamEndCapture(cs, &g);
-    cudaStreamDestroy(cs);
-    if (re != cudaSuccess) return cuda_fail(re, "record V-cycle");
-    if (e != cudaSuccess) return cuda_fail(e, "end capture");
-    size_t nnodes = 0;
-    int64_t nkern = 0;
-    if (cudaGraphGetNodes(g, nullptr, &nnodes) == cudaSuccess && nnodes) {
-      std::vector<cudaGraphNode_t> nodes(nnodes);
-      if (cudaGraphGetNodes(g, nodes.data(), &nnodes) == cudaSuccess)
-        for (auto n : nodes) {
-          cudaGraphNodeType t;
-          if (cudaGraphNodeGetType(n, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nkern;
-        }
-    }
-    cudaGraphExec_t ge;
-    e = cudaGraphInstantiate(&ge, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
-    it = ps->graphs.emplace(key, ge).first;
-    ps->graph_kernels[key] = nkern;
+static int64_t count_kernel_nodes(cudaGraph_t g) {
+  size_t nnodes = 0;
+  int64_t nkern = 0;
+  if (cudaGraphGetNodes(g, nullptr, &nnodes) == cudaSuccess && nnodes) {
+    std::vector<cudaGraphNode_t> nodes(nnodes);
+    if (cudaGraphGetNodes(g, nodes.data(), &nnodes) == cudaSuccess)
+      for (auto n : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(n, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nkern;
+      }
   }
-  // state: eps, niter = 1, active = 1
+  return nkern;
+}
+
+// The graph of one iteration for (batch size, form), captured on first use
+// after the autotuning pass over its stencil launches.
+static int iteration_graph(gpw_poisson* ps, int nb, int prec, cudaStream_t st, cudaGraphExec_t* out) {
+  gpw_poisson::GraphKey key{nb, prec};
+  auto it = ps->graphs.find(key);
+  if (it != ps->graphs.end()) {
+    *out = it->second;
+    return GPW_OK;
+  }
+  // autotune the stencil launches of the iteration on the engine's own
+  // buffers (before the inputs are copied in), then capture it
+  cudaError_t e = record_iteration(ps, nb, prec, st, true);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "stencil autotuning");
+  cudaGraph_t g;
+  cudaStream_t cs;
+  if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e, "stream");
+  if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    return cuda_fail(e, "begin capture");
+  }
+  cudaError_t re = record_iteration(ps, nb, prec, cs);
+  e = cudaStreamEndCapture(cs, &g);
+  cudaStreamDestroy(cs);
+  if (re != cudaSuccess) return cuda_fail(re, "record V-cycle");
+  if (e != cudaSuccess) return cuda_fail(e, "end capture");
+  const int64_t nkern = count_kernel_nodes(g);
+  cudaGraphExec_t ge;
+  e = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+  ps->graphs.emplace(key, ge);
+  ps->graph_kernels[key] = nkern;
+  *out = ge;
+  return GPW_OK;
+}
+
+// Capture one iteration of engine `ps` into `body`, the child graph of a
+// conditional while node whose condition the iteration's convergence kernel
+// sets (loop while any solve of the batch is active).
+static cudaError_t capture_loop_body(gpw_poisson* ps, int nb, int prec, cudaGraph_t body,
+                                     cudaGraphConditionalHandle h) {
+  cudaStream_t cs;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    return e;
+  }
+  cudaError_t re = record_iteration(ps, nb, prec, cs, false, &h);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(cs, &g);
+  cudaStreamDestroy(cs);
+  return re != cudaSuccess ? re : e;
+}
+
+// Add a while node running engine ps's iterations to `parent` (after `dep`
+// when given); returns the node.
+static cudaError_t add_loop_node(gpw_poisson* ps, int nb, int prec, cudaGraph_t parent, const cudaGraphNode_t* dep,
+                                 cudaGraphNode_t* node) {
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, parent, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  e = cudaGraphAddNode(node, parent, dep, dep ? 1 : 0, &np);
+  if (e != cudaSuccess) return e;
+  return capture_loop_body(ps, nb, prec, np.conditional.phGraph_out[0], h);
+}
+
+// The device-side convergence loop for (batch size, form): null when
+// conditional graph nodes are not available (the host then replays the
+// iteration graph).
+static cudaGraphExec_t loop_graph(gpw_poisson* ps, int nb, int prec) {
+  gpw_poisson::GraphKey key{nb, prec};
+  auto it = ps->loops.find(key);
+  if (it != ps->loops.end()) return it->second;
+  cudaGraphExec_t ge = nullptr;
+  cudaGraph_t parent;
+  if (cudaGraphCreate(&parent, 0) == cudaSuccess) {
+    cudaGraphNode_t node;
+    if (add_loop_node(ps, nb, prec, parent, nullptr, &node) != cudaSuccess ||
+        cudaGraphInstantiate(&ge, parent, 0) != cudaSuccess)
+      ge = nullptr;
+    cudaGraphDestroy(parent);
+  }
+  cudaGetLastError();  // a failed attempt leaves no sticky state
+  ps->loops[key] = ge;
+  return ge;
+}
+
+// Solve-state set-up and inputs: eps, niter = 1, active = 1, phi / rho
+// copied into the engine layout, and (float32 form) the initial defect.
+static int solve_prologue(gpw_poisson* ps, double* phi, const double* rho, int nb, const double* eps, int maxiter,
+                          int precision, cudaStream_t st) {
+  Level& L0 = ps->lv[0];
   std::vector<int> ones(nb, 1);
   std::vector<unsigned char> act(nb, 1);
+  cudaError_t e;
   if ((e = cudaMemcpyAsync(ps->d_eps.ptr, eps, nb * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(ps->d_niter.ptr, ones.data(), nb * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(ps->d_active.ptr, act.data(), nb, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
@@ -652,6 +777,9 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
       (e = cudaMemcpy2DAsync(L0.rho.ptr, L0.v.s1 * 8, rho, (size_t)L0.v.n[2] * 8, (size_t)L0.v.n[2] * 8,
                              (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return cuda_fail(e, "poisson setup copies");
+  // the host copies above stage from pageable memory: wait for them before
+  // the vectors go out of scope
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "poisson setup copies");
   if (precision == 1 && fused_dc(ps)) {
     // initial defect: float32 rhs and first level-0 sweep, fused
     e = launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr, nb,
@@ -664,18 +792,15 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
                        bc, 1.0, (const unsigned char*)ps->d_active.ptr, ps->sums.gs(), st);
     if (e != cudaSuccess) return cuda_fail(e, "poisson initial residual");
   }
-  ps->last_kernels = (precision == 1) ? 1 : 0;
-  ps->last_graphs = 0;
-  // replay until no solve of the batch is active
-  for (int iter = 0; iter < maxiter + 1; ++iter) {
-    if ((e = cudaGraphLaunch(it->second, st)) != cudaSuccess) return cuda_fail(e, "graph launch");
-    ps->last_graphs += 1;
-    ps->last_kernels += ps->graph_kernels[key];
-    if ((e = cudaMemcpyAsync(ps->h_any, ps->d_any.ptr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-      return cuda_fail(e, "flag copy");
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "V-cycle");
-    if (!*ps->h_any) break;
-  }
+  stamp_kernel<<<1, 1, 0, st>>>((int64_t*)ps->d_t0.ptr);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "stamp");
+  return GPW_OK;
+}
+
+static int solve_epilogue(gpw_poisson* ps, double* phi, int nb, int maxiter, int* niter, double* error,
+                          cudaStream_t st) {
+  Level& L0 = ps->lv[0];
+  cudaError_t e;
   if ((e = cudaMemcpy2DAsync(phi, (size_t)L0.v.n[2] * 8, L0.phi[0].ptr, L0.v.s1 * 8, (size_t)L0.v.n[2] * 8,
                              (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(niter, ps->d_niter.ptr, nb * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
@@ -685,6 +810,155 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
   for (int b = 0; b < nb; ++b)
     if (niter[b] >= maxiter) return fail(GPW_ECONV, "Poisson solver did not converge in maxiter iterations");
   return GPW_OK;
+}
+
+static int check_solve_args(gpw_poisson* ps, int64_t nbatch, int precision, int maxiter) {
+  if (nbatch < 1 || nbatch > ps->nbmax) return fail(GPW_EINVAL, "poisson: nbatch out of range");
+  if (precision != 0 && precision != 1) return fail(GPW_EINVAL, "poisson: precision must be 0 or 1");
+  if (precision == 1 && ps->relax_method != 2) return fail(GPW_ENOTSUP, "poisson: float32 form needs Jacobi");
+  if (maxiter < 1) return fail(GPW_EINVAL, "poisson: maxiter < 1");
+  int rc;
+  if (precision == 1 && (rc = ensure_f32(ps))) return rc;
+  return GPW_OK;
+}
+
+int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t nbatch, const double* eps, int maxiter,
+                      int precision, int* niter, double* error, gpw_stream stream) {
+  if (!ps || !phi || !rho || !eps || !niter || !error) return fail(GPW_EINVAL, "null argument");
+  int rc = check_solve_args(ps, nbatch, precision, maxiter);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = (int)nbatch;
+  gpw_poisson::GraphKey key{nbatch, precision};
+  cudaGraphExec_t iter = nullptr;
+  if ((rc = iteration_graph(ps, nb, precision, st, &iter))) return rc;
+  cudaGraphExec_t loop = ps->device_loop ? loop_graph(ps, nb, precision) : nullptr;
+  if ((rc = solve_prologue(ps, phi, rho, nb, eps, maxiter, precision, st))) return rc;
+  ps->last_kernels = (precision == 1) ? 2 : 1;
+  ps->last_graphs = 0;
+  cudaError_t e;
+  if (loop) {
+    // the whole convergence loop on the device: one graph launch
+    if ((e = cudaGraphLaunch(loop, st)) != cudaSuccess) return cuda_fail(e, "loop graph launch");
+  } else {
+    // replay until no solve of the batch is active
+    for (int it = 0; it < maxiter + 1; ++it) {
+      if ((e = cudaGraphLaunch(iter, st)) != cudaSuccess) return cuda_fail(e, "graph launch");
+      ps->last_graphs += 1;
+      ps->last_kernels += ps->graph_kernels[key];
+      if ((e = cudaMemcpyAsync(ps->h_any, ps->d_any.ptr, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "flag copy");
+      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "V-cycle");
+      if (!*ps->h_any) break;
+    }
+  }
+  rc = solve_epilogue(ps, phi, nb, maxiter, niter, error, st);
+  if (loop) {
+    // iterations run = the largest iteration count of the batch
+    int64_t mx = 0;
+    for (int b = 0; b < nb; ++b) mx = std::max<int64_t>(mx, niter[b]);
+    ps->last_graphs = mx;
+    ps->last_kernels += mx * ps->graph_kernels[key];
+  }
+  return rc;
+}
+
+// Per-solve latency of the last solve: device time from the start of the
+// iterations to the end of the iteration in which each solve converged.
+extern "C" int gpw_poisson_last_latency(gpw_poisson* ps, int64_t nbatch, double* ms, gpw_stream stream) {
+  if (!ps || !ms) return fail(GPW_EINVAL, "null argument");
+  if (nbatch < 1 || nbatch > ps->nbmax) return fail(GPW_EINVAL, "poisson: nbatch out of range");
+  std::vector<int64_t> t(nbatch + 1);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(t.data(), ps->d_tdone.ptr, nbatch * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(t.data() + nbatch, ps->d_t0.ptr, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cuda_fail(e, "latency copies");
+  for (int64_t b = 0; b < nbatch; ++b) ms[b] = (double)(t[b] - t[nbatch]) * 1e-6;
+  return GPW_OK;
+}
+
+// Several engines (e.g. one per grid size) solved by ONE graph launch: a
+// parent graph with one device-side while loop per engine; the loops are
+// independent branches and run concurrently.  Arguments are per engine as
+// in gpw_poisson_solve.  Cached per (engines, batch sizes, form).
+struct MultiKey {
+  std::vector<const void*> eng;
+  std::vector<int> nb;
+  int prec;
+  bool operator<(const MultiKey& o) const {
+    if (prec != o.prec) return prec < o.prec;
+    if (eng != o.eng) return eng < o.eng;
+    return nb < o.nb;
+  }
+};
+static std::mutex g_multi_mu;
+static std::map<MultiKey, cudaGraphExec_t> g_multi;
+
+extern "C" int gpw_poisson_solve_many(int nengines, gpw_poisson* const* engines, double* const* phis,
+                                      const double* const* rhos, const int64_t* nbatch,
+                                      const double* const* eps, int maxiter, int precision, int* const* niters,
+                                      double* const* errors, gpw_stream stream) {
+  if (nengines < 1 || !engines || !phis || !rhos || !nbatch || !eps || !niters || !errors)
+    return fail(GPW_EINVAL, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  MultiKey key;
+  key.prec = precision;
+  int rc;
+  for (int i = 0; i < nengines; ++i) {
+    gpw_poisson* ps = engines[i];
+    if (!ps || !phis[i] || !rhos[i] || !eps[i] || !niters[i] || !errors[i]) return fail(GPW_EINVAL, "null argument");
+    for (int j = 0; j < i; ++j)
+      if (engines[j] == ps) return fail(GPW_EINVAL, "solve_many: an engine appears twice");
+    if ((rc = check_solve_args(ps, nbatch[i], precision, maxiter))) return rc;
+    cudaGraphExec_t iter;
+    if ((rc = iteration_graph(ps, (int)nbatch[i], precision, st, &iter))) return rc;  // tunes the stencils
+    key.eng.push_back(ps);
+    key.nb.push_back((int)nbatch[i]);
+  }
+  cudaGraphExec_t ge = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_multi_mu);
+    auto it = g_multi.find(key);
+    if (it != g_multi.end()) ge = it->second;
+  }
+  if (!ge) {
+    cudaGraph_t parent;
+    cudaError_t e = cudaGraphCreate(&parent, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "graph create");
+    for (int i = 0; i < nengines && e == cudaSuccess; ++i) {
+      cudaGraphNode_t node;
+      e = add_loop_node(engines[i], (int)nbatch[i], precision, parent, nullptr, &node);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, parent, 0);
+    cudaGraphDestroy(parent);
+    if (e != cudaSuccess) return cuda_fail(e, "solve_many: device-side loop graph");
+    std::lock_guard<std::mutex> lock(g_multi_mu);
+    g_multi[key] = ge;
+  }
+  for (int i = 0; i < nengines; ++i)
+    if ((rc = solve_prologue(engines[i], phis[i], rhos[i], (int)nbatch[i], eps[i], maxiter, precision, st)))
+      return rc;
+  // one clock origin for every engine's latencies: just before the launch
+  stamp_kernel<<<1, 1, 0, st>>>((int64_t*)engines[0]->d_t0.ptr);
+  for (int i = 1; i < nengines; ++i) {
+    cudaError_t e = cudaMemcpyAsync(engines[i]->d_t0.ptr, engines[0]->d_t0.ptr, 8, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e, "clock origin");
+  }
+  cudaError_t e = cudaGraphLaunch(ge, st);
+  if (e != cudaSuccess) return cuda_fail(e, "solve_many launch");
+  int first_rc = GPW_OK;
+  for (int i = 0; i < nengines; ++i) {
+    gpw_poisson* ps = engines[i];
+    rc = solve_epilogue(ps, phis[i], (int)nbatch[i], maxiter, niters[i], errors[i], st);
+    if (rc && !first_rc) first_rc = rc;
+    int64_t mx = 0;
+    for (int b = 0; b < nbatch[i]; ++b) mx = std::max<int64_t>(mx, niters[i][b]);
+    ps->last_graphs = mx;
+    ps->last_kernels = mx * ps->graph_kernels[gpw_poisson::GraphKey{nbatch[i], precision}] + (precision ? 2 : 1);
+  }
+  return first_rc;
 }
 
 // Float32 inner V-cycle schedule of the defect-correction form (precision 1):
@@ -727,5 +1001,62 @@ extern "C" int gpw_poisson_set_inner_schedule(gpw_poisson* ps, const int* npre, 
       ++it;
     }
   }
+  return GPW_OK;
+}
+
+// Live per-launch breakdown of one iteration: the iteration's launches run
+// eagerly on the engine's buffers (contents overwritten; call between
+// solves, after a solve of this batch size and form tuned the stencils),
+// each followed by an event.  Writes up to `cap` entries: labels
+// (NUL-separated into `labels`, `labels_len` bytes) and milliseconds.
+extern "C" int gpw_poisson_profile_iteration(gpw_poisson* ps, int64_t nbatch, int precision, int reps, char* labels,
+                                             int labels_len, double* ms, int cap, int* count, gpw_stream stream) {
+  if (!ps || !labels || !ms || !count || cap < 1 || reps < 1) return fail(GPW_EINVAL, "null argument");
+  int rc = check_solve_args(ps, nbatch, precision, 1);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = (int)nbatch;
+  std::vector<unsigned char> act(nb, 1);
+  std::vector<std::string> names;
+  std::vector<double> acc;
+  cudaError_t e;
+  for (int rep = 0; rep <= reps; ++rep) {
+    // every solve active (the state of a first iteration)
+    e = cudaMemcpyAsync(ps->d_active.ptr, act.data(), nb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "profile setup");
+    std::vector<std::pair<std::string, cudaEvent_t>> ev;
+    cudaEvent_t e0;
+    cudaEventCreate(&e0);
+    cudaEventRecord(e0, st);
+    cudaError_t re = record_iteration(ps, nb, precision, st, false, nullptr, &ev);
+    e = cudaStreamSynchronize(st);
+    if (re == cudaSuccess && e == cudaSuccess && rep > 0) {  // rep 0 warms up
+      cudaEvent_t prev = e0;
+      for (size_t i = 0; i < ev.size(); ++i) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, prev, ev[i].second);
+        prev = ev[i].second;
+        if (rep == 1) {
+          names.push_back(ev[i].first);
+          acc.push_back(0.0);
+        }
+        if (i < acc.size()) acc[i] += t;
+      }
+    }
+    cudaEventDestroy(e0);
+    for (auto& x : ev) cudaEventDestroy(x.second);
+    if (re != cudaSuccess) return cuda_fail(re, "profile iteration");
+    if (e != cudaSuccess) return cuda_fail(e, "profile sync");
+  }
+  int n = 0, off = 0;
+  for (size_t i = 0; i < names.size() && n < cap; ++i) {
+    const int len = (int)names[i].size() + 1;
+    if (off + len > labels_len) break;
+    std::memcpy(labels + off, names[i].c_str(), len);
+    off += len;
+    ms[n++] = acc[i] / reps;
+  }
+  *count = n;
   return GPW_OK;
 }

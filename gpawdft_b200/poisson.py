@@ -378,6 +378,32 @@ class FDPoissonSolver:
                                 -sums[b] / npts)
         return niter
 
+    def profile_iteration(self, nbatch=None, reps=5):
+        """Live per-launch times (ms) of one outer iteration on the engine's
+        buffers: a list of (label, ms).  Call after a solve of this batch
+        size (it overwrites the engine's buffers)."""
+        nb = self._engine[1] if nbatch is None else int(nbatch)
+        cap = 256
+        labels = ctypes.create_string_buffer(cap * 64)
+        ms = np.zeros(cap)
+        count = ctypes.c_int()
+        _lib.check(self._lib.gpw_poisson_profile_iteration(
+            self._engine[0], nb, _PREC[self.precision], int(reps), labels,
+            cap * 64, ms.ctypes.data, cap, ctypes.byref(count),
+            arrays.stream()))
+        names = labels.raw.split(b'\0')[:count.value]
+        return [(n.decode(), float(t)) for n, t in zip(names, ms)]
+
+    def last_latency(self, nbatch=None):
+        """Per-solve device latency (ms) of the last solve: from the start of
+        the iterations to the end of the iteration in which each solve
+        converged."""
+        nb = self._engine[1] if nbatch is None else int(nbatch)
+        ms = np.zeros(nb)
+        _lib.check(self._lib.gpw_poisson_last_latency(
+            self._engine[0], nb, ms.ctypes.data, arrays.stream()))
+        return ms
+
     def solve_batch(self, phi_b, rho_b, eps=None):
         """Independent neutral solves of a batch (nb, *n_c) on one grid.
 
@@ -409,3 +435,61 @@ class FDPoissonSolver:
     def __repr__(self):
         return 'PoissonSolver(relax=\'%s\', nn=%s, eps=%e)' % (
             self.relax, repr(self.nn), self.eps)
+
+
+def solve_many(solvers, phis, rhos, eps):
+    """Independent neutral solves on several grids in ONE graph launch.
+
+    ``solvers[i]`` is an initialised FDPoissonSolver (its own grid, same
+    ``precision`` for all), ``phis[i]`` / ``rhos[i]`` device or host arrays of
+    shape (nb_i, *n_c), ``eps[i]`` the per-solve tolerances (scalar or nb_i
+    values).  Every solver's convergence loop runs on the device as one
+    branch of a single CUDA graph (gpw_poisson_solve_many).  Returns the
+    per-solve iteration counts.
+    """
+    n = len(solvers)
+    if not (len(phis) == len(rhos) == len(eps) == n) or n == 0:
+        raise ValueError('solvers, phis, rhos and eps must have one entry per '
+                         'solver')
+    prec = {s.precision for s in solvers}
+    if len(prec) != 1:
+        raise ValueError('all solvers must use the same precision')
+    lib = _lib.load()
+    handles, phid, rhod, nbs, epsa, nits, errs, hosts = [], [], [], [], [], \
+        [], [], []
+    for s, phi, rho, e in zip(solvers, phis, rhos, eps):
+        if s.B is not None or s.gd.pbc_c.any():
+            raise NotImplementedError('solve_many: zero-boundary grids with '
+                                      'the nn=1..6 stencils only')
+        nb = int(phi.shape[0])
+        s._make_engine(nb)
+        p = arrays.to_device(phi)
+        r = arrays.to_device(rho)
+        handles.append(s._engine[0])
+        phid.append(p)
+        rhod.append(r)
+        hosts.append(phi)
+        nbs.append(nb)
+        epsa.append(np.ascontiguousarray(np.broadcast_to(
+            np.asarray(e, float), (nb,))))
+        nits.append(np.zeros(nb, np.int32))
+        errs.append(np.zeros(nb))
+    VP = ctypes.c_void_p
+    rc = lib.gpw_poisson_solve_many(
+        n, (VP * n)(*[h.value for h in handles]),
+        (VP * n)(*[arrays.ptr(p) for p in phid]),
+        (VP * n)(*[arrays.ptr(r) for r in rhod]),
+        np.ascontiguousarray(nbs, np.int64).ctypes.data,
+        (VP * n)(*[a.ctypes.data for a in epsa]), int(solvers[0].maxiter),
+        _PREC[solvers[0].precision], (VP * n)(*[a.ctypes.data for a in nits]),
+        (VP * n)(*[a.ctypes.data for a in errs]), arrays.stream())
+    for s, e in zip(solvers, errs):
+        s.last_errors = e
+    if rc == _lib.GPW_ECONV:
+        raise PoissonConvergenceError('Poisson solver did not converge in %d '
+                                      'iterations!' % solvers[0].maxiter)
+    _lib.check(rc)
+    for h, p in zip(hosts, phid):
+        if not arrays.is_device(h):
+            arrays.writeback(h, p)
+    return nits

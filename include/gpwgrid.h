@@ -200,6 +200,27 @@ int gpw_poisson_solve(gpw_poisson *ps, double *phi, const double *rho,
                       int precision, int *niter, double *error,
                       gpw_stream stream);
 
+/* Several engines (e.g. one per grid size) solved by ONE graph launch (no
+ * counterpart in the reference, which solves one grid per call): each
+ * engine's convergence loop runs on the device as a conditional while node
+ * of one parent graph, the loops being independent branches that run
+ * concurrently.  Arguments per engine i as in gpw_poisson_solve (phis[i],
+ * rhos[i]: nbatch[i] grids of that engine's shape).  The graph is built on
+ * the first call for a set of (engines, batch sizes, precision) and reused.
+ * Synchronises the stream; GPW_ECONV if any solve reached maxiter.          */
+int gpw_poisson_solve_many(int nengines, gpw_poisson *const *engines,
+                           double *const *phis, const double *const *rhos,
+                           const int64_t *nbatch, const double *const *eps,
+                           int maxiter, int precision, int *const *niters,
+                           double *const *errors, gpw_stream stream);
+
+/* Per-solve latency of the engine's last solve (milliseconds of device time
+ * from the start of the iterations to the end of the iteration in which
+ * each of the `nbatch` solves converged; for gpw_poisson_solve_many, from
+ * the start of the one launch).  No counterpart in the reference.          */
+int gpw_poisson_last_latency(gpw_poisson *ps, int64_t nbatch, double *ms,
+                             gpw_stream stream);
+
 /* Counters of the last gpw_poisson_solve call: device kernels launched
  * (graph kernel nodes x replays + direct launches) and graph replays.       */
 int gpw_poisson_last_stats(const gpw_poisson *ps, int64_t *kernel_launches,
@@ -228,6 +249,19 @@ int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
 int gpw_poisson_set_inner_schedule(gpw_poisson *ps, const int *npre,
                                    const int *npost, const double *weights,
                                    int nweights);
+
+/* Live per-launch breakdown of one iteration of the engine (a profiling aid
+ * with no counterpart in the reference beyond its Timer): the iteration's
+ * launches run eagerly on the engine's buffers (contents overwritten; call
+ * between solves, after a solve of this batch size and precision), each
+ * followed by a CUDA event; averaged over `reps` repetitions after one
+ * warm-up.  Writes up to `cap` entries: NUL-separated labels into `labels`
+ * (`labels_len` bytes), milliseconds into ms[], the entry count into
+ * *count.  Synchronises the stream.                                        */
+int gpw_poisson_profile_iteration(gpw_poisson *ps, int64_t nbatch,
+                                  int precision, int reps, char *labels,
+                                  int labels_len, double *ms, int cap,
+                                  int *count, gpw_stream stream);
 
 void gpw_poisson_free(gpw_poisson *ps);
 

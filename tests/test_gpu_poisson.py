@@ -222,3 +222,60 @@ def test_full_size_127_trajectory(cuda):
     assert n == on
     assert np.abs(phi - ophi).max() < 1e-11 * np.abs(ophi).max()
     assert abs(hartree(ogd, phi, rho) - hartree(ogd, ophi, rho)) < 1e-8
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_solve_many_equals_single(cuda, precision):
+    """Three grid sizes in one graph launch (device-side loops): every solve
+    equals its own single solve (same V-cycles, identical potential), and the
+    per-solve latencies are positive and ordered within the launch."""
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver, solve_many
+    sizes = [(32, 2), (40, 1), (48, 3)]
+    solvers, phis, rhos, epss = [], [], [], []
+    for k, (N, nb) in enumerate(sizes):
+        rl = []
+        for j in range(nb):
+            r, L = gaussian_density(N, 0.2, 4 + 2 * j, 100 * k + j)
+            rl.append(r)
+        gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+        ps = PoissonSolver(nn=3, batch=nb, precision=precision, maxiter=200)
+        ps.set_grid_descriptor(gd)
+        ps.initialize()
+        solvers.append(ps)
+        rhos.append(np.array(rl))
+        phis.append(np.zeros((nb,) + tuple(gd.n_c)))
+        epss.append([1e-20 * float(np.dot(r.ravel(), r.ravel())) * gd.dv
+                     for r in rl])
+    nits = solve_many(solvers, phis, rhos, epss)
+    for ps, phib, rhob, e, nit in zip(solvers, phis, rhos, epss, nits):
+        lat = ps.last_latency(len(nit))
+        assert (lat > 0).all()
+        for b in range(len(nit)):
+            phi = ps.gd.zeros()
+            n = ps.solve_neutral(phi, rhob[b], eps=e[b])
+            assert n == nit[b]
+            assert np.array_equal(phi, phib[b])
+
+
+def test_device_loop_latencies(cuda):
+    """One batched solve: per-solve latencies grow with the iteration count."""
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    N = 32
+    rhos = []
+    for s in range(3):
+        rho, L = gaussian_density(N, 0.2, 8, 60 + s)
+        rhos.append(rho)
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    ps = PoissonSolver(nn=3, batch=3, maxiter=200)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    eps = [1e-12, 1e-16, 1e-20]
+    eps = [e * float(np.dot(r.ravel(), r.ravel())) * gd.dv
+           for e, r in zip(eps, rhos)]
+    n = ps.solve_batch(np.zeros((3,) + tuple(gd.n_c)), np.array(rhos),
+                       eps=eps)
+    lat = ps.last_latency(3)
+    assert n[0] < n[1] < n[2]
+    assert 0 < lat[0] < lat[1] < lat[2]
