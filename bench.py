@@ -599,6 +599,99 @@ def run_uneven(args):
     print(json.dumps(line), flush=True)
 
 
+def run_learned(args):
+    """Learned warm start at N_c = 128 (127^3, h = 0.2 A): the U-Net is
+    trained on `--pairs` (default 20000) fresh (density, potential) pairs --
+    densities of 8-64 neutral Gaussians with widths log-uniform in 0.3-2.0 A
+    generated on the device, potentials from the float32 multigrid to
+    relative residual 1e-6 -- then, on held-out densities (batch of 16):
+    learned + float32 solves/s to relative residual 1e-10 (network
+    inference, judged first iteration and the rest of the multigrid solve
+    inside the timed region) vs the plain float64 method and the float32
+    form from a zero start; V-cycles saved; held-out potential error."""
+    import torch
+    from gpawdft_b200 import blas, learned
+    B = 16
+    net = learned.PoissonUNet(seed=0)
+    t0 = time.time()
+    hist = learned.train(net, pairs=args.pairs, batch=4, N_c=128, lr=1e-3,
+                         seed=6, log_every=500, logger=None)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    if args.save_weights:
+        net.save(args.save_weights)
+    sampler = learned.DensitySampler(N_c=128, seed=7)   # held out
+    rho = sampler.sample(B)
+    ps32 = learned.make_solver(128, batch=B, precision='fp32')
+    ps64 = learned.make_solver(128, batch=B, precision='fp64')
+    eps = learned.rel_eps(rho, ps32.gd.dv, 1e-10)
+    ref = torch.zeros_like(rho)
+    ps64.solve_batch(ref, rho, eps=eps)   # reference potentials
+    phi = torch.zeros_like(rho)
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        out = None
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps, out
+
+    def plain64():
+        phi.zero_()
+        return ps64.solve_batch(phi, rho, eps=eps)
+
+    def zero32():
+        phi.zero_()
+        return ps32.solve_batch(phi, rho, eps=eps)
+
+    def learned32():
+        phi0, used, k = learned.warm_start(net, ps32, rho)
+        n = ps32.solve_batch(phi0, rho, eps=eps) + k
+        phi.copy_(phi0)
+        return n, used
+
+    t64, n64 = timed(plain64, args.steps)
+    t32, n32 = timed(zero32, args.steps)
+    tl, (nl, used) = timed(learned32, args.steps)
+    d = phi - ref
+    final_err = np.sqrt(blas.vector_dots(d, d, B) /
+                        blas.vector_dots(ref, ref, B))
+    pred = net.predict(rho)
+    d = pred - ref
+    pred_err = np.sqrt(blas.vector_dots(d, d, B) /
+                       blas.vector_dots(ref, ref, B))
+    # inference alone (pack + forward + unpack)
+    t_inf, _ = timed(lambda: net.predict(rho), args.steps)
+    line = {'metric': 'poisson_solves_per_s_128^3_rel1e-10_learned_fp32',
+            'value': B / tl, 'unit': 'solves/s', 'higher_is_better': True,
+            'n_gpus': 1, 'steps': args.steps, 'warmup': 2,
+            'dtype': 'bf16 net + f32/f64 multigrid', 'data': 'synthetic',
+            'config': {'workload': 'learned warm start, N_c=128 (127^3), '
+                                   'U-Net 16/32/64/64, %d training pairs, '
+                                   'held-out batch %d' % (args.pairs, B)},
+            'plain_fp64': {'value': B / t64, 'vcycles_mean':
+                           float(np.mean(n64))},
+            'fp32_zero_start': {'value': B / t32, 'vcycles_mean':
+                                float(np.mean(n32))},
+            'learned_fp32': {'value': B / tl, 'vcycles_mean':
+                             float(np.mean(nl)), 'guess_kept':
+                             int(np.sum(used))},
+            'speedup_vs_plain_fp64': t64 / tl,
+            'vcycles_saved_vs_fp32_zero_start': float(np.mean(n32) -
+                                                      np.mean(nl)),
+            'heldout_prediction_rel_error': [float(x) for x in pred_err],
+            'final_potential_rel_error_vs_fp64': float(final_err.max()),
+            'inference_ms_batch': 1e3 * t_inf,
+            'train_s': t_train, 'train_loss_history': hist[-5:]}
+    print(json.dumps(line), flush=True)
+
+
 def run_bands(args):
     """256 complex Bloch bands on a 96^3 periodic grid (h = 0.18 A, random k,
     phase-wrapped halos): Laplace nn=3 (scale -1/2), Gradient x/y/z n=3,
@@ -672,13 +765,18 @@ def main():
     ap.add_argument('--batch', type=int, default=16)
     ap.add_argument('--precision', default='fp32', choices=['fp64', 'fp32'])
     ap.add_argument('--workload', default='poisson128',
-                    choices=['poisson128', 'mixed192', 'uneven512', 'bands96'])
+                    choices=['poisson128', 'mixed192', 'uneven512', 'bands96',
+                             'learned128'])
+    ap.add_argument('--pairs', type=int, default=20000,
+                    help='learned128: training pairs')
+    ap.add_argument('--save-weights', default=None,
+                    help='learned128: save the trained network (.npz)')
     ap.add_argument('--no-cpu', action='store_true',
                     help='skip the cpu_baseline sample')
     args = ap.parse_args()
     if args.workload != 'poisson128':
         {'mixed192': run_mixed192, 'uneven512': run_uneven,
-         'bands96': run_bands}[args.workload](args)
+         'bands96': run_bands, 'learned128': run_learned}[args.workload](args)
         return
     args.warmup = max(args.warmup, 3) if args.impl == 'ours' else args.warmup
     world = int(os.environ.get('WORLD_SIZE', '1'))

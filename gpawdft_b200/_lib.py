@@ -32,6 +32,13 @@ EXPORTS = [
     'gpw_poisson_time_level0', 'gpw_poisson_set_inner_schedule',
     'gpw_poisson_solve_many', 'gpw_poisson_last_latency',
     'gpw_poisson_profile_iteration', 'gpw_poisson_free',
+    'gpw_nn_conv3', 'gpw_nn_wgrad_scratch', 'gpw_nn_conv3_wgrad',
+    'gpw_nn_flip_weights', 'gpw_nn_gelu_backward', 'gpw_nn_pool2',
+    'gpw_nn_pool2_backward', 'gpw_nn_upsample2_add',
+    'gpw_nn_upsample2_backward', 'gpw_nn_head', 'gpw_nn_head_backward',
+    'gpw_nn_partials', 'gpw_nn_pack_input', 'gpw_nn_upsample_add_f32',
+    'gpw_nn_downsum_f32', 'gpw_nn_mse', 'gpw_nn_unpack_output', 'gpw_nn_adam',
+    'gpw_nn_gaussians', 'gpw_nn_channel_sum',
 ]
 
 _c_i64p = ctypes.POINTER(ctypes.c_int64)
@@ -93,6 +100,26 @@ _SIGS = {
                                                      _vp, ctypes.c_int, _vp,
                                                      ctypes.c_int, _vp, _vp]),
     'gpw_poisson_free': (None, [_vp]),
+    'gpw_nn_conv3': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    'gpw_nn_wgrad_scratch': (ctypes.c_int64, [ctypes.c_int, ctypes.c_int]),
+    'gpw_nn_conv3_wgrad': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    'gpw_nn_flip_weights': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    'gpw_nn_gelu_backward': (ctypes.c_int, [ctypes.c_int64, _vp, _vp, _vp, _vp]),
+    'gpw_nn_pool2': (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    'gpw_nn_pool2_backward': (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    'gpw_nn_upsample2_add': (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    'gpw_nn_upsample2_backward': (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    'gpw_nn_head': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
+    'gpw_nn_head_backward': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int64, _vp]),
+    'gpw_nn_partials': (ctypes.c_int, []),
+    'gpw_nn_channel_sum': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int64, _vp]),
+    'gpw_nn_pack_input': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    'gpw_nn_upsample_add_f32': (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    'gpw_nn_downsum_f32': (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    'gpw_nn_mse': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int64, _vp]),
+    'gpw_nn_unpack_output': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    'gpw_nn_adam': (ctypes.c_int, [ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    'gpw_nn_gaussians': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

@@ -349,7 +349,16 @@ class FDPoissonSolver:
             arrays.writeback(phi, phi_d)
         return int(niters[0])
 
-    def _run(self, phi_d, rho_d, nb, eps_list):
+    def iterate_batch(self, phi_b, rho_b, k):
+        """Exactly k outer iterations (V-cycles, or defect-correction steps)
+        on a batch of device tensors, whatever the residual; returns the
+        per-member error sum(r^2) dv after them."""
+        nb = int(phi_b.shape[0])
+        self._run(arrays.to_device(phi_b), arrays.to_device(rho_b), nb,
+                  [0.0] * nb, maxiter=int(k), exact=True)
+        return np.array(self.last_errors)
+
+    def _run(self, phi_d, rho_d, nb, eps_list, maxiter=None, exact=False):
         if self.B is not None:
             rho2 = arrays.empty_like_device(rho_d.shape,
                                             arrays.np_dtype_of(rho_d))
@@ -361,9 +370,12 @@ class FDPoissonSolver:
         err = np.zeros(nb, float)
         rc = self._lib.gpw_poisson_solve(
             self._engine[0], arrays.ptr(phi_d), arrays.ptr(rho_d), nb,
-            eps_a.ctypes.data, int(self.maxiter), _PREC[self.precision],
-            niter.ctypes.data, err.ctypes.data, arrays.stream())
+            eps_a.ctypes.data, int(maxiter or self.maxiter),
+            _PREC[self.precision], niter.ctypes.data, err.ctypes.data,
+            arrays.stream())
         self.last_errors = err
+        if exact and rc == _lib.GPW_ECONV:
+            rc = _lib.GPW_OK  # the requested iteration count, not a failure
         if rc == _lib.GPW_ECONV:
             raise PoissonConvergenceError(
                 'Poisson solver did not converge in %d iterations!' %
@@ -393,6 +405,15 @@ class FDPoissonSolver:
             arrays.stream()))
         names = labels.raw.split(b'\0')[:count.value]
         return [(n.decode(), float(t)) for n, t in zip(names, ms)]
+
+    def residual_norms(self, phi_b, rho_b):
+        """||A phi - rho||_2 of each member of a batch (level-0 operator,
+        device tensors (nb, *n_c))."""
+        out = np.zeros(phi_b.shape[0])
+        for b in range(phi_b.shape[0]):
+            out[b] = np.sqrt(float(
+                self.operators[0].residual(phi_b[b], rho_b[b])[0].item()))
+        return out
 
     def last_latency(self, nbatch=None):
         """Per-solve device latency (ms) of the last solve: from the start of

@@ -265,6 +265,91 @@ int gpw_poisson_profile_iteration(gpw_poisson *ps, int64_t nbatch,
 
 void gpw_poisson_free(gpw_poisson *ps);
 
+/* ------------------------------------------------------------ learned warm start */
+/* Kernels of the 3D convolutional U-Net that supplies the float32 solve's
+ * initial potential (no counterpart in the reference).  Activations are
+ * bf16 NDHWC ([B][D][H][W][C]), C in {16, 32, 64}; conv weights bf16
+ * [27 taps][cout][cin] with tap = (kd * 3 + kh) * 3 + kw; accumulation and
+ * every gradient reduction in fp32.  All calls are asynchronous on `stream`.*/
+
+/* 3x3x3 convolution, stride 1, zero padding 1 (cross-correlation), on the
+ * tensor cores: out = epilogue(conv(x, w) + bias + add); epilogue 0 linear,
+ * 1 GELU (erf form; z, if non-null, receives the pre-activation).  bias
+ * (fp32 [cout]) and add ([..][cout]) may be NULL.  The data gradient of a
+ * convolution is this call on the output gradient with the weights of
+ * gpw_nn_flip_weights (cin and cout swapped).                              */
+int gpw_nn_conv3(int cin, int cout, int epilogue, const void *x,
+                 const void *w, const float *bias, const void *add, void *z,
+                 void *out, int B, int D, int H, int W, gpw_stream stream);
+/* dw[27][cout][cin] (fp32) = sum over points of dz[p][co] x[p + tap][ci];
+ * scratch: gpw_nn_wgrad_scratch(cin, cout) floats of partial sums.        */
+int64_t gpw_nn_wgrad_scratch(int cin, int cout);
+int gpw_nn_conv3_wgrad(int cin, int cout, const void *x, const void *dz,
+                       float *dw, float *scratch, int64_t scratch_floats,
+                       int B, int D, int H, int W, gpw_stream stream);
+/* wt[tap][ci][co] = w[26 - tap][co][ci]                                     */
+int gpw_nn_flip_weights(int cin, int cout, const void *w, void *wt,
+                        gpw_stream stream);
+/* dz = da * GELU'(z), n elements                                            */
+int gpw_nn_gelu_backward(int64_t n, const void *z, const void *da, void *dz,
+                         gpw_stream stream);
+/* 2x2x2 average pooling of x (dims D, H, W, even) and its gradient
+ * (dx (+)= dy / 8 on the children)                                         */
+int gpw_nn_pool2(int c, const void *x, void *y, int B, int D, int H, int W,
+                 gpw_stream stream);
+int gpw_nn_pool2_backward(int c, const void *dy, void *dx, int B, int D,
+                          int H, int W, int accumulate, gpw_stream stream);
+/* y = nearest 2x upsampling of x (+ skip), y of dims D, H, W; gradient
+ * dx (+)= sum of the 2x2x2 children of dy                                   */
+int gpw_nn_upsample2_add(int c, const void *x, const void *skip, void *y,
+                         int B, int D, int H, int W, gpw_stream stream);
+int gpw_nn_upsample2_backward(int c, const void *dy, void *dx, int B, int D,
+                              int H, int W, int accumulate, gpw_stream stream);
+/* 1x1x1 head to one fp32 channel, c in {16, 64}: out[p] = w . x[p] + bias;
+ * backward: dx (+)= w dout, dwb[0..c-1] = dw, dwb[c] = dbias (scratch:
+ * gpw_nn_partials() * (c + 1) floats)                                       */
+int gpw_nn_head(int c, int64_t npts, const void *x, const float *w,
+                const float *bias, float *out, gpw_stream stream);
+int gpw_nn_head_backward(int c, int64_t npts, const void *x, const float *w,
+                         const float *dout, void *dx, int accumulate,
+                         float *dwb, float *scratch, int64_t scratch_floats,
+                         gpw_stream stream);
+/* number of CTA partials of gpw_nn_mse / gpw_nn_head_backward              */
+int gpw_nn_partials(void);
+/* out[c] = sum over the npts points of x[p][c] (a bias gradient); scratch:
+ * gpw_nn_partials() * c floats                                             */
+int gpw_nn_channel_sum(int c, int64_t npts, const void *x, float *out,
+                       float *scratch, int64_t scratch_floats,
+                       gpw_stream stream);
+/* x[B][N^3][16] bf16: channel 0 = rho[b] * scale[b] on the n^3 interior     */
+int gpw_nn_pack_input(const double *rho, const double *scale, int B, int n,
+                      int N, void *x, gpw_stream stream);
+/* fine (+)= nearest f-fold upsampling of coarse (fp32, N^3 / (N/f)^3) and
+ * its gradient (coarse = sum of the f^3 children)                           */
+int gpw_nn_upsample_add_f32(int f, const float *coarse, float *fine, int B,
+                            int N, gpw_stream stream);
+int gpw_nn_downsum_f32(int f, const float *fine, float *coarse, int B, int N,
+                       gpw_stream stream);
+/* mean squared error on the n^3 interior: diff = pred - target * tscale[b];
+ * dpred = d loss / d pred; partial[0..gpw_nn_partials()) sum to the loss    */
+int gpw_nn_mse(const float *pred, const double *target, const double *tscale,
+               int B, int n, int N, float *dpred, double *partial,
+               int64_t partial_len, gpw_stream stream);
+/* phi[b] (float64 n^3) = pred[b] * scale[b]                                 */
+int gpw_nn_unpack_output(const float *pred, const double *scale, int B, int n,
+                         int N, double *phi, gpw_stream stream);
+/* Adam step `step` (1-based) on fp32 params; param_bf16 (may be NULL)
+ * receives the updated values rounded to bf16                               */
+int gpw_nn_adam(int64_t n, float *param, const float *grad, float *m,
+                float *v, double lr, double b1, double b2, double eps,
+                int step, void *param_bf16, gpw_stream stream);
+/* Gaussian-sum densities on the device: rho[b][i0][i1][i2] = sum over k <
+ * counts[b] of q (2 pi s^2)^(-3/2) exp(-|r - c|^2 / 2 s^2) at r = (index +
+ * beg) h; params[b][k] = (cx, cy, cz, s, q), maxg entries per b.            */
+int gpw_nn_gaussians(int B, int n, double h, double beg, int maxg,
+                     const int *counts, const double *params, double *rho,
+                     gpw_stream stream);
+
 #ifdef __cplusplus
 }
 #endif
