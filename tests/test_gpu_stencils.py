@@ -227,3 +227,28 @@ def test_residual_and_norm(cuda):
     assert relerr(r.cpu().numpy(), ref) < 1e-12
     exp = (ref.reshape(2, -1) ** 2).sum(1)
     assert np.allclose(ss.cpu().numpy(), exp, rtol=1e-12)
+
+
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (1, 0, 1), (0, 1, 0), (0, 0, 0)])
+@pytest.mark.parametrize('dtype', [np.complex128, np.complex64])
+@pytest.mark.parametrize('nn', [1, 2, 3])
+def test_complex_tma_apply(cuda, pbc, dtype, nn):
+    """Complex Bloch-phase Laplace and gradients (radius 1-3) on mixed
+    zero / periodic boundaries, batched: wrapped halos on every axis with
+    their phases."""
+    from gpawdft_b200.fd_operators import Gradient, Laplace
+    N = (12, 16, 20)
+    gd, ogd = gds(N, (2.4, 3.1, 3.9), pbc)
+    a = rand((2,) + tuple(gd.n_c), dtype, 5 + nn)
+    ph = phases_for(ogd, dtype, seed=13)
+    for make, omake in ((lambda: Laplace(gd, -0.5, nn, dtype),
+                         lambda: ol.Laplace(ogd, -0.5, nn, complex)),
+                        (lambda: Gradient(gd, 1, 1.0, nn, dtype),
+                         lambda: ol.Gradient(ogd, 1, 1.0, nn, complex)),
+                        (lambda: Gradient(gd, 0, 1.0, nn, dtype),
+                         lambda: ol.Gradient(ogd, 0, 1.0, nn, complex))):
+        out = np.zeros_like(a)
+        make().apply(a, out, ph)
+        ref = np.zeros(a.shape, complex)
+        omake().apply(a.astype(complex), ref, ph)
+        assert relerr(out, ref) < TOL[np.dtype(dtype)]
