@@ -486,6 +486,117 @@ bool restrict_sweep_ok(const TrDesc& d, int dtype) {
   return d.k == 2 && !d.interpolate && (dtype == GPW_F64 || dtype == GPW_F32);
 }
 
+// TMA restriction (restrict_k2_tma_kernel): zero boundaries with pad 0 on
+// every axis, 16-byte aligned input with 16-byte strides.
+static bool k2r_tma_ok(const TransferArgs& a, size_t es, int nbatch) {
+  if (!tensor_map_encoder()) return false;
+  for (int c = 0; c < 3; ++c)
+    if (a.bc.periodic[c] || a.pad0[c] != 0) return false;
+  if (((uintptr_t)a.in & 15u) || (a.vin.s1 * es) % 16 || (a.vin.s0 * es) % 16 ||
+      (nbatch > 1 && (a.vin.sb * es) % 16))
+    return false;
+  return a.vout.n[2] >= 16;
+}
+
+template <typename S>
+static cudaError_t run_restrict_tma(TransferArgs a, int nbatch, cudaStream_t st) {
+  using C = RkCfg<S>;
+  static std::once_flag once;
+  static cudaError_t oe = cudaSuccess;
+  static int per_sm = 1;
+  std::call_once(once, [] {
+    oe = smem_optin(restrict_k2_tma_kernel<S>, C::smem);
+    if (oe == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, restrict_k2_tma_kernel<S>, RK_TX * RK_TY, C::smem) !=
+            cudaSuccess)
+      per_sm = 1;
+  });
+  if (oe != cudaSuccess) return oe;
+  auto enc = tensor_map_encoder();
+  CUtensorMap map;
+  const GridView& v = a.vin;
+  const size_t es = sizeof(S);
+  cuuint64_t dims[4] = {(cuuint64_t)v.n[2], (cuuint64_t)v.n[1], (cuuint64_t)v.n[0], (cuuint64_t)nbatch};
+  cuuint64_t strides[3] = {(cuuint64_t)(v.s1 * es), (cuuint64_t)(v.s0 * es),
+                           (cuuint64_t)(std::max<int64_t>(v.sb, v.s0 * v.n[0]) * es)};
+  cuuint32_t box[4] = {(cuuint32_t)RK_W, (cuuint32_t)RK_H, 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  if (enc(&map, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+          const_cast<void*>(a.in), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  dim3 grid((a.vout.n[2] + RK_TX - 1) / RK_TX, (a.vout.n[1] + RK_TY - 1) / RK_TY, 1);
+  const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
+  const int64_t want = (int64_t)std::max(1, per_sm) * num_sms();
+  int64_t nc = std::max<int64_t>(1, (want + tiles - 1) / tiles);
+  nc = std::min<int64_t>(nc, std::max(1, a.vout.n[0] / 2));
+  a.nchunk = (int)nc;
+  a.zchunk = (a.vout.n[0] + a.nchunk - 1) / a.nchunk;
+  grid.z = a.nchunk * nbatch;
+  restrict_k2_tma_kernel<S><<<grid, dim3(RK_TX, RK_TY), C::smem, st>>>(map, a, device_status_word());
+  return cudaGetLastError();
+}
+
+// TMA interpolation-subtraction (interpolate_k2_tma_kernel): zero
+// boundaries with pad 1 and skip 1 on every axis, 16-byte aligned coarse
+// input, base and output with 16-byte strides.
+static bool k2i_tma_ok(const TransferArgs& a, size_t es, int nbatch) {
+  if (!tensor_map_encoder() || !a.subtract || !a.base) return false;
+  for (int c = 0; c < 3; ++c)
+    if (a.bc.periodic[c] || a.pad0[c] != 1 || a.skip0[c] != 1) return false;
+  auto ok = [&](const void* p, const GridView& v) {
+    return !((uintptr_t)p & 15u) && (v.s1 * es) % 16 == 0 && (v.s0 * es) % 16 == 0 &&
+           (nbatch == 1 || (v.sb * es) % 16 == 0);
+  };
+  if (!ok(a.in, a.vin) || !ok(a.base, a.vbase) || !ok(a.out, a.vout)) return false;
+  for (int c = 0; c < 3; ++c)
+    if (a.vbase.n[c] != a.vout.n[c]) return false;
+  return a.vout.n[2] >= 32;
+}
+
+template <typename S>
+static cudaError_t run_interp_tma(TransferArgs a, int nbatch, cudaStream_t st) {
+  using C = IkCfg<S>;
+  static std::once_flag once;
+  static cudaError_t oe = cudaSuccess;
+  static int per_sm = 1;
+  std::call_once(once, [] {
+    oe = smem_optin(interpolate_k2_tma_kernel<S>, C::smem);
+    if (oe == cudaSuccess && cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                 &per_sm, interpolate_k2_tma_kernel<S>, IK_TX * IK_NTY, C::smem) != cudaSuccess)
+      per_sm = 1;
+  });
+  if (oe != cudaSuccess) return oe;
+  auto enc = tensor_map_encoder();
+  const size_t es = sizeof(S);
+  auto encode = [&](CUtensorMap* m, const void* base, const GridView& v, int bw, int bh) {
+    cuuint64_t dims[4] = {(cuuint64_t)v.n[2], (cuuint64_t)v.n[1], (cuuint64_t)v.n[0], (cuuint64_t)nbatch};
+    cuuint64_t strides[3] = {(cuuint64_t)(v.s1 * es), (cuuint64_t)(v.s0 * es),
+                             (cuuint64_t)(std::max<int64_t>(v.sb, v.s0 * v.n[0]) * es)};
+    cuuint32_t box[4] = {(cuuint32_t)bw, (cuuint32_t)bh, 1, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+               const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  CUtensorMap cmap, bmap;
+  if (!encode(&cmap, a.in, a.vin, IK_CW, IK_CH) || !encode(&bmap, a.base, a.vbase, IK_FW, IK_FH))
+    return cudaErrorInvalidValue;
+  dim3 grid((a.vout.n[2] + IK_FW - 1) / IK_FW, (a.vout.n[1] + IK_FH - 1) / IK_FH, 1);
+  const int nm = a.vout.n[0] / 2 + 1;
+  const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
+  const int64_t want = (int64_t)std::max(1, per_sm) * num_sms();
+  int64_t nc = std::max<int64_t>(1, (want + tiles - 1) / tiles);
+  nc = std::min<int64_t>(nc, std::max(1, nm / 2));
+  a.nchunk = (int)nc;
+  a.zchunk = (nm + a.nchunk - 1) / a.nchunk;
+  grid.z = a.nchunk * nbatch;
+  interpolate_k2_tma_kernel<S><<<grid, dim3(IK_TX, IK_NTY), C::smem, st>>>(cmap, bmap, a, device_status_word());
+  return cudaGetLastError();
+}
+
 // The vector restriction needs zero boundaries and pad 0 along axis 2 (fine
 // taps 2 I2 .. 2 I2 + 8 start 16-byte aligned) and aligned input rows.
 static bool k2r_vec_ok(const TransferArgs& a) {
@@ -525,6 +636,8 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
     a.w2 = sweep->w;
     a.c02 = sweep->c0;
   }
+  if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32) && !interp && k2r_tma_ok(a, elt_size(dtype), nbatch))
+    return dtype == GPW_F64 ? run_restrict_tma<double>(a, nbatch, st) : run_restrict_tma<float>(a, nbatch, st);
   if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32) && !interp && k2r_vec_ok(a)) {
     dim3 grid((vout.n[2] + 2 * K2V_TX - 1) / (2 * K2V_TX), (vout.n[1] + K2V_TY - 1) / K2V_TY, 1);
     // ~8 CTAs of 256 threads per SM; chunks of at least 4 output planes
@@ -542,6 +655,8 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
       restrict_k2_vec_kernel<float><<<grid, blk, 0, st>>>(a);
     return cudaGetLastError();
   }
+  if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32) && interp && k2i_tma_ok(a, elt_size(dtype), nbatch))
+    return dtype == GPW_F64 ? run_interp_tma<double>(a, nbatch, st) : run_interp_tma<float>(a, nbatch, st);
   if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32) && interp && k2_vec_ok(a)) {
     dim3 grid((vout.n[2] + 4 * K2V_TX - 1) / (4 * K2V_TX), (vout.n[1] + K2V_TY - 1) / K2V_TY, 1);
     // ~8 CTAs of 256 threads per SM; chunks of at least 8 output planes

@@ -18,6 +18,7 @@
 #include <climits>
 
 #include "gpw_common.cuh"
+#include "gpw_star_tma.cuh"
 #include "gpw_transfer.cuh"
 
 namespace gpw {
@@ -391,6 +392,223 @@ __global__ void __launch_bounds__(K2V_TX* K2V_TY) restrict_k2_vec_kernel(const T
     st2(out + (int64_t)I0 * a.vout.s0, v0, v1v, nvalid);
     if (out2) st2(out2 + (int64_t)I0 * a.vout.s0, wc * v0, wc * v1v, nvalid);
   }
+}
+
+// ------------------------------------------------------------------ TMA restriction
+// K = 2 restriction of zero-boundary real grids (fine centre 2I + 1) fed by
+// TMA: a CTA owns a 32 (axis 2) x 8 (axis 1) tile of coarse points and a
+// chunk of coarse planes; each fine plane of the tile's footprint (68 x 17
+// points from (2 X0, 2 Y0), the last columns / rows past the grid
+// zero-filled) arrives as one tensor-map box on its own mbarrier, RK_D coarse
+// planes ahead.  Each thread evaluates its coarse point from the three
+// staged fine planes with the expressions of restrict_k2_kernel
+// (bit-identical) and writes it, and the level's first Jacobi sweep from
+// zero if requested.  Every wait is bounded.
+constexpr int RK_TX = 32, RK_TY = 8;          // coarse tile
+constexpr int RK_W = 2 * RK_TX + 4;           // fine box width (16-byte multiple for f32 / f64)
+constexpr int RK_H = 2 * RK_TY + 1;           // fine box height
+constexpr int RK_D = 2;                        // coarse planes of prefetch
+constexpr int RK_NS = 3 + 2 * RK_D;            // fine-plane stages
+
+template <typename S>
+struct RkCfg {
+  static constexpr int STAGE = (RK_W * RK_H * (int)sizeof(S) + 127) / 128 * 128;
+  static constexpr size_t smem = (size_t)RK_NS * STAGE + RK_NS * 8 + 128;
+};
+
+template <typename S>
+__global__ void __launch_bounds__(RK_TX* RK_TY) restrict_k2_tma_kernel(const __grid_constant__ CUtensorMap map,
+                                                                       const TransferArgs a, int* status) {
+  using C = RkCfg<S>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* ring = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + RK_NS * C::STAGE);
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int nc0 = a.vout.n[0];
+  const int C0 = (int)((int64_t)chunk * nc0 / a.nchunk), C1 = (int)((int64_t)(chunk + 1) * nc0 / a.nchunk);
+  const int X0 = blockIdx.x * RK_TX, Y0 = blockIdx.y * RK_TY;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + RK_TX * ty;
+  const int I2 = X0 + tx, I1 = Y0 + ty;
+  const bool inside = I1 < a.vout.n[1] && I2 < a.vout.n[2];
+  bool timed_out = false;
+  if (tid == 0) {
+    for (int i = 0; i < RK_NS; ++i) mbar_init(mbar_u32(&bars[i]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (C0 >= C1) return;
+  // fine planes 2 C0 .. 2 C1 (step i = fine plane 2 C0 + i)
+  const int nsteps = 2 * (C1 - C0) + 1;
+  auto issue = [&](int i) {
+    const unsigned bar = mbar_u32(&bars[i % RK_NS]);
+    mbar_expect_tx(bar, (unsigned)(RK_W * RK_H * sizeof(S)));
+    tma_load_4d(smem_u32(ring + (i % RK_NS) * C::STAGE), &map, 2 * X0, 2 * Y0, 2 * C0 + i, b, bar);
+  };
+  if (tid == 0)
+    for (int i = 0; i < 3 + 2 * RK_D && i < nsteps; ++i) issue(i);
+  S* __restrict__ out = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)I1 * a.vout.s1 + I2;
+  S* __restrict__ out2 =
+      a.out2 ? static_cast<S*>(a.out2) + (int64_t)b * a.vout.sb + (int64_t)I1 * a.vout.s1 + I2 : nullptr;
+  const S wc = (S)a.w2 / (S)a.c02;
+  for (int c = 0; c < C1 - C0; ++c) {
+    // coarse plane C0 + c: fine steps 2c, 2c + 1, 2c + 2
+    for (int d = (c == 0 ? 0 : 1); d <= 2; ++d) {
+      const int i = 2 * c + d;
+      if (!mbar_wait_bounded(mbar_u32(&bars[i % RK_NS]), (unsigned)((i / RK_NS) & 1))) timed_out = true;
+    }
+    if (inside) {
+      S y[3];
+#pragma unroll
+      for (int d0 = 0; d0 < 3; ++d0) {
+        const S* pl = reinterpret_cast<const S*>(ring + ((2 * c + d0) % RK_NS) * C::STAGE);
+        S z[3];
+#pragma unroll
+        for (int d1 = 0; d1 < 3; ++d1) {
+          const S* row = pl + (2 * ty + d1) * RK_W + 2 * tx;
+          z[d1] = r2(row[0], row[1], row[2]);
+        }
+        y[d0] = r2(z[0], z[1], z[2]);
+      }
+      const S v = r2(y[0], y[1], y[2]);
+      out[(int64_t)(C0 + c) * a.vout.s0] = v;
+      if (out2) out2[(int64_t)(C0 + c) * a.vout.s0] = wc * v;
+    }
+    __syncthreads();  // fine steps 2c, 2c + 1 are consumed (their slots are refilled next)
+    if (tid == 0) {
+      const int n1 = 2 * c + 3 + 2 * RK_D;  // next steps to issue: two per coarse plane
+      if (n1 < nsteps) issue(n1);
+      if (n1 + 1 < nsteps) issue(n1 + 1);
+    }
+  }
+  if (timed_out && status) atomicExch(status, GPW_ETIMEDOUT);
+}
+
+// ------------------------------------------------------------------ TMA interpolation
+// K = 2 interpolation with subtraction, out = base - I(e), on zero-boundary
+// real grids (pad 1, skip 1 per axis: fine o takes coarse u = (o+1)/2 - 1,
+// midpoint with u + 1 when o is even) fed by TMA.  A CTA owns a 64 (axis 2)
+// x 16 (axis 1) fine tile and a chunk of coarse planes m; per m one
+// mbarrier covers the coarse plane m (a 40 x 10 box from the 16-byte aligned
+// column 32 bx - 4 and row 8 by - 1) and the base planes 2m and 2m + 1
+// (64 x 16 boxes).  Fine planes 2m, 2m + 1 need coarse planes m - 1 and m.
+// Each thread owns 2 adjacent axis-2 points x 2 rows and evaluates them with
+// the expressions of interpolate_k2_kernel (bit-identical).  Bounded waits.
+constexpr int IK_TX = 32, IK_NTY = 8;              // threads
+constexpr int IK_FW = 64, IK_FH = 16;              // fine tile
+constexpr int IK_CW = 40, IK_CH = 10;              // coarse box
+constexpr int IK_D = 2;                             // coarse planes of prefetch
+constexpr int IK_NS = IK_D + 2;                     // stages (plane m - 1 stays resident)
+
+template <typename S>
+struct IkCfg {
+  static constexpr int CB = (IK_CW * IK_CH * (int)sizeof(S) + 127) / 128 * 128;
+  static constexpr int FB = (IK_FW * IK_FH * (int)sizeof(S) + 127) / 128 * 128;
+  static constexpr int STAGE = CB + 2 * FB;
+  static constexpr size_t smem = (size_t)IK_NS * STAGE + IK_NS * 8 + 128;
+};
+
+template <typename S>
+__global__ void __launch_bounds__(IK_TX* IK_NTY) interpolate_k2_tma_kernel(const __grid_constant__ CUtensorMap cmap,
+                                                                           const __grid_constant__ CUtensorMap bmap,
+                                                                           const TransferArgs a, int* status) {
+  using C = IkCfg<S>;
+  using V = typename Vec2<S>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* ring = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + IK_NS * C::STAGE);
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int nf0 = a.vout.n[0];
+  const int nm = nf0 / 2 + 1;  // coarse planes m whose fine planes 2m, 2m+1 start inside the grid
+  const int M0 = (int)((int64_t)chunk * nm / a.nchunk), M1 = (int)((int64_t)(chunk + 1) * nm / a.nchunk);
+  const int x0 = blockIdx.x * IK_FW, y0 = blockIdx.y * IK_FH;
+  const int cx0 = x0 / 2 - 4, cy0 = y0 / 2 - 1;  // coarse box origin
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + IK_TX * ty;
+  bool timed_out = false;
+  if (tid == 0) {
+    for (int i = 0; i < IK_NS; ++i) mbar_init(mbar_u32(&bars[i]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (M0 >= M1) return;
+  // steps: coarse planes M0 - 1 .. M1 - 1 (step i = plane M0 - 1 + i); the
+  // first carries no base planes
+  const int nsteps = M1 - M0 + 1;
+  auto issue = [&](int i) {
+    unsigned char* st = ring + (i % IK_NS) * C::STAGE;
+    const unsigned bar = mbar_u32(&bars[i % IK_NS]);
+    const int m = M0 - 1 + i;
+    const bool base = i > 0;
+    mbar_expect_tx(bar, (unsigned)(IK_CW * IK_CH * sizeof(S) + (base ? 2 * IK_FW * IK_FH * sizeof(S) : 0)));
+    tma_load_4d(smem_u32(st), &cmap, cx0, cy0, m, b, bar);
+    if (base) {
+      tma_load_4d(smem_u32(st + C::CB), &bmap, x0, y0, 2 * m, b, bar);
+      tma_load_4d(smem_u32(st + C::CB + C::FB), &bmap, x0, y0, 2 * m + 1, b, bar);
+    }
+  };
+  if (tid == 0)
+    for (int i = 0; i <= IK_D && i < nsteps; ++i) issue(i);
+  // this thread's fine points: x = x0 + 2 tx + {0, 1}, y = y0 + 2 ty + {0, 1}
+  const int lx = 2 * tx, ly = 2 * ty;
+  const bool xin0 = x0 + lx < a.vout.n[2], xin1 = x0 + lx + 1 < a.vout.n[2];
+  // per axis: o + 1 = 2 u' + e with u' the padded coarse index, i.e. coarse
+  // u = u' - 1; local coarse column u - cx0 = u' + 3 - x0/2
+  int cu2[2], ce2[2], cu1[2], ce1[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int t2 = x0 + lx + k + 1, t1 = y0 + ly + k + 1;
+    cu2[k] = (t2 >> 1) - 1 - cx0;
+    ce2[k] = t2 & 1;
+    cu1[k] = (t1 >> 1) - 1 - cy0;
+    ce1[k] = t1 & 1;
+  }
+  // Y(u0)[j][k]: the axis-2 and axis-1 passes on coarse plane stage `cp`
+  auto Y = [&](const S* cp, int j, int k) -> S {
+    const S* r0 = cp + cu1[j] * IK_CW;
+    S z0 = r0[cu2[k]];
+    if (ce2[k]) z0 = i2h(z0, r0[cu2[k] + 1]);
+    if (!ce1[j]) return z0;
+    const S* r1 = r0 + IK_CW;
+    S z1 = r1[cu2[k]];
+    if (ce2[k]) z1 = i2h(z1, r1[cu2[k] + 1]);
+    return i2h(z0, z1);
+  };
+  for (int i = 0; i < nsteps; ++i) {
+    if (!mbar_wait_bounded(mbar_u32(&bars[i % IK_NS]), (unsigned)((i / IK_NS) & 1))) timed_out = true;
+    if (i > 0) {
+      const int m = M0 - 1 + i;
+      const S* cm1 = reinterpret_cast<const S*>(ring + ((i - 1) % IK_NS) * C::STAGE);  // plane m - 1
+      const S* cm = reinterpret_cast<const S*>(ring + (i % IK_NS) * C::STAGE);         // plane m
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {  // fine plane 2m + f: even -> midpoint of m-1, m; odd -> m
+        const int o = 2 * m + f;
+        if (o >= nf0) break;
+        const S* base = reinterpret_cast<const S*>(ring + (i % IK_NS) * C::STAGE + C::CB + f * C::FB);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int y = y0 + ly + j;
+          if (y >= a.vout.n[1] || !xin0) continue;
+          S v[2];
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            const S ya = Y(f == 0 ? cm1 : cm, j, k);
+            v[k] = (f == 0) ? i2h(ya, Y(cm, j, k)) : ya;
+          }
+          const V bv = *reinterpret_cast<const V*>(base + (ly + j) * IK_FW + lx);
+          S* op = static_cast<S*>(a.out) + (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 +
+                  x0 + lx;
+          if (xin1)
+            *reinterpret_cast<V*>(op) = V{bv.x - v[0], bv.y - v[1]};
+          else
+            op[0] = bv.x - v[0];
+        }
+      }
+    }
+    __syncthreads();  // plane step i - 1 is consumed
+    if (tid == 0 && i + IK_D + 1 < nsteps) issue(i + IK_D + 1);
+  }
+  if (timed_out && status) atomicExch(status, GPW_ETIMEDOUT);
 }
 
 }  // namespace gpw
