@@ -87,6 +87,37 @@ __global__ void converge_update_kernel(int nbatch, const double* __restrict__ su
 
 __global__ void stamp_kernel(int64_t* t) { *t = global_ns(); }
 
+// Per-solve state at the start of a solve; eps is read from the engine's
+// mapped pinned mailbox, so no copy engine is involved.
+__global__ void solve_setup_kernel(int nb, const double* __restrict__ h_eps, int maxiter, double* __restrict__ eps,
+                                   int* __restrict__ niter, unsigned char* __restrict__ active, int* maxiter_out) {
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    eps[b] = h_eps[b];
+    niter[b] = 1;
+    active[b] = 1;
+  }
+  if (threadIdx.x == 0) *maxiter_out = maxiter;
+}
+
+// Per-solve results into the mapped pinned mailbox.
+__global__ void solve_readback_kernel(int nb, const int* __restrict__ niter, const double* __restrict__ err,
+                                      int* __restrict__ h_niter, double* __restrict__ h_err) {
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    h_niter[b] = niter[b];
+    h_err[b] = err[b];
+  }
+}
+
+// rows of `len` doubles between two row pitches (elements); one warp a row
+__global__ void pitch_copy_kernel(int64_t rows, int len, const double* __restrict__ src, int64_t src_pitch,
+                                  double* __restrict__ dst, int64_t dst_pitch) {
+  const int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= rows) return;
+  const double* s = src + r * src_pitch;
+  double* d = dst + r * dst_pitch;
+  for (int c = threadIdx.x & 31; c < len; c += 32) d[c] = s[c];
+}
+
 template <typename T>
 __global__ void copy_kernel(int64_t n, const T* __restrict__ x, T* __restrict__ y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -126,6 +157,14 @@ struct gpw_poisson {
   Workspace d_err, d_eps, d_niter, d_active, d_any, d_r64, d_gs_old, d_maxiter, d_tdone, d_t0;
   SumScratch sums;
   int* h_any = nullptr;  // pinned
+  // mapped pinned mailbox: eps in, niter / error out (nbmax each)
+  void* h_io = nullptr;
+  double* h_eps = nullptr;
+  double* h_err = nullptr;
+  int* h_niter = nullptr;
+  double* m_eps = nullptr;  // the same three, as device pointers
+  double* m_err = nullptr;
+  int* m_niter = nullptr;
   struct GraphKey {
     int64_t nb;
     int prec;
@@ -143,6 +182,7 @@ struct gpw_poisson {
     for (auto& kv : loops)
       if (kv.second) cudaGraphExecDestroy(kv.second);
     if (h_any) cudaFreeHost(h_any);
+    if (h_io) cudaFreeHost(h_io);
   }
 };
 
@@ -470,6 +510,17 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
   if (!device_status_word()) return fail(GPW_ENOMEM, "status word allocation");
   cudaError_t e = cudaMallocHost(&ps->h_any, sizeof(int));
   if (e != cudaSuccess) return cuda_fail(e, "pinned alloc");
+  e = cudaHostAlloc(&ps->h_io, (size_t)nbatch_max * 20 + 64, cudaHostAllocMapped | cudaHostAllocPortable);
+  if (e != cudaSuccess) return cuda_fail(e, "pinned mailbox");
+  ps->h_eps = (double*)ps->h_io;
+  ps->h_err = ps->h_eps + nbatch_max;
+  ps->h_niter = (int*)(ps->h_err + nbatch_max);
+  void* dio = nullptr;
+  e = cudaHostGetDevicePointer(&dio, ps->h_io, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "pinned mailbox mapping");
+  ps->m_eps = (double*)dio;
+  ps->m_err = ps->m_eps + nbatch_max;
+  ps->m_niter = (int*)(ps->m_err + nbatch_max);
   *out = ps.release();
   return GPW_OK;
 }
@@ -760,26 +811,33 @@ static cudaGraphExec_t loop_graph(gpw_poisson* ps, int nb, int prec) {
   return ge;
 }
 
+// Copies between a caller's C-contiguous (nb, n0, n1, n2) array and the
+// engine's row-pitched level-0 layout, as a kernel (no copy engine: the
+// caller's own host<->device transfers of other batches may be in flight).
+static cudaError_t pitch_copy(const GridView& v, int nb, const double* src, int64_t src_pitch, double* dst,
+                              int64_t dst_pitch, cudaStream_t st) {
+  const int64_t rows = (int64_t)v.n[0] * v.n[1] * nb;
+  const int thr = 256;
+  const int64_t blocks = (rows + thr / 32 - 1) / (thr / 32);
+  pitch_copy_kernel<<<(unsigned)blocks, thr, 0, st>>>(rows, (int)v.n[2], src, src_pitch, dst, dst_pitch);
+  return cudaGetLastError();
+}
+
 // Solve-state set-up and inputs: eps, niter = 1, active = 1, phi / rho
 // copied into the engine layout, and (float32 form) the initial defect.
+// Everything is a kernel on `st`; eps travels through the mapped mailbox,
+// which the previous solve on this engine has finished with (solves end in
+// a stream synchronisation).
 static int solve_prologue(gpw_poisson* ps, double* phi, const double* rho, int nb, const double* eps, int maxiter,
                           int precision, cudaStream_t st) {
   Level& L0 = ps->lv[0];
-  std::vector<int> ones(nb, 1);
-  std::vector<unsigned char> act(nb, 1);
-  cudaError_t e;
-  if ((e = cudaMemcpyAsync(ps->d_eps.ptr, eps, nb * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(ps->d_niter.ptr, ones.data(), nb * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(ps->d_active.ptr, act.data(), nb, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(ps->d_maxiter.ptr, &maxiter, sizeof(int), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpy2DAsync(L0.phi[0].ptr, L0.v.s1 * 8, phi, (size_t)L0.v.n[2] * 8, (size_t)L0.v.n[2] * 8,
-                             (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpy2DAsync(L0.rho.ptr, L0.v.s1 * 8, rho, (size_t)L0.v.n[2] * 8, (size_t)L0.v.n[2] * 8,
-                             (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
-    return cuda_fail(e, "poisson setup copies");
-  // the host copies above stage from pageable memory: wait for them before
-  // the vectors go out of scope
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "poisson setup copies");
+  std::memcpy(ps->h_eps, eps, (size_t)nb * 8);
+  solve_setup_kernel<<<1, 128, 0, st>>>(nb, ps->m_eps, maxiter, (double*)ps->d_eps.ptr, (int*)ps->d_niter.ptr,
+                                        (unsigned char*)ps->d_active.ptr, (int*)ps->d_maxiter.ptr);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = pitch_copy(L0.v, nb, phi, L0.v.n[2], (double*)L0.phi[0].ptr, L0.v.s1, st);
+  if (e == cudaSuccess) e = pitch_copy(L0.v, nb, rho, L0.v.n[2], (double*)L0.rho.ptr, L0.v.s1, st);
+  if (e != cudaSuccess) return cuda_fail(e, "poisson setup");
   if (precision == 1 && fused_dc(ps)) {
     // initial defect: float32 rhs and first level-0 sweep, fused
     e = launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr, nb,
@@ -797,16 +855,21 @@ static int solve_prologue(gpw_poisson* ps, double* phi, const double* rho, int n
   return GPW_OK;
 }
 
+// Result copy and per-solve statistics (kernels on `st`), then the one
+// stream synchronisation of a solve.
 static int solve_epilogue(gpw_poisson* ps, double* phi, int nb, int maxiter, int* niter, double* error,
                           cudaStream_t st) {
   Level& L0 = ps->lv[0];
-  cudaError_t e;
-  if ((e = cudaMemcpy2DAsync(phi, (size_t)L0.v.n[2] * 8, L0.phi[0].ptr, L0.v.s1 * 8, (size_t)L0.v.n[2] * 8,
-                             (size_t)L0.v.n[0] * L0.v.n[1] * nb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(niter, ps->d_niter.ptr, nb * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(error, ps->d_err.ptr, nb * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-      (e = cudaStreamSynchronize(st)) != cudaSuccess)
-    return cuda_fail(e, "poisson result copies");
+  cudaError_t e = pitch_copy(L0.v, nb, (const double*)L0.phi[0].ptr, L0.v.s1, phi, L0.v.n[2], st);
+  if (e == cudaSuccess) {
+    solve_readback_kernel<<<1, 128, 0, st>>>(nb, (const int*)ps->d_niter.ptr, (const double*)ps->d_err.ptr,
+                                             ps->m_niter, ps->m_err);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "poisson result copies");
+  std::memcpy(niter, ps->h_niter, (size_t)nb * 4);
+  std::memcpy(error, ps->h_err, (size_t)nb * 8);
   for (int b = 0; b < nb; ++b)
     if (niter[b] >= maxiter) return fail(GPW_ECONV, "Poisson solver did not converge in maxiter iterations");
   return GPW_OK;
@@ -943,7 +1006,8 @@ extern "C" int gpw_poisson_solve_many(int nengines, gpw_poisson* const* engines,
   // one clock origin for every engine's latencies: just before the launch
   stamp_kernel<<<1, 1, 0, st>>>((int64_t*)engines[0]->d_t0.ptr);
   for (int i = 1; i < nengines; ++i) {
-    cudaError_t e = cudaMemcpyAsync(engines[i]->d_t0.ptr, engines[0]->d_t0.ptr, 8, cudaMemcpyDeviceToDevice, st);
+    copy_kernel<int64_t><<<1, 32, 0, st>>>(1, (const int64_t*)engines[0]->d_t0.ptr, (int64_t*)engines[i]->d_t0.ptr);
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "clock origin");
   }
   cudaError_t e = cudaGraphLaunch(ge, st);

@@ -445,6 +445,96 @@ class FDPoissonSolver:
             arrays.writeback(phi_b, phi_d)
         return niter
 
+    def solve_stream(self, rhos, phis=None, eps=None, out=None):
+        """Independent neutral solves of a sequence of host batches, each
+        (nb, *n_c) float64, with the host<->device transfers overlapped with
+        the solves: while batch k is solved, batch k+1's densities travel to
+        the device and batch k-1's potentials back (two device slots, one
+        copy stream per direction).
+
+        Host tensors should be pinned (``torch.Tensor.pin_memory()``);
+        pageable arrays are accepted but their copies do not overlap.
+        ``phis``: initial guesses (None: zero, nothing transferred).
+        ``out``: host tensors receiving the potentials (None: allocated
+        pinned).  Each solve stops at its own ``error <= eps`` exactly as in
+        ``solve_batch``.  Returns (out, per-batch iteration counts).
+        """
+        import torch
+        arrays.require_cuda()
+        if self._engine is None:
+            self.initialize()
+        n = len(rhos)
+        if n == 0:
+            return [], []
+        if eps is None:
+            eps = self.eps
+        shape = tuple(rhos[0].shape)
+        nb = int(shape[0])
+        dev = torch.device('cuda', torch.cuda.current_device())
+
+        def host(a):
+            return a if isinstance(a, torch.Tensor) else torch.from_numpy(
+                np.ascontiguousarray(a, float))
+
+        rhos = [host(r) for r in rhos]
+        if any(tuple(r.shape) != shape or r.dtype != torch.float64
+               for r in rhos):
+            raise ValueError('solve_stream: batches must share one float64 '
+                             'shape')
+        if phis is not None:
+            phis = [host(p) for p in phis]
+        if out is None:
+            out = [torch.empty(shape, dtype=torch.float64).pin_memory()
+                   for _ in range(n)]
+        compute = torch.cuda.current_stream()
+        up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        rho_d = [torch.empty(shape, dtype=torch.float64, device=dev)
+                 for _ in range(2)]
+        phi_d = [torch.empty_like(rho_d[0]) for _ in range(2)]
+        rho_free = [None, None]   # the slot's last solve has read its rho
+        phi_free = [None, None]   # the slot's last result has left
+        arrived = [None] * n
+
+        def upload(k):
+            s = k % 2
+            with torch.cuda.stream(up):
+                if rho_free[s] is not None:
+                    up.wait_event(rho_free[s])
+                if phi_free[s] is not None:
+                    up.wait_event(phi_free[s])
+                rho_d[s].copy_(rhos[k], non_blocking=True)
+                if phis is not None:
+                    phi_d[s].copy_(phis[k], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(up)
+            arrived[k] = ev
+
+        niters = []
+        upload(0)
+        if n > 1:
+            upload(1)
+        for k in range(n):
+            s = k % 2
+            compute.wait_event(arrived[k])
+            if phis is None:
+                if phi_free[s] is not None:
+                    compute.wait_event(phi_free[s])
+                phi_d[s].zero_()
+            niters.append(self.solve_batch(phi_d[s], rho_d[s], eps=eps))
+            done = torch.cuda.Event()
+            done.record(compute)
+            rho_free[s] = done
+            with torch.cuda.stream(down):
+                down.wait_event(done)
+                out[k].copy_(phi_d[s], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(down)
+            phi_free[s] = ev
+            if k + 2 < n:
+                upload(k + 2)
+        down.synchronize()   # every copy and solve has finished
+        return out, niters
+
     def estimate_memory(self, mem=None):
         gdbytes = int(np.prod(self.gd.n_c)) * 8
         nbytes = 0

@@ -196,6 +196,47 @@ def test_fp32_batch_equals_single(cuda):
         assert np.array_equal(phi, phib[s])
 
 
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_solve_stream_equals_batch(cuda, precision):
+    """Host batches solved with overlapped transfers (two device slots, copy
+    streams): every batch's potentials and iteration counts equal those of
+    solve_batch, for pinned and pageable inputs and given initial guesses."""
+    import torch
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    N, nb, nbatches = 32, 2, 5
+    rhos = []
+    for k in range(nbatches):
+        batch = []
+        for s in range(nb):
+            rho, L = gaussian_density(N, 0.2, 3 + 2 * s + k, 60 + 7 * k + s)
+            batch.append(rho)
+        rhos.append(np.array(batch))
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    ps = PoissonSolver(nn=3, batch=nb, precision=precision, maxiter=200)
+    ps.set_grid_descriptor(gd)
+    ps.initialize()
+    eps = 1e-20 * max(float(np.dot(r.ravel(), r.ravel())) for r in rhos[0])
+    want, want_n = [], []
+    for k in range(nbatches):
+        phi = np.zeros_like(rhos[k])
+        want_n.append(ps.solve_batch(phi, rhos[k], eps=eps))
+        want.append(phi)
+    pinned = [torch.from_numpy(r).pin_memory() for r in rhos]
+    for inputs in (pinned, rhos):
+        out, niters = ps.solve_stream(inputs, eps=eps)
+        for k in range(nbatches):
+            assert np.array_equal(niters[k], want_n[k])
+            assert np.array_equal(out[k].numpy(), want[k])
+    # initial guesses travel too: restarting from the answers converges at
+    # once and keeps them within the tolerance
+    out, niters = ps.solve_stream(pinned, phis=want, eps=eps)
+    for k in range(nbatches):
+        assert (np.asarray(niters[k]) <= 2).all()
+        assert np.abs(out[k].numpy() - want[k]).max() < 1e-6 * np.abs(
+            want[k]).max()
+
+
 def test_full_size_127_trajectory(cuda):
     """127^3 (the benchmark grid): the engine's vector transfers, TMA
     stencil variants and one-CTA coarse levels reproduce the reference's
