@@ -1,0 +1,308 @@
+// Launch of the periodic / Bloch TMA star-stencil kernel (gpw_bloch_tma.cuh):
+// eligibility, tensor maps, axis-0 chunking and a per-shape choice between
+// 4- and 8-warp tiles, timed on the first launch of a shape outside stream
+// capture (an apply recomputes its output from an input it does not write,
+// so the timed repetitions leave the same result).
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "gpw_bloch_tma.cuh"
+#include "gpw_internal.h"
+#include "gpw_tma_launch.cuh"
+
+namespace gpw {
+
+namespace {
+
+// A tile layout: VEC points per lane, WPR warps spanning a row, NW warps
+// per CTA (TY = NW / WPR * PY rows), and the axis-0 chunking; vec == 0
+// stands for the cp.async kernel of gpw_stencil.cuh.
+struct BlochChoice {
+  int vec, wpr, nw;
+  int nchunk;  // 0: wave model, < 0: model x -nchunk
+};
+
+// Tuned per element type, radius, axes carrying coefficients (a Laplacian
+// and a gradient of one radius cost differently), grid and batch.
+struct BlochKey {
+  int dtype, R, axes, n0, n1, n2, nbatch;
+  bool operator<(const BlochKey& o) const {
+    const int a[7] = {dtype, R, axes, n0, n1, n2, nbatch};
+    const int b[7] = {o.dtype, o.R, o.axes, o.n0, o.n1, o.n2, o.nbatch};
+    for (int i = 0; i < 7; ++i)
+      if (a[i] != b[i]) return a[i] < b[i];
+    return false;
+  }
+};
+
+int coef_axes(const StarCoefs& sc, int R) {
+  int m = 0;
+  for (int i = 0; i <= 2 * R; ++i) {
+    if (sc.cx[i] != 0.0) m |= 1;
+    if (sc.cy[i] != 0.0) m |= 2;
+    if (sc.cz[i] != 0.0) m |= 4;
+  }
+  return m;
+}
+std::mutex g_bloch_mu;
+std::map<BlochKey, BlochChoice> g_bloch_tune;
+std::atomic<int> g_bloch_force{0};  // test hook: pinned candidate layout (1-based; 0: tuned)
+std::atomic<long long> g_bloch_launches{0};  // kernel launches so far (tests read it)
+
+constexpr int BLOCH_D = 2;  // planes in flight ahead of the one being read
+
+inline int bloch_py(size_t es) { return es >= 16 ? 1 : 2; }
+
+bool encode_rows_map(CUtensorMap* map, size_t es, bool cpx, const void* base, const GridView& v, int nbatch,
+                     int rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const size_t ses = cpx ? es / 2 : es;  // scalar size
+  const int inner = v.n[2] * (cpx ? 2 : 1);
+  cuuint64_t dims[4] = {(cuuint64_t)inner, (cuuint64_t)v.n[1], (cuuint64_t)v.n[0], (cuuint64_t)nbatch};
+  cuuint64_t strides[3] = {(cuuint64_t)(v.s1 * es), (cuuint64_t)(v.s0 * es),
+                           (cuuint64_t)(std::max<int64_t>(v.sb, v.s0 * v.n[0]) * es)};
+  cuuint32_t box[4] = {(cuuint32_t)inner, (cuuint32_t)rows, 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(map, ses == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// The layout fits the grid: whole tiles along axis 1, every staged box
+// (R halo rows, TY rows) starting 128-byte aligned in shared memory, and the
+// ring within the opt-in shared memory of a CTA.
+bool bloch_shape_ok(size_t es, int R, const BlochChoice& c, const GridView& v) {
+  const int ty = c.nw / c.wpr * bloch_py(es);
+  const int64_t rowbytes = (int64_t)v.n[2] * (int64_t)es;
+  if (c.wpr * 32 * c.vec < v.n[2]) return false;
+  if (v.n[1] % ty || ty < R) return false;
+  if ((rowbytes * R) % 128 || (rowbytes * ty) % 128) return false;
+  const int64_t smem = (int64_t)(BLOCH_D + 3) * (ty + 2 * R) * rowbytes + 2 * (BLOCH_D + 3) * 8 + 128;
+  return smem <= 200 * 1024;
+}
+
+// Candidate layouts of a shape: a warp per row (VEC = n2 / 32 rounded up;
+// 4 or 8 warps), and for complex rows wider than a warp, one point a lane
+// with WPR warps per row (tiles of 4 or 8 rows).
+std::vector<BlochChoice> bloch_candidates(int dtype, int R, const GridView& v) {
+  const size_t es = elt_size(dtype);
+  std::vector<BlochChoice> out;
+  const int vec = (v.n[2] + 31) / 32;
+  for (int nw : {4, 8}) {
+    BlochChoice c{vec, 1, nw, 0};
+    if (bloch_shape_ok(es, R, c, v)) out.push_back(c);
+  }
+  if (is_complex(dtype) && vec > 1) {
+    for (int ty : {4, 8}) {
+      BlochChoice c{1, vec, vec * ty / bloch_py(es), 0};
+      if (bloch_shape_ok(es, R, c, v)) out.push_back(c);
+    }
+  }
+  return out;
+}
+
+template <typename T, int R, int VEC, int NW, int WPR>
+cudaError_t bloch_run(const void* in, const GridView& vin, void* out, const GridView& vout, int nbatch,
+                      const Boundary& bc, const StarCoefs& sc, int nchunk, cudaStream_t st) {
+  using C = BlochCfg<T, R, VEC, NW, BLOCH_D, WPR>;
+  using S = typename EltTraits<T>::S;
+  constexpr bool cpx = EltTraits<T>::cpx;
+  const int rowbytes = vout.n[2] * (int)sizeof(T);
+  const int stage = C::ROWS * rowbytes;
+  const size_t smem = (size_t)C::NS * stage + 2 * C::NS * 8 + 128;
+  auto kern = bloch_star_kernel<T, R, VEC, NW, BLOCH_D, WPR>;
+  cudaError_t e = smem_optin_bytes(kern, smem);
+  if (e != cudaSuccess) return e;
+  CUtensorMap tmain, thalo;
+  if (!encode_rows_map(&tmain, sizeof(T), cpx, in, vin, nbatch, C::TY) ||
+      !encode_rows_map(&thalo, sizeof(T), cpx, in, vin, nbatch, R))
+    return cudaErrorInvalidValue;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NT, smem)) != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int tiles_y = vout.n[1] / C::TY;
+  const int64_t tiles = (int64_t)tiles_y * nbatch;
+  int nc = nchunk > 0 ? nchunk
+                      : tma_model_chunks(vout.n[0], tiles, R, (int64_t)per_sm * num_sms()) * std::max(1, -nchunk);
+  nc = std::max(1, std::min(nc, tma_max_chunks(vout.n[0], R)));
+  BlochArgs a;
+  a.out = out;
+  a.vout = vout;
+  a.bc = bc;
+  a.nchunk = nc;
+  a.rowbytes = rowbytes;
+  a.stage_bytes = stage;
+  a.status = device_status_word();
+  BlochCoefs<S> k{};
+  bool has_y = false, has_z = false;
+  for (int i = 0; i <= 2 * R; ++i) {
+    k.cx[i] = (S)sc.cx[i];
+    k.cy[i] = (S)sc.cy[i];
+    k.cz[i] = (S)sc.cz[i];
+    has_y |= sc.cy[i] != 0.0;
+    has_z |= sc.cz[i] != 0.0;
+  }
+  k.cc = (S)sc.cc;
+  k.has_y = has_y;
+  k.has_z = has_z;
+  dim3 grid(1, tiles_y, nc * nbatch);
+  kern<<<grid, C::NT, smem, st>>>(tmain, thalo, a, k);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) g_bloch_launches.fetch_add(1);
+  return e;
+}
+
+template <typename T, int R>
+cudaError_t bloch_run_layout(const BlochChoice& c, const void* in, const GridView& vin, void* out,
+                             const GridView& vout, int nbatch, const Boundary& bc, const StarCoefs& sc,
+                             cudaStream_t st) {
+#define GPW_BLOCH_CASE(V, N, W)                                                                 \
+  if (c.vec == V && c.nw == N && c.wpr == W)                                                    \
+    return bloch_run<T, R, V, N, W>(in, vin, out, vout, nbatch, bc, sc, c.nchunk, st);
+  // a warp per row
+  GPW_BLOCH_CASE(1, 4, 1) GPW_BLOCH_CASE(1, 8, 1)
+  GPW_BLOCH_CASE(2, 4, 1) GPW_BLOCH_CASE(2, 8, 1)
+  GPW_BLOCH_CASE(3, 4, 1) GPW_BLOCH_CASE(3, 8, 1)
+  GPW_BLOCH_CASE(4, 4, 1) GPW_BLOCH_CASE(4, 8, 1)
+  if constexpr (EltTraits<T>::cpx) {
+    // one point a lane, WPR warps per row, 4- or 8-row tiles
+    constexpr int P = sizeof(T) >= 16 ? 1 : 2;
+    GPW_BLOCH_CASE(1, 2 * 4 / P, 2) GPW_BLOCH_CASE(1, 2 * 8 / P, 2)
+    GPW_BLOCH_CASE(1, 3 * 4 / P, 3) GPW_BLOCH_CASE(1, 3 * 8 / P, 3)
+    GPW_BLOCH_CASE(1, 4 * 4 / P, 4) GPW_BLOCH_CASE(1, 4 * 8 / P, 4)
+  }
+#undef GPW_BLOCH_CASE
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
+cudaError_t bloch_dispatch(int R, const BlochChoice& ch, const void* in, const GridView& vin, void* out,
+                           const GridView& vout, int nbatch, const Boundary& bc, const StarCoefs& sc,
+                           cudaStream_t st) {
+  switch (R) {
+    case 1: return bloch_run_layout<T, 1>(ch, in, vin, out, vout, nbatch, bc, sc, st);
+    case 2: return bloch_run_layout<T, 2>(ch, in, vin, out, vout, nbatch, bc, sc, st);
+    case 3: return bloch_run_layout<T, 3>(ch, in, vin, out, vout, nbatch, bc, sc, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t bloch_launch(int dtype, int R, const BlochChoice& ch, const void* in, const GridView& vin, void* out,
+                         const GridView& vout, int nbatch, const Boundary& bc, const StarCoefs& sc,
+                         cudaStream_t st) {
+  switch (dtype) {
+    case GPW_F64: return bloch_dispatch<double>(R, ch, in, vin, out, vout, nbatch, bc, sc, st);
+    case GPW_F32: return bloch_dispatch<float>(R, ch, in, vin, out, vout, nbatch, bc, sc, st);
+    case GPW_C128: return bloch_dispatch<double2>(R, ch, in, vin, out, vout, nbatch, bc, sc, st);
+    case GPW_C64: return bloch_dispatch<float2>(R, ch, in, vin, out, vout, nbatch, bc, sc, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+bool bloch_path_ok(const OpDesc& d, int dtype, const void* in, const GridView& vin, const void* out,
+                   const GridView& vout, int nbatch) {
+  if (!valid_dtype(dtype) || !d.star || d.R < 1 || d.R > 3) return false;
+  if (in == out || !out || !tensor_map_encoder()) return false;
+  for (int c = 0; c < 3; ++c)
+    if (vin.n[c] != vout.n[c]) return false;
+  const size_t es = elt_size(dtype);
+  if (vout.n[2] > 128 || vout.n[2] < 1) return false;  // one warp a row, <= 4 points a lane
+  if (((size_t)vout.n[2] * es) % 16) return false;      // TMA box rows of whole 16-byte units
+  if ((reinterpret_cast<uintptr_t>(in) & 15u) || (reinterpret_cast<uintptr_t>(out) & 15u)) return false;
+  if ((vin.s1 * (int64_t)es) % 16 || (vin.s0 * (int64_t)es) % 16) return false;
+  if (nbatch > 1 && (vin.sb * (int64_t)es) % 16) return false;
+  return !bloch_candidates(dtype, d.R, vout).empty();
+}
+
+cudaError_t launch_bloch(const OpDesc& d, int dtype, const StencilArgs& sa, int nbatch, cudaStream_t st) {
+  const void* in = sa.in;
+  void* out = sa.out;
+  const GridView &vin = sa.vin, &vout = sa.vout;
+  const Boundary& bc = sa.bc;
+  const std::vector<BlochChoice> cands = bloch_candidates(dtype, d.R, vout);
+  if (cands.empty()) return cudaErrorInvalidValue;
+  auto run = [&](const BlochChoice& c) {
+    return c.vec == 0 ? launch_apply_cpasync(d, dtype, sa, nbatch, st)
+                      : bloch_launch(dtype, d.R, c, in, vin, out, vout, nbatch, bc, d.sc, st);
+  };
+  // pinned layout (test hook): the shape's forced-th candidate, if it has one
+  const int forced = g_bloch_force.load();
+  if (forced > 0 && forced <= (int)cands.size()) return run(cands[forced - 1]);
+  const BlochKey key{dtype, d.R, coef_axes(d.sc, d.R), vout.n[0], vout.n[1], vout.n[2], nbatch};
+  BlochChoice ch = cands[0];
+  bool tuned;
+  {
+    std::lock_guard<std::mutex> lock(g_bloch_mu);
+    auto it = g_bloch_tune.find(key);
+    tuned = it != g_bloch_tune.end();
+    if (tuned) ch = it->second;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (!tuned && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+      float best = 1e30f;
+      std::vector<BlochChoice> trial;
+      for (const BlochChoice& base : cands)
+        for (int nc : {0, -2}) {
+          BlochChoice c = base;
+          c.nchunk = nc;
+          trial.push_back(c);
+        }
+      trial.push_back(BlochChoice{0, 0, 0, 0});  // the cp.async kernel
+      for (const BlochChoice& c : trial) {
+        {
+          cudaError_t e = run(c);  // warm-up
+          if (e != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+          }
+          cudaEventRecord(e0, st);
+          for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = run(c);
+          cudaEventRecord(e1, st);
+          if (cudaEventSynchronize(e1) != cudaSuccess || e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return e != cudaSuccess ? e : cudaGetLastError();
+          }
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (ms < best) {
+            best = ms;
+            ch = c;
+          }
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      std::lock_guard<std::mutex> lock(g_bloch_mu);
+      g_bloch_tune[key] = ch;
+    }
+  }
+  return run(ch);
+}
+
+}  // namespace gpw
+
+// Pins the tile layout of the periodic / Bloch stencil kernel: the k-th
+// candidate layout of each shape (k >= 1; shapes with fewer candidates keep
+// the tuned one), 0 = the tuned choice.  Process-wide; for tests and tuning
+// studies.
+extern "C" int gpw_set_bloch_layout(int k) {
+  if (k < 0 || k > 16) return gpw::fail(GPW_EINVAL, "bloch layout index must be 0-16");
+  gpw::g_bloch_force.store(k);
+  return GPW_OK;
+}
+
+// Launches of the periodic / Bloch stencil kernel so far in this process.
+extern "C" int64_t gpw_bloch_launch_count(void) { return (int64_t)gpw::g_bloch_launches.load(); }

@@ -200,6 +200,15 @@ struct SumScratch {
 
 int num_sms();
 
+// Periodic / Bloch (or mixed-boundary) star applies on the TMA row kernel
+// (gpw_bloch.cu): eligibility and launch.
+bool bloch_path_ok(const OpDesc& d, int dtype, const void* in, const GridView& vin, const void* out,
+                   const GridView& vout, int nbatch);
+struct StencilArgs;
+cudaError_t launch_bloch(const OpDesc& d, int dtype, const StencilArgs& a, int nbatch, cudaStream_t st);
+// The cp.async star / general kernel for an apply.
+cudaError_t launch_apply_cpasync(const OpDesc& d, int dtype, const StencilArgs& a, int nbatch, cudaStream_t st);
+
 // Device status word written by kernels whose bounded waits expire
 // (GPW_ETIMEDOUT); allocated on first use, which must not happen inside a
 // stream capture (handle constructors call it).

@@ -1,6 +1,7 @@
 // Kernel launchers: dtype / radius / tap-count dispatch, launch geometry and
 // shared-memory opt-in for every device kernel of the library.
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 
@@ -111,6 +112,23 @@ static cudaError_t dispatch_mode(const StencilArgs& a, const OpDesc& d, int nbat
 
 static bool star_radius_ok(int R) { return R >= 1 && R <= 4; }
 
+// The cp.async star / general kernel for an apply (the periodic TMA row
+// kernel's tuner times it beside its own layouts).
+cudaError_t launch_apply_cpasync(const OpDesc& d, int dtype, const StencilArgs& a, int nbatch, cudaStream_t st) {
+  OpDesc dd = d;
+  if (!star_radius_ok(dd.R)) {
+    dd.star = false;
+    dd.star_jacobi = false;
+  }
+  switch (dtype) {
+    case GPW_F64: return dispatch_mode<double, MODE_APPLY>(a, dd, nbatch, st);
+    case GPW_C128: return dispatch_mode<double2, MODE_APPLY>(a, dd, nbatch, st);
+    case GPW_F32: return dispatch_mode<float, MODE_APPLY>(a, dd, nbatch, st);
+    case GPW_C64: return dispatch_mode<float2, MODE_APPLY>(a, dd, nbatch, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
 int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& v, int nbatch) {
   const bool use_star = ((mode == MODE_JACOBI) ? d.star_jacobi : d.star) && star_radius_ok(d.R);
   int tz, ty, minz;
@@ -188,7 +206,21 @@ std::mutex g_tune_mu;
 std::map<TuneKey, TmaChoice> g_tune;
 }  // namespace
 
+// Pinned choice (variant >= 0): every TMA stencil launch whose dtype and
+// radius have that variant uses it with this chunking, instead of the
+// tuned one (set through gpw_set_tma_variant).
+static std::atomic<int> g_force_var{-1};
+static std::atomic<int> g_force_nc{0};
+
+static bool tma_variant_available(int dtype, int R, int var) {
+  if (var < 0 || var >= TMA_NVARIANT) return false;
+  if (var >= 5 && dtype != GPW_F32) return false;  // 4-point variants: float32 only
+  return (R == 1 || R == 3) || var == (R == 4 ? 1 : 2);
+}
+
 static TmaChoice tma_choice(int dtype, int R, int mode, const GridView& v, int nbatch) {
+  const int fv = g_force_var.load();
+  if (fv >= 0 && tma_variant_available(dtype, R, fv)) return TmaChoice{fv, g_force_nc.load()};
   std::lock_guard<std::mutex> lock(g_tune_mu);
   auto it = g_tune.find(TuneKey{dtype, R, mode, v.n[0], v.n[1], v.n[2], nbatch});
   if (it != g_tune.end()) return it->second;
@@ -204,6 +236,13 @@ static cudaError_t tma_launch(int dtype, int mode, int R, const TmaChoice& ch, c
                               const StarCoefs& sc, cudaStream_t st) {
   if (dtype == GPW_F64) return tma_stencil_f64(mode, R, ch.var, a, nbatch, sc, ch.nchunk, st);
   return tma_stencil_f32(mode, R, ch.var, a, nbatch, sc, ch.nchunk, st);
+}
+
+extern "C" int gpw_set_tma_variant(int variant, int nchunk) {
+  if (variant < -1 || variant >= TMA_NVARIANT) return fail(GPW_EINVAL, "tma variant out of range");
+  g_force_nc.store(nchunk);
+  g_force_var.store(variant);
+  return GPW_OK;
 }
 
 int tuned_stencil_count() {
@@ -248,7 +287,7 @@ cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in,
     // first launch of an untuned shape outside stream capture: tune it now
     // (apply / residual / Jacobi recompute their output from inputs they do
     // not overwrite, so the timed repetitions leave the same result)
-    if (!active && out != rho && !tma_tuned(dtype, d.R, mode, vout, nbatch)) {
+    if (!active && out != rho && g_force_var.load() < 0 && !tma_tuned(dtype, d.R, mode, vout, nbatch)) {
       cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
       if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
         cudaError_t te = tune_stencil(d, dtype, mode, in, vin, out, vout, rho, vrho, nullptr, nbatch, w, gs, st);
@@ -258,6 +297,8 @@ cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in,
     const TmaChoice ch = tma_choice(dtype, d.R, mode, vout, nbatch);
     return tma_launch(dtype, mode, d.R, ch, a, nbatch, d.sc, st);
   }
+  if (mode == MODE_APPLY && !active && bloch_path_ok(d, dtype, in, vin, out, vout, nbatch))
+    return launch_bloch(d, dtype, a, nbatch, st);
   OpDesc dd = d;
   if (!star_radius_ok(dd.R)) {
     dd.star = false;

@@ -25,27 +25,77 @@
 namespace gpw {
 
 // Tile-shape variants (the launcher's autotuner times them per grid, dtype,
-// radius and epilogue and keeps the fastest): NTY thread rows of 32 threads,
-// PY axis-1 rows per thread, D planes of TMA prefetch beyond the current one,
-// MINB CTAs per SM the register allocation must allow.
-template <int NTY_, int PY_, int D_, int MINB_>
+// radius and epilogue and keeps the fastest): NTX threads along axis 2 with
+// VEC adjacent points each, NTY thread rows, PY axis-1 rows per thread, D
+// planes of TMA prefetch beyond the current one, MINB CTAs per SM the
+// register allocation must allow.
+template <int NTX_, int VEC_, int NTY_, int PY_, int D_, int MINB_>
 struct TmaShape {
-  static constexpr int NTY = NTY_, PY = PY_, D = D_, MINB = MINB_;
+  static constexpr int NTX = NTX_, VEC = VEC_, NTY = NTY_, PY = PY_, D = D_, MINB = MINB_;
 };
 template <int V> struct TmaVariant;
-template <> struct TmaVariant<0> { using T = TmaShape<8, 2, 1, 2>; };  // 64 x 16 tile, 1 plane ahead
-template <> struct TmaVariant<1> { using T = TmaShape<4, 2, 2, 1>; };  // 64 x 8 tile, 2 planes ahead
-template <> struct TmaVariant<2> { using T = TmaShape<8, 2, 2, 2>; };  // 64 x 16 tile, 2 planes ahead
-template <> struct TmaVariant<3> { using T = TmaShape<4, 4, 2, 2>; };  // 64 x 16 tile, 4 rows per thread
-template <> struct TmaVariant<4> { using T = TmaShape<8, 2, 3, 2>; };  // 64 x 16 tile, 3 planes ahead
+template <> struct TmaVariant<0> { using T = TmaShape<32, 2, 8, 2, 1, 2>; };  // 64 x 16 tile, 1 plane ahead
+template <> struct TmaVariant<1> { using T = TmaShape<32, 2, 4, 2, 2, 1>; };  // 64 x 8 tile, 2 planes ahead
+template <> struct TmaVariant<2> { using T = TmaShape<32, 2, 8, 2, 2, 2>; };  // 64 x 16 tile, 2 planes ahead
+template <> struct TmaVariant<3> { using T = TmaShape<32, 2, 4, 4, 2, 2>; };  // 64 x 16 tile, 4 rows per thread
+template <> struct TmaVariant<4> { using T = TmaShape<32, 2, 8, 2, 3, 2>; };  // 64 x 16 tile, 3 planes ahead
+// float32 only: 4 points per thread (16-byte shared-memory reads)
+template <> struct TmaVariant<5> { using T = TmaShape<16, 4, 8, 2, 2, 3>; };  // 64 x 16 tile, 128 threads
+template <> struct TmaVariant<6> { using T = TmaShape<16, 4, 8, 1, 2, 4>; };  // 64 x 8 tile, 128 threads
+
+// VEC elements of S moved as one vector load / store
+template <typename S, int N> struct VecT;
+template <> struct VecT<float, 2> { using T = float2; };
+template <> struct VecT<float, 4> { using T = float4; };
+template <> struct VecT<double, 2> { using T = double2; };
+template <typename S, int N>
+struct Pack {
+  S v[N];
+};
+template <typename S, int N>
+__device__ __forceinline__ Pack<S, N> ldv(const S* p) {
+  const typename VecT<S, N>::T t = *reinterpret_cast<const typename VecT<S, N>::T*>(p);
+  Pack<S, N> r;
+  if constexpr (N == 2) {
+    r.v[0] = t.x;
+    r.v[1] = t.y;
+  } else {
+    r.v[0] = t.x;
+    r.v[1] = t.y;
+    r.v[2] = t.z;
+    r.v[3] = t.w;
+  }
+  return r;
+}
+template <typename S, int N>
+__device__ __forceinline__ void stv(S* p, const Pack<S, N>& r) {
+  typename VecT<S, N>::T t;
+  if constexpr (N == 2) {
+    t.x = r.v[0];
+    t.y = r.v[1];
+  } else {
+    t.x = r.v[0];
+    t.y = r.v[1];
+    t.z = r.v[2];
+    t.w = r.v[3];
+  }
+  *reinterpret_cast<typename VecT<S, N>::T*>(p) = t;
+}
+// the first `n` of N elements (n < N): scalar stores
+template <typename S, int N>
+__device__ __forceinline__ void stv_part(S* p, const Pack<S, N>& r, int n) {
+#pragma unroll
+  for (int e = 0; e < N; ++e)
+    if (e < n) p[e] = r.v[e];
+}
 
 constexpr int tma_align128(int b) { return (b + 127) / 128 * 128; }
 
 template <typename S, int R, int MODE, int V = 0>
 struct TmaCfg {
   using Sh = typename TmaVariant<V>::T;
-  static constexpr int VEC = 2;                        // points per thread along axis 2
-  static constexpr int NTX = 32;                       // threads along axis 2
+  static constexpr int VEC = Sh::VEC;                  // points per thread along axis 2
+  static constexpr int NTX = Sh::NTX;                  // threads along axis 2
   static constexpr int TZ = NTX * VEC;                 // tile width (points)
   static constexpr int PY = Sh::PY;                    // axis-1 rows per thread
   static constexpr int NTY = Sh::NTY;                  // threads along axis 1
@@ -71,6 +121,33 @@ struct TmaCfg {
   static constexpr int NR = 2 * R + 1;
   static constexpr size_t smem = (size_t)NS * STAGE_BYTES + (size_t)NS * 8 + 128;
 };
+
+// Coefficients and relaxation weights in the kernel's element type, rounded
+// once on the host with the same roundings a per-use conversion would make
+// (the kernel reads them as constant-bank operands).
+template <typename S>
+struct TmaCoefs {
+  S cx[9], cy[9], cz[9];  // per-axis coefficients indexed offset + R (R <= 4)
+  S cc;                   // total centre coefficient
+  S w1, wc;               // Jacobi: 1 - w and w / c0
+  float wc2;              // RESID_DC: the float32 first sweep's w2 / c0
+};
+
+template <typename S>
+inline TmaCoefs<S> tma_coefs(const StarCoefs& sc, int R, double w, double c0, double w2) {
+  TmaCoefs<S> t{};
+  for (int i = 0; i <= 2 * R && i < 9; ++i) {
+    t.cx[i] = (S)sc.cx[i];
+    t.cy[i] = (S)sc.cy[i];
+    t.cz[i] = (S)sc.cz[i];
+  }
+  t.cc = (S)sc.cc;
+  const S ws = (S)w;
+  t.w1 = S(1) - ws;
+  t.wc = c0 != 0.0 ? ws / (S)c0 : S(0);
+  t.wc2 = c0 != 0.0 ? (float)w2 / (float)c0 : 0.0f;
+  return t;
+}
 
 struct TmaArgs {
   StencilArgs s;          // views, rho, w, c0, active, gsum, chunking
@@ -109,17 +186,14 @@ __device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map
       : "memory");
 }
 
-template <typename S> struct Vec2;
-template <> struct Vec2<double> { using T = double2; };
-template <> struct Vec2<float> { using T = float2; };
-
 template <typename S, int R, int MODE, int VAR>
 __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE, VAR>::MINB)
     star_tma_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap tmap_rho,
-                    const __grid_constant__ CUtensorMap tmap_aux, const TmaArgs ta, const StarCoefs k) {
+                    const __grid_constant__ CUtensorMap tmap_aux, const TmaArgs ta, const TmaCoefs<S> k) {
   using C = TmaCfg<S, R, MODE, VAR>;
-  using V = typename Vec2<S>::T;
-  constexpr int W = C::W, NS = C::NS, NR = C::NR, PY = C::PY, D = C::D;
+  constexpr int W = C::W, NS = C::NS, NR = C::NR, PY = C::PY, D = C::D, VEC = C::VEC, XL = C::XL;
+  using P = Pack<S, VEC>;
+  static_assert(XL % VEC == 0, "halo loads are whole vectors");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // 128-byte aligned ring of stages (TMA destinations), then the mbarriers;
   // the launch reserves 128 bytes for the alignment shift
@@ -137,10 +211,10 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
   const int z1 = (int)((int64_t)(chunk + 1) * n0 / a.nchunk);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + C::NTX * ty;
-  const int xl = C::XL + C::VEC * tx;     // local column of this thread's first point
-  const int x = x0 + C::VEC * tx;         // global axis-2 index of the first point
-  const int yb = ty * PY;                 // first local output row
-  const bool xin0 = x < a.vout.n[2], xin1 = x + 1 < a.vout.n[2];
+  const int xl = XL + VEC * tx;       // local column of this thread's first point
+  const int x = x0 + VEC * tx;        // global axis-2 index of the first point
+  const int yb = ty * PY;             // first local output row
+  const int nx = min(VEC, a.vout.n[2] - x);  // this thread's points inside the grid (<= 0: none)
   double sumsq = 0.0;
   bool timed_out = false;
 
@@ -162,7 +236,7 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
       const bool with_out = C::HAS_RHO && o >= z0;
       const unsigned bytes = C::IN_BYTES + (with_out ? C::RHO_BYTES + C::AUX_BYTES : 0);
       mbar_expect_tx(bar, bytes);
-      tma_load_4d(smem_u32(st), &tmap, x0 - C::XL, y0 - R, pfirst + i, b, bar);
+      tma_load_4d(smem_u32(st), &tmap, x0 - XL, y0 - R, pfirst + i, b, bar);
       if (with_out) {
         tma_load_4d(smem_u32(st + C::RHO_OFF), &tmap_rho, x0, y0, o, b, bar);
         if constexpr (C::HAS_AUX) tma_load_4d(smem_u32(st + C::AUX_OFF), &tmap_aux, x0, y0, o, b, bar);
@@ -170,11 +244,13 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
     };
     if (tid == 0)
       for (int i = 0; i <= D && i < nsteps; ++i) issue(i);
-    V acc[PY][NR];
+    P acc[PY][NR];
 #pragma unroll
     for (int j = 0; j < PY; ++j)
 #pragma unroll
-      for (int m = 0; m < NR; ++m) acc[j][m] = V{S(0), S(0)};
+      for (int m = 0; m < NR; ++m)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) acc[j][m].v[e] = S(0);
 
     for (int sb = 0; sb < nsteps; sb += NR) {
 #pragma unroll
@@ -187,51 +263,52 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
         const int o = pfirst + s - R;  // output plane completed by this step
         if (!mbar_wait_bounded(mbar_u32(&bars[slot]), (unsigned)((s / NS) & 1))) timed_out = true;
 
-        // column of PY + 2R rows (2 points each) at this thread's columns
-        V col[PY + 2 * R];
+        // column of PY + 2R rows (VEC points each) at this thread's columns
+        P col[PY + 2 * R];
 #pragma unroll
-        for (int i = 0; i < PY + 2 * R; ++i) col[i] = *reinterpret_cast<const V*>(sl + (yb + i) * W + xl);
+        for (int i = 0; i < PY + 2 * R; ++i) col[i] = ldv<S, VEC>(sl + (yb + i) * W + xl);
 #pragma unroll
         for (int j = 0; j < PY; ++j) {
           const S* row = sl + (yb + j + R) * W + xl;
-          // axis-2 neighbours of the two points: row[-XL .. 1 + XL]
-          S nb[2 * C::XL + 2];
+          // axis-2 neighbours of the VEC points: row[-XL .. VEC - 1 + XL]
+          S nb[2 * XL + VEC];
 #pragma unroll
-          for (int q = 0; q < C::XL; q += 2) {
-            const V lo = *reinterpret_cast<const V*>(row - C::XL + q);
-            const V hi = *reinterpret_cast<const V*>(row + 2 + q);
-            nb[q] = lo.x;
-            nb[q + 1] = lo.y;
-            nb[C::XL + 2 + q] = hi.x;
-            nb[C::XL + 2 + q + 1] = hi.y;
+          for (int q = 0; q < XL; q += VEC) {
+            const P lo = ldv<S, VEC>(row - XL + q);
+            const P hi = ldv<S, VEC>(row + VEC + q);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+              nb[q + e] = lo.v[e];
+              nb[XL + VEC + q + e] = hi.v[e];
+            }
           }
-          const V c = col[j + R];
-          nb[C::XL] = c.x;
-          nb[C::XL + 1] = c.y;
+          const P c = col[j + R];
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) nb[XL + e] = c.v[e];
           constexpr bool sweep = (MODE == MODE_JACOBI || MODE == MODE_JACOBI_ADD64);
-          S p0 = sweep ? S(0) : (S)k.cc * c.x;
-          S p1 = sweep ? S(0) : (S)k.cc * c.y;
+          S p[VEC];
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) p[e] = sweep ? S(0) : k.cc * c.v[e];
 #pragma unroll
           for (int q = 1; q <= R; ++q) {
-            p0 = fma((S)k.cy[R + q], col[j + R + q].x, p0);
-            p1 = fma((S)k.cy[R + q], col[j + R + q].y, p1);
-            p0 = fma((S)k.cy[R - q], col[j + R - q].x, p0);
-            p1 = fma((S)k.cy[R - q], col[j + R - q].y, p1);
-            p0 = fma((S)k.cz[R + q], nb[C::XL + q], p0);
-            p1 = fma((S)k.cz[R + q], nb[C::XL + 1 + q], p1);
-            p0 = fma((S)k.cz[R - q], nb[C::XL - q], p0);
-            p1 = fma((S)k.cz[R - q], nb[C::XL + 1 - q], p1);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+              p[e] = fma(k.cy[R + q], col[j + R + q].v[e], p[e]);
+              p[e] = fma(k.cy[R - q], col[j + R - q].v[e], p[e]);
+              p[e] = fma(k.cz[R + q], nb[XL + e + q], p[e]);
+              p[e] = fma(k.cz[R - q], nb[XL + e - q], p[e]);
+            }
           }
           // scatter along axis 0 (logical slot m receives offset R - m)
 #pragma unroll
           for (int m = 0; m < NR; ++m) {
             const int pm = (m + ph) % NR;
-            if (m == R) {
-              acc[j][pm].x += p0;
-              acc[j][pm].y += p1;
-            } else {
-              acc[j][pm].x = fma((S)k.cx[2 * R - m], c.x, acc[j][pm].x);
-              acc[j][pm].y = fma((S)k.cx[2 * R - m], c.y, acc[j][pm].y);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+              if (m == R)
+                acc[j][pm].v[e] += p[e];
+              else
+                acc[j][pm].v[e] = fma(k.cx[2 * R - m], c.v[e], acc[j][pm].v[e]);
             }
           }
         }
@@ -243,61 +320,78 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
 #pragma unroll
           for (int j = 0; j < PY; ++j) {
             const int y = y0 + yb + j;
-            if (y < a.vout.n[1] && xin0) {
-              V av = acc[j][ph];
-              V res;
-              V rho = V{S(0), S(0)};
-              if constexpr (C::HAS_RHO) rho = *reinterpret_cast<const V*>(rsl + (yb + j) * C::TZ + C::VEC * tx);
+            if (y < a.vout.n[1] && nx > 0) {
+              const P av = acc[j][ph];
+              P res;
+              P rho{};
+              if constexpr (C::HAS_RHO) rho = ldv<S, VEC>(rsl + (yb + j) * C::TZ + VEC * tx);
               const int64_t oidx =
                   (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
               if constexpr (MODE == MODE_APPLY) {
                 res = av;
               } else if constexpr (MODE == MODE_RESIDUAL || MODE == MODE_RESID_DC) {
-                res.x = av.x - rho.x;
-                res.y = av.y - rho.y;
-                sumsq += (double)res.x * res.x + (xin1 ? (double)res.y * res.y : 0.0);
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) res.v[e] = av.v[e] - rho.v[e];
+                if (a.gsum.partial) {
+                  if constexpr (VEC == 2) {
+                    sumsq += (double)res.v[0] * res.v[0] + (nx > 1 ? (double)res.v[1] * res.v[1] : 0.0);
+                  } else {
+                    double t = (double)res.v[0] * res.v[0];
+#pragma unroll
+                    for (int e = 1; e < VEC; ++e) t += e < nx ? (double)res.v[e] * res.v[e] : 0.0;
+                    sumsq += t;
+                  }
+                }
               } else {
-                const V cur = *reinterpret_cast<const V*>(osl + (yb + j + R) * W + xl);
-                const S w = (S)a.w, wc = w / (S)a.c0;
-                res.x = (S(1) - w) * cur.x + wc * (rho.x - av.x);
-                res.y = (S(1) - w) * cur.y + wc * (rho.y - av.y);
+                const P cur = ldv<S, VEC>(osl + (yb + j + R) * W + xl);
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) res.v[e] = k.w1 * cur.v[e] + k.wc * (rho.v[e] - av.v[e]);
               }
               if constexpr (MODE == MODE_RESID_DC) {
                 // float32 defect and first inner Jacobi iterate from zero
-                const float2 rhs = make_float2((float)(-res.x), (float)(-res.y));
-                const float wc = (float)a.w2 / (float)a.c0;
-                const float2 e1 = make_float2(wc * rhs.x, wc * rhs.y);
+                Pack<float, VEC> rhs, e1;
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) {
+                  rhs.v[e] = (float)(-res.v[e]);
+                  e1.v[e] = k.wc2 * rhs.v[e];
+                }
                 float* rp = static_cast<float*>(a.out) + oidx;
                 float* ep = static_cast<float*>(a.out2) + oidx;
-                if (xin1) {
-                  *reinterpret_cast<float2*>(rp) = rhs;
-                  *reinterpret_cast<float2*>(ep) = e1;
+                if (nx == VEC) {
+                  stv<float, VEC>(rp, rhs);
+                  stv<float, VEC>(ep, e1);
                 } else {
-                  rp[0] = rhs.x;
-                  ep[0] = e1.x;
+                  stv_part<float, VEC>(rp, rhs, nx);
+                  stv_part<float, VEC>(ep, e1, nx);
                 }
               } else if constexpr (MODE == MODE_JACOBI_ADD64) {
                 // phi64 += e (the inner correction), e never stored
                 double* pp = static_cast<double*>(a.out2) + oidx;
-                double2 pv = *reinterpret_cast<const double2*>(asl + (yb + j) * C::TZ + C::VEC * tx);
-                pv.x += (double)res.x;
-                pv.y += (double)res.y;
-                if (xin1)
-                  *reinterpret_cast<double2*>(pp) = pv;
-                else
-                  pp[0] = pv.x;
+                const double* ap = asl + (yb + j) * C::TZ + VEC * tx;
+#pragma unroll
+                for (int h = 0; h < VEC; h += 2) {
+                  Pack<double, 2> pv = ldv<double, 2>(ap + h);
+                  pv.v[0] += (double)res.v[h];
+                  pv.v[1] += (double)res.v[h + 1];
+                  if (h + 2 <= nx)
+                    stv<double, 2>(pp + h, pv);
+                  else
+                    stv_part<double, 2>(pp + h, pv, nx - h);
+                }
               } else if (MODE != MODE_RESIDUAL || a.out) {
                 S* op = static_cast<S*>(a.out) + oidx;
-                if (xin1)
-                  *reinterpret_cast<V*>(op) = res;
+                if (nx == VEC)
+                  stv<S, VEC>(op, res);
                 else
-                  op[0] = res.x;
+                  stv_part<S, VEC>(op, res, nx);
               }
             }
           }
         }
 #pragma unroll
-        for (int j = 0; j < PY; ++j) acc[j][ph] = V{S(0), S(0)};
+        for (int j = 0; j < PY; ++j)
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) acc[j][ph].v[e] = S(0);
         __syncthreads();  // every thread is done with plane s - R (its slot is refilled next)
         if (tid == 0 && s + D + 1 < nsteps) issue(s + D + 1);
       }

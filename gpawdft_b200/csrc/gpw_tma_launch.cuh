@@ -17,9 +17,12 @@ namespace gpw {
 // Every variant is compiled for radius 1 (coarse multigrid levels) and 3
 // (the nn=3 Laplacian of level 0); radius 2 uses variant 2 only and radius 4
 // variant 1 (128 threads: its float64 accumulators do not fit the register
-// share of two 256-thread CTAs per SM).
+// share of two 256-thread CTAs per SM).  The 4-point variants (5, 6) are
+// float32 only.
 __host__ __device__ constexpr int tma_default_variant(int R) { return R == 4 ? 1 : 2; }
+template <typename S>
 __host__ __device__ constexpr bool tma_variant_compiled(int R, int v) {
+  if (v >= 5 && sizeof(S) != 4) return false;
   return (R == 1 || R == 3) ? (v >= 0 && v < TMA_NVARIANT) : v == tma_default_variant(R);
 }
 
@@ -104,7 +107,8 @@ struct TmaKernel {
     grid.z = nc * nbatch;
     a.nblk_seg = grid.x * grid.y * nc;
     TmaArgs ta{a, device_status_word()};
-    star_tma_kernel<S, R, MODE, VAR><<<grid, dim3(C::NTX, C::NTY), C::smem, st>>>(map_in, map_rho, map_aux, ta, sc);
+    const TmaCoefs<S> kc = tma_coefs<S>(sc, R, a.w, a.c0, a.w2);
+    star_tma_kernel<S, R, MODE, VAR><<<grid, dim3(C::NTX, C::NTY), C::smem, st>>>(map_in, map_rho, map_aux, ta, kc);
     return cudaGetLastError();
   }
 };
@@ -112,7 +116,7 @@ struct TmaKernel {
 template <typename S, int R, int MODE>
 cudaError_t tma_run_variant(int var, const StencilArgs& a, int nbatch, const StarCoefs& sc, int nchunk,
                             cudaStream_t st) {
-  if (!tma_variant_compiled(R, var)) return cudaErrorInvalidValue;
+  if (!tma_variant_compiled<S>(R, var)) return cudaErrorInvalidValue;
   if constexpr (R == 1 || R == 3) {
     switch (var) {
       case 0: return TmaKernel<S, R, MODE, 0>::run(a, nbatch, sc, nchunk, st);
@@ -120,6 +124,12 @@ cudaError_t tma_run_variant(int var, const StencilArgs& a, int nbatch, const Sta
       case 2: return TmaKernel<S, R, MODE, 2>::run(a, nbatch, sc, nchunk, st);
       case 3: return TmaKernel<S, R, MODE, 3>::run(a, nbatch, sc, nchunk, st);
       case 4: return TmaKernel<S, R, MODE, 4>::run(a, nbatch, sc, nchunk, st);
+    }
+    if constexpr (sizeof(S) == 4) {
+      switch (var) {
+        case 5: return TmaKernel<S, R, MODE, 5>::run(a, nbatch, sc, nchunk, st);
+        case 6: return TmaKernel<S, R, MODE, 6>::run(a, nbatch, sc, nchunk, st);
+      }
     }
     return cudaErrorInvalidValue;
   } else {

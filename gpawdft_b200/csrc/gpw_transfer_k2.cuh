@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(IK_TX* IK_NTY) interpolate_k2_tma_kernel(const
                                                                            const __grid_constant__ CUtensorMap bmap,
                                                                            const TransferArgs a, int* status) {
   using C = IkCfg<S>;
-  using V = typename Vec2<S>::T;
+  using V = typename VecT<S, 2>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* ring = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + IK_NS * C::STAGE);

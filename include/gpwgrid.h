@@ -237,6 +237,28 @@ int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
                             int reps, double *ms_per_launch,
                             double *bytes_per_launch, gpw_stream stream);
 
+/* Pins the tile variant of the TMA star-stencil kernels (no counterpart in
+ * the reference): with variant >= 0 every later TMA stencil launch whose
+ * element type and radius have that variant uses it, with `nchunk` axis-0
+ * chunks (0 = the wave model, < 0 = the model's count times -nchunk);
+ * variant -1 returns to the autotuned choice.  Variants 0-4 exist for both
+ * element types, 5-6 (4 points per thread) for float32 only.  Process-wide;
+ * meant for tests and tuning studies.  GPW_EINVAL outside [-1, 6].        */
+int gpw_set_tma_variant(int variant, int nchunk);
+
+/* Pins the tile layout of the star-stencil kernel that serves applies on
+ * grids with a periodic axis (no counterpart in the reference): each shape
+ * has up to 4 candidate layouts (a warp per row with 4 or 8 warps per CTA;
+ * for complex rows wider than a warp, one point a lane with several warps
+ * per row); k >= 1 pins the k-th (shapes with fewer keep the tuned one),
+ * 0 returns to the tuned choice.  Process-wide; for tests and tuning
+ * studies.  GPW_EINVAL outside [0, 16].                                   */
+int gpw_set_bloch_layout(int k);
+
+/* Launches of that kernel so far in this process (tests use it to see that
+ * a shape took the kernel rather than the general one).                   */
+int64_t gpw_bloch_launch_count(void);
+
 /* Inner V-cycle schedule of the float32 defect-correction form
  * (precision 1; no counterpart in the reference, whose only schedule is the
  * float64 one of gpaw/poisson.py:111-128, 191-192, which precision 0 keeps).
