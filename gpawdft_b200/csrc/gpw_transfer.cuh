@@ -43,48 +43,73 @@ struct TransferArgs {
   double w2, c02;
 };
 
-// Load plane p of the box rows [ys, ys+H) x cols [xs, xs+W) (unpadded input
-// coordinates) into `slot` (row pitch W), zero-filling zero-boundary halo.
-template <typename T>
-__device__ __forceinline__ void load_box(T* slot, const T* in, const GridView& v, const Boundary& bc, int p,
-                                         int ys, int xs, int H, int W) {
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const int nthr = blockDim.x * blockDim.y;
-  int j0, s0;
-  const bool ok0 = wrap_axis(p, v.n[0], bc.periodic[0], j0, s0);
-  const T* base = in + (int64_t)j0 * v.s0;
-  for (int idx = tid; idx < H * W; idx += nthr) {
-    const int r = idx / W, c = idx - r * W;
-    int j1, j2, s1, s2;
-    const bool ok = ok0 && wrap_axis(ys + r, v.n[1], bc.periodic[1], j1, s1) &&
-                    wrap_axis(xs + c, v.n[2], bc.periodic[2], j2, s2);
-    cp_async<sizeof(T)>(slot + idx, ok ? base + (int64_t)j1 * v.s1 + j2 : in, ok);
-  }
-}
+// Per-thread descriptors of a box's cells (H x W, NT threads, cell k of a
+// thread = tid + k NT): the box origin in (axis 1, axis 2) is fixed for the
+// CTA, so each cell's in-plane source offset, validity and wrap sides are
+// computed once; loading a plane is then one cp.async per cell and the
+// Bloch fix-up touches only wrapped cells.
+template <typename T, int H, int W, int NT>
+struct BoxLoader {
+  static constexpr int NLD = (H * W + NT - 1) / NT;
+  int off[NLD];            // j1 * s1 + j2
+  unsigned valid = 0;      // bit k: cell k is inside the grid or a periodic image
+  unsigned wrapped = 0;    // bit k: cell k is a periodic image along axis 1 or 2
+  unsigned char side[NLD]; // wrap sides: bits 0-1 axis 1 (+1), bits 2-3 axis 2 (+1)
 
-template <typename T>
-__device__ __forceinline__ void fix_box(T* slot, const GridView& v, const Boundary& bc, int p, int ys, int xs,
-                                        int H, int W) {
-  if constexpr (EltTraits<T>::cpx) {
+  __device__ __forceinline__ void init(const GridView& v, const Boundary& bc, int ys, int xs) {
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    const int nthr = blockDim.x * blockDim.y;
-    int j0, s0;
-    if (!wrap_axis(p, v.n[0], bc.periodic[0], j0, s0)) return;
-    for (int idx = tid; idx < H * W; idx += nthr) {
+#pragma unroll
+    for (int k = 0; k < NLD; ++k) {
+      const int idx = tid + k * NT;
       const int r = idx / W, c = idx - r * W;
-      int j1, j2, s1, s2;
-      const bool ok = wrap_axis(ys + r, v.n[1], bc.periodic[1], j1, s1) &&
+      int j1 = 0, j2 = 0, s1 = -1, s2 = -1;
+      const bool ok = idx < H * W && wrap_axis(ys + r, v.n[1], bc.periodic[1], j1, s1) &&
                       wrap_axis(xs + c, v.n[2], bc.periodic[2], j2, s2);
-      if (!ok || (s0 < 0 && s1 < 0 && s2 < 0)) continue;
-      // axis by axis, as the reference's chained halo copies apply them
-      T val = slot[idx];
-      if (s0 >= 0) val = phase_mul(bc.ph[0][s0], val);
-      if (s1 >= 0) val = phase_mul(bc.ph[1][s1], val);
-      if (s2 >= 0) val = phase_mul(bc.ph[2][s2], val);
-      slot[idx] = val;
+      off[k] = ok ? (int)((int64_t)j1 * v.s1 + j2) : 0;
+      if (ok) valid |= 1u << k;
+      if (ok && (s1 >= 0 || s2 >= 0)) wrapped |= 1u << k;
+      side[k] = (unsigned char)((s1 + 1) | ((s2 + 1) << 2));
     }
   }
-}
+
+  // plane p into `slot` (row pitch W); zero-boundary cells read zeros
+  __device__ __forceinline__ void load(T* slot, const T* in, const GridView& v, const Boundary& bc, int p) const {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    int j0, s0;
+    const bool ok0 = wrap_axis(p, v.n[0], bc.periodic[0], j0, s0);
+    const T* base = in + (int64_t)j0 * v.s0;
+#pragma unroll
+    for (int k = 0; k < NLD; ++k) {
+      const int idx = tid + k * NT;
+      if ((H * W) % NT == 0 || idx < H * W) {
+        const bool ok = ok0 && ((valid >> k) & 1u);
+        cp_async<sizeof(T)>(slot + idx, ok ? base + off[k] : in, ok);
+      }
+    }
+  }
+
+  // Bloch phases of the periodic images, axis by axis as the reference's
+  // chained halo copies apply them (each thread fixes its own copies)
+  __device__ __forceinline__ void fix(T* slot, const GridView& v, const Boundary& bc, int p) const {
+    if constexpr (EltTraits<T>::cpx) {
+      const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+      int j0, s0;
+      if (!wrap_axis(p, v.n[0], bc.periodic[0], j0, s0)) return;
+      const unsigned todo = s0 >= 0 ? valid : wrapped;
+#pragma unroll
+      for (int k = 0; k < NLD; ++k) {
+        if (!((todo >> k) & 1u)) continue;
+        const int idx = tid + k * NT;
+        const int s1 = (side[k] & 3) - 1, s2 = ((side[k] >> 2) & 3) - 1;
+        T val = slot[idx];
+        if (s0 >= 0) val = phase_mul(bc.ph[0][s0], val);
+        if (s1 >= 0) val = phase_mul(bc.ph[1][s1], val);
+        if (s2 >= 0) val = phase_mul(bc.ph[2][s2], val);
+        slot[idx] = val;
+      }
+    }
+  }
+};
 
 // unfused helpers for exact reference arithmetic
 __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
@@ -189,21 +214,23 @@ __global__ void __launch_bounds__(RS_OZ* RS_OY) restrict_kernel(const TransferAr
 #pragma unroll
   for (int i = 0; i < NQ; ++i) q[i] = zero<T>();
 
+  BoxLoader<T, H, W, RS_OZ * RS_OY> ld;
+  ld.init(a.vin, a.bc, ys, xs);
 #pragma unroll
   for (int st = 0; st < NS - 1; ++st) {
-    if (st < nsteps) load_box<T>(ring + st * H * W, in, a.vin, a.bc, pfirst + st, ys, xs, H, W);
+    if (st < nsteps) ld.load(ring + st * H * W, in, a.vin, a.bc, pfirst + st);
     cp_async_commit();
   }
   for (int s = 0; s < nsteps; ++s) {
     const int p = pfirst + s;
     {
       const int sn = s + NS - 1;
-      if (sn < nsteps) load_box<T>(ring + (sn % NS) * H * W, in, a.vin, a.bc, pfirst + sn, ys, xs, H, W);
+      if (sn < nsteps) ld.load(ring + (sn % NS) * H * W, in, a.vin, a.bc, pfirst + sn);
       cp_async_commit();
     }
     cp_async_wait<NS - 1>();
     T* sl = ring + (s % NS) * H * W;
-    if (a.bc.use_phase) fix_box<T>(sl, a.vin, a.bc, p, ys, xs, H, W);
+    if (a.bc.use_phase) ld.fix(sl, a.vin, a.bc, p);
     __syncthreads();
     // axis-2 pass: zb[r][J] for all H rows
     for (int idx = tid; idx < H * RS_OZ; idx += RS_OZ * RS_OY) {
@@ -276,21 +303,23 @@ __global__ void __launch_bounds__(IP_OZ* IP_OY) interpolate_kernel(const Transfe
 #pragma unroll
   for (int i = 0; i < NQ; ++i) q[i] = zero<T>();
 
+  BoxLoader<T, H, W, IP_OZ * IP_OY> ld;
+  ld.init(a.vin, a.bc, ys, xs);
 #pragma unroll
   for (int st = 0; st < NS - 1; ++st) {
-    if (st < nsteps) load_box<T>(ring + st * H * W, in, a.vin, a.bc, pfirst + st, ys, xs, H, W);
+    if (st < nsteps) ld.load(ring + st * H * W, in, a.vin, a.bc, pfirst + st);
     cp_async_commit();
   }
   for (int s = 0; s < nsteps; ++s) {
     const int p = pfirst + s;
     {
       const int sn = s + NS - 1;
-      if (sn < nsteps) load_box<T>(ring + (sn % NS) * H * W, in, a.vin, a.bc, pfirst + sn, ys, xs, H, W);
+      if (sn < nsteps) ld.load(ring + (sn % NS) * H * W, in, a.vin, a.bc, pfirst + sn);
       cp_async_commit();
     }
     cp_async_wait<NS - 1>();
     T* sl = ring + (s % NS) * H * W;
-    if (a.bc.use_phase) fix_box<T>(sl, a.vin, a.bc, p, ys, xs, H, W);
+    if (a.bc.use_phase) ld.fix(sl, a.vin, a.bc, p);
     __syncthreads();
     // axis-2 pass: zb[r][x] for each fine output column x of the tile
     for (int idx = tid; idx < H * IP_OZ; idx += IP_OZ * IP_OY) {
