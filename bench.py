@@ -39,6 +39,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_GRID = 128
+N_GRID_PTS = (N_GRID - 1) ** 3   # unknowns of one zero-boundary grid
 H_ANG = 0.2
 N_GAUSS = 8
 REL_TOL = 1e-10
@@ -264,6 +265,8 @@ def run_ours(args, rank, world, dist):
                        batch=B)
     ps.set_grid_descriptor(gd)
     ps.initialize()
+    if args.host_loop:
+        ps.set_device_loop(False)
     lib = _lib.load()
     rho_d = torch.from_numpy(rho_h).to(dev)
     phi_d = torch.zeros_like(rho_d)
@@ -353,6 +356,13 @@ def run_ours(args, rank, world, dist):
         kernels[which] = (ms.value / 1e3, nbytes.value)
     # the dominant kernel: the largest time per outer iteration
     dom = max(per_iter, key=lambda w: kernels[w][0] * per_iter[w])
+    # DRAM bytes (read + write) per grid point of the level-0 kernels, from
+    # single-launch ncu captures of these kernels at 8 x 127^3 points
+    # ((dram__bytes_read.sum + dram__bytes_write.sum) / points); traffic
+    # grows with the points, so a launch's traffic is this times its points
+    ncu_bytes_per_point = {2: (139.83e6 + 40.00e6) / 16387064,
+                           4: (292.3e6 + 103.9e6) / 16387064,
+                           3: (268.9e6 + 90.9e6) / 16387064}
     t_sweep, sweep_bytes = kernels[dom]
     achieved = sweep_bytes / t_sweep / 1e9
     peak, peak_src = measured_peak()
@@ -404,7 +414,10 @@ def run_ours(args, rank, world, dist):
                    'd2h_bytes_per_step': io_bytes},
            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                         'unit': 'GB/s', 'frac': achieved / peak,
-                        'traffic': None,
+                        'traffic': (ncu_bytes_per_point[dom] * B * N_GRID_PTS
+                                    if dom in ncu_bytes_per_point else None),
+                        'traffic_source': 'ncu capture at batch 8, scaled to '
+                                          'the launch\'s grid points',
                         'kernel': names[dom] + ' (batch %d)' % B,
                         'algorithmic_bytes_per_launch': sweep_bytes,
                         'launch_ms': t_sweep * 1e3,
@@ -774,6 +787,9 @@ def main():
                     help='learned128: training pairs')
     ap.add_argument('--save-weights', default=None,
                     help='learned128: save the trained network (.npz)')
+    ap.add_argument('--host-loop', action='store_true',
+                    help='replay the iteration graph from the host instead of '
+                         'the device-side loop (for per-kernel profiling)')
     ap.add_argument('--no-cpu', action='store_true',
                     help='skip the cpu_baseline sample')
     args = ap.parse_args()

@@ -187,7 +187,8 @@ struct PadGeom {
 };
 
 template <typename S>
-__device__ __forceinline__ void pg_jacobi(const CoarseLevel& L, const S* src, S* dst, const S* rho, double wd) {
+__device__ __forceinline__ void pg_jacobi(const CoarseLevel& L, const S* __restrict__ src, S* __restrict__ dst,
+                                          const S* __restrict__ rho, double wd) {
   const PadGeom g(L);
   const S w = (S)wd, wc = w / (S)L.cc;
   const S c0m = (S)L.cm[0], c0p = (S)L.cp[0], c1m = (S)L.cm[1], c1p = (S)L.cp[1], c2m = (S)L.cm[2],
@@ -195,6 +196,7 @@ __device__ __forceinline__ void pg_jacobi(const CoarseLevel& L, const S* src, S*
   for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
     const int i1 = c / g.n2, i2 = c - i1 * g.n2;
     int k = g.at(0, i1, i2);
+#pragma unroll 4
     for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) {
       S av = c2m * src[k - 1];
       av = fmac(c2p, src[k + 1], av);
@@ -209,13 +211,15 @@ __device__ __forceinline__ void pg_jacobi(const CoarseLevel& L, const S* src, S*
 }
 
 template <typename S>
-__device__ __forceinline__ void pg_residual(const CoarseLevel& L, const S* phi, S* r, const S* rho) {
+__device__ __forceinline__ void pg_residual(const CoarseLevel& L, const S* __restrict__ phi, S* __restrict__ r,
+                                            const S* __restrict__ rho) {
   const PadGeom g(L);
   const S c0m = (S)L.cm[0], c0p = (S)L.cp[0], c1m = (S)L.cm[1], c1p = (S)L.cp[1], c2m = (S)L.cm[2],
           c2p = (S)L.cp[2], cc = (S)L.cc;
   for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
     const int i1 = c / g.n2, i2 = c - i1 * g.n2;
     int k = g.at(0, i1, i2);
+#pragma unroll 4
     for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) {
       S av = c2m * phi[k - 1];
       av = fmac(c2p, phi[k + 1], av);
@@ -231,13 +235,14 @@ __device__ __forceinline__ void pg_residual(const CoarseLevel& L, const S* phi, 
 
 // rho_C = R r_F and phi_C = 0 (zero boundaries: fine centre 2I + 1)
 template <typename S>
-__device__ __forceinline__ void pg_restrict(const CoarseLevel& F, const S* r, const CoarseLevel& C, S* rho_c,
-                                            S* phi_c) {
+__device__ __forceinline__ void pg_restrict(const CoarseLevel& F, const S* __restrict__ r, const CoarseLevel& C,
+                                            S* __restrict__ rho_c, S* __restrict__ phi_c) {
   const PadGeom f(F), g(C);
   for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
     const int I1 = c / g.n2, I2 = c - I1 * g.n2;
     int k = g.at(0, I1, I2);
     int kf = f.at(1, 2 * I1 + 1, 2 * I2 + 1);  // fine centre of I0 = 0
+#pragma unroll 2
     for (int I0 = 0; I0 < g.n0; ++I0, k += g.sz, kf += 2 * f.sz) {
       S y[3];
 #pragma unroll
@@ -269,8 +274,8 @@ __device__ __forceinline__ S pg_interp_plane(const S* e, const PadGeom& g, int q
 }
 
 template <typename S>
-__device__ __forceinline__ void pg_interp_sub(const CoarseLevel& F, const S* base, S* dst, const CoarseLevel& C,
-                                              const S* e) {
+__device__ __forceinline__ void pg_interp_sub(const CoarseLevel& F, const S* __restrict__ base, S* __restrict__ dst,
+                                              const CoarseLevel& C, const S* __restrict__ e) {
   const PadGeom f(F), g(C);
   for (int c = threadIdx.x; c < f.n1 * f.n2; c += blockDim.x) {
     const int o1 = c / f.n2, o2 = c - o1 * f.n2;
@@ -279,6 +284,7 @@ __device__ __forceinline__ void pg_interp_sub(const CoarseLevel& F, const S* bas
     const int e1 = t1 & 1, e2 = t2 & 1;
     const int qc = (t1 >> 1) * g.sy + (t2 >> 1);  // padded in-plane coarse index
     int k = f.at(0, o1, o2);
+#pragma unroll 4
     for (int o0 = 0; o0 < f.n0; ++o0, k += f.sz) {
       const int t0 = o0 + 1;
       const int q = (t0 >> 1) * g.sz + qc;

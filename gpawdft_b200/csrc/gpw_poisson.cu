@@ -926,6 +926,16 @@ int gpw_poisson_solve(gpw_poisson* ps, double* phi, const double* rho, int64_t n
   return rc;
 }
 
+// Convergence loop driver: on (default) the device-side loop (a conditional
+// graph node); off the host replays the iteration graph, one graph launch
+// per outer iteration (the same kernels; profilers that cannot see inside
+// conditional graph nodes time each kernel this way).
+extern "C" int gpw_poisson_set_device_loop(gpw_poisson* ps, int on) {
+  if (!ps) return fail(GPW_EINVAL, "null argument");
+  ps->device_loop = on != 0;
+  return GPW_OK;
+}
+
 // Per-solve latency of the last solve: device time from the start of the
 // iterations to the end of the iteration in which each solve converged.
 extern "C" int gpw_poisson_last_latency(gpw_poisson* ps, int64_t nbatch, double* ms, gpw_stream stream) {

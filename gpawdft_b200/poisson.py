@@ -247,6 +247,8 @@ class FDPoissonSolver:
                                        int(nbatch), ctypes.byref(h)))
         self._engine = (h, int(nbatch))
         self._lib = lib
+        if not getattr(self, '_device_loop', True):
+            _lib.check(lib.gpw_poisson_set_device_loop(h, 0))
         if (self.precision == 'fp32' and self.inner == 'chebyshev' and
                 self.relax_method == 2 and L > 1):
             npre, npost, ws = inner_schedule(self.operators)
@@ -255,6 +257,17 @@ class FDPoissonSolver:
             a_w = (ctypes.c_double * len(ws))(*ws)
             _lib.check(lib.gpw_poisson_set_inner_schedule(h, a_pre, a_post,
                                                           a_w, len(ws)))
+
+    def set_device_loop(self, on=True):
+        """Run the convergence loop on the device (default) or replay one
+        iteration graph per outer iteration from the host (same kernels and
+        results; for profilers that cannot look inside conditional graph
+        nodes)."""
+        if self._engine is None:
+            self.initialize()
+        _lib.check(self._lib.gpw_poisson_set_device_loop(self._engine[0],
+                                                         int(bool(on))))
+        self._device_loop = bool(on)
 
     def _free_engine(self):
         if self._engine is not None:

@@ -237,6 +237,13 @@ int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
                             int reps, double *ms_per_launch,
                             double *bytes_per_launch, gpw_stream stream);
 
+/* Convergence loop driver of a Poisson engine (no counterpart in the
+ * reference): on = 1 (default) runs the whole loop on the device as a
+ * conditional graph node; on = 0 replays the iteration graph from the host,
+ * one graph launch per outer iteration (the same kernels and results;
+ * profilers that cannot look inside conditional graph nodes need it).     */
+int gpw_poisson_set_device_loop(gpw_poisson *ps, int on);
+
 /* Pins the tile variant of the TMA star-stencil kernels (no counterpart in
  * the reference): with variant >= 0 every later TMA stencil launch whose
  * element type and radius have that variant uses it, with `nchunk` axis-0
