@@ -107,7 +107,10 @@ struct TmaCfg {
   static constexpr int W = TZ + 2 * XL;                // box width (elements)
   static constexpr int H = TY + 2 * R;                 // box height
   static constexpr int D = Sh::D;                      // planes prefetched beyond the current one
-  static constexpr int NS = R + D + 1;                 // ring stages
+  // ring stages: a Jacobi sweep re-reads its centre value R planes behind;
+  // the other epilogues read each plane once, at arrival
+  static constexpr bool KEEP_CENTRE = MODE == MODE_JACOBI || MODE == MODE_JACOBI_ADD64;
+  static constexpr int NS = KEEP_CENTRE ? R + D + 1 : D + 1;
   // per stage: the input plane (with halo), the rho plane of the output
   // completed at that step, and (JACOBI_ADD64) the float64 phi plane
   static constexpr bool HAS_RHO = MODE != MODE_APPLY;
@@ -314,7 +317,6 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
         }
         // output plane o is complete: logical slot 0 = physical ph
         if (o >= z0) {
-          const S* osl = reinterpret_cast<const S*>(ring + ((s + NS - R) % NS) * C::STAGE_BYTES);
           const S* rsl = reinterpret_cast<const S*>(stg + C::RHO_OFF);
           const double* asl = reinterpret_cast<const double*>(stg + C::AUX_OFF);
 #pragma unroll
@@ -343,6 +345,8 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
                   }
                 }
               } else {
+                // the centre value, R planes behind in the ring
+                const S* osl = reinterpret_cast<const S*>(ring + ((s + NS - R) % NS) * C::STAGE_BYTES);
                 const P cur = ldv<S, VEC>(osl + (yb + j + R) * W + xl);
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) res.v[e] = k.w1 * cur.v[e] + k.wc * (rho.v[e] - av.v[e]);
