@@ -359,6 +359,7 @@ __device__ void coarse_vcycle_padded(const CoarseArgs& a, S* sm, int b) {
 
 template <typename S>
 __global__ void __launch_bounds__(CG_THREADS, 1) coarse_vcycle_kernel(const CoarseArgs a) {
+  pdl_wait();
   const int b = blockIdx.x;
   if (a.active && !a.active[b]) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];

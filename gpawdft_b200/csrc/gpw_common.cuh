@@ -14,6 +14,16 @@
 
 namespace gpw {
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may be dispatched while its predecessor in the stream still
+// runs.  It calls pdl_wait() before its first access to global memory (the
+// wait returns once the predecessor has finished and its writes are
+// visible; without the launch attribute it returns at once), and
+// pdl_trigger() once its own main loop is done, letting its successor's CTAs
+// take SM slots as this grid drains.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // ------------------------------------------------------------------ scalars
 // Element types: double (f64), float (f32), double2 (c128), float2 (c64).
 // Coefficients are always real, as in the reference (bmgsstencil.coefs is

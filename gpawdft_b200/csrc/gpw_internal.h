@@ -200,6 +200,26 @@ struct SumScratch {
 
 int num_sms();
 
+// Programmatic dependent launch of the V-cycle's kernels (gpw_set_pdl; on by
+// default): the kernel is launched with programmatic stream serialization
+// and must call pdl_wait() before touching global memory.
+bool pdl_enabled();
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 // Periodic / Bloch (or mixed-boundary) star applies on the TMA row kernel
 // (gpw_bloch.cu): eligibility and launch.
 bool bloch_path_ok(const OpDesc& d, int dtype, const void* in, const GridView& vin, const void* out,

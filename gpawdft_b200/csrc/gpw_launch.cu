@@ -16,6 +16,9 @@
 
 namespace gpw {
 
+static std::atomic<int> g_pdl{1};
+bool pdl_enabled() { return g_pdl.load() != 0; }
+
 int num_sms() {
   static int sms = 0;
   if (!sms) {
@@ -236,6 +239,11 @@ static cudaError_t tma_launch(int dtype, int mode, int R, const TmaChoice& ch, c
                               const StarCoefs& sc, cudaStream_t st) {
   if (dtype == GPW_F64) return tma_stencil_f64(mode, R, ch.var, a, nbatch, sc, ch.nchunk, st);
   return tma_stencil_f32(mode, R, ch.var, a, nbatch, sc, ch.nchunk, st);
+}
+
+extern "C" int gpw_set_pdl(int on) {
+  g_pdl.store(on ? 1 : 0);
+  return GPW_OK;
 }
 
 extern "C" int gpw_set_tma_variant(int variant, int nchunk) {
@@ -484,7 +492,6 @@ static cudaError_t dispatch_transfer(const TransferArgs& a, int k, bool interp, 
 // ------------------------------------------------------------------ coarse levels
 cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatch, cudaStream_t st) {
   if (a.nl < 1 || a.nl > CG_MAXL || nbatch < 1 || smem > 200 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e;
   if (dtype == GPW_F64) {
     static std::once_flag once;
     static cudaError_t oe = cudaSuccess;
@@ -493,7 +500,7 @@ cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatc
                                 200 * 1024);
     });
     if (oe != cudaSuccess) return oe;
-    coarse_vcycle_kernel<double><<<nbatch, CG_THREADS, smem, st>>>(a);
+    return launch_pdl(coarse_vcycle_kernel<double>, dim3(nbatch), dim3(CG_THREADS), smem, st, a);
   } else if (dtype == GPW_F32) {
     static std::once_flag once;
     static cudaError_t oe = cudaSuccess;
@@ -502,12 +509,9 @@ cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatc
                                 200 * 1024);
     });
     if (oe != cudaSuccess) return oe;
-    coarse_vcycle_kernel<float><<<nbatch, CG_THREADS, smem, st>>>(a);
-  } else {
-    return cudaErrorInvalidValue;
+    return launch_pdl(coarse_vcycle_kernel<float>, dim3(nbatch), dim3(CG_THREADS), smem, st, a);
   }
-  e = cudaGetLastError();
-  return e;
+  return cudaErrorInvalidValue;
 }
 
 // The vector interpolation needs 16-byte aligned rows / planes / batch
@@ -575,7 +579,9 @@ static cudaError_t run_restrict_tma(TransferArgs a, int nbatch, cudaStream_t st)
   a.nchunk = (int)nc;
   a.zchunk = (a.vout.n[0] + a.nchunk - 1) / a.nchunk;
   grid.z = a.nchunk * nbatch;
-  restrict_k2_tma_kernel<S><<<grid, dim3(RK_TX, RK_TY), C::smem, st>>>(map, a, device_status_word());
+  cudaError_t le = launch_pdl(restrict_k2_tma_kernel<S>, grid, dim3(RK_TX, RK_TY), C::smem, st, map, a,
+                              device_status_word());
+  if (le != cudaSuccess) return le;
   return cudaGetLastError();
 }
 
@@ -634,7 +640,9 @@ static cudaError_t run_interp_tma(TransferArgs a, int nbatch, cudaStream_t st) {
   a.nchunk = (int)nc;
   a.zchunk = (nm + a.nchunk - 1) / a.nchunk;
   grid.z = a.nchunk * nbatch;
-  interpolate_k2_tma_kernel<S><<<grid, dim3(IK_TX, IK_NTY), C::smem, st>>>(cmap, bmap, a, device_status_word());
+  cudaError_t le = launch_pdl(interpolate_k2_tma_kernel<S>, grid, dim3(IK_TX, IK_NTY), C::smem, st, cmap, bmap, a,
+                              device_status_word());
+  if (le != cudaSuccess) return le;
   return cudaGetLastError();
 }
 
@@ -690,11 +698,8 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
     a.nchunk = (vout.n[0] + a.zchunk - 1) / a.zchunk;
     grid.z = a.nchunk * nbatch;
     const dim3 blk(K2V_TX, K2V_TY);
-    if (dtype == GPW_F64)
-      restrict_k2_vec_kernel<double><<<grid, blk, 0, st>>>(a);
-    else
-      restrict_k2_vec_kernel<float><<<grid, blk, 0, st>>>(a);
-    return cudaGetLastError();
+    if (dtype == GPW_F64) return launch_pdl(restrict_k2_vec_kernel<double>, grid, blk, 0, st, a);
+    return launch_pdl(restrict_k2_vec_kernel<float>, grid, blk, 0, st, a);
   }
   if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32) && interp && k2i_tma_ok(a, elt_size(dtype), nbatch))
     return dtype == GPW_F64 ? run_interp_tma<double>(a, nbatch, st) : run_interp_tma<float>(a, nbatch, st);
@@ -709,11 +714,8 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
     a.nchunk = (vout.n[0] + a.zchunk - 1) / a.zchunk;
     grid.z = a.nchunk * nbatch;
     const dim3 blk(K2V_TX, K2V_TY);
-    if (dtype == GPW_F64)
-      interpolate_k2_vec_kernel<double><<<grid, blk, 0, st>>>(a);
-    else
-      interpolate_k2_vec_kernel<float><<<grid, blk, 0, st>>>(a);
-    return cudaGetLastError();
+    if (dtype == GPW_F64) return launch_pdl(interpolate_k2_vec_kernel<double>, grid, blk, 0, st, a);
+    return launch_pdl(interpolate_k2_vec_kernel<float>, grid, blk, 0, st, a);
   }
   if (d.k == 2 && (dtype == GPW_F64 || dtype == GPW_F32)) {
     dim3 grid((vout.n[2] + K2_TX - 1) / K2_TX, (vout.n[1] + K2_TY - 1) / K2_TY, 1);
@@ -722,14 +724,14 @@ cudaError_t launch_transfer(const TrDesc& d, int dtype, const void* in, const Gr
     const dim3 blk(K2_TX, K2_TY);
     if (dtype == GPW_F64) {
       if (interp)
-        interpolate_k2_kernel<double><<<grid, blk, 0, st>>>(a);
+        return launch_pdl(interpolate_k2_kernel<double>, grid, blk, 0, st, a);
       else
-        restrict_k2_kernel<double><<<grid, blk, 0, st>>>(a);
+        return launch_pdl(restrict_k2_kernel<double>, grid, blk, 0, st, a);
     } else {
       if (interp)
-        interpolate_k2_kernel<float><<<grid, blk, 0, st>>>(a);
+        return launch_pdl(interpolate_k2_kernel<float>, grid, blk, 0, st, a);
       else
-        restrict_k2_kernel<float><<<grid, blk, 0, st>>>(a);
+        return launch_pdl(restrict_k2_kernel<float>, grid, blk, 0, st, a);
     }
     return cudaGetLastError();
   }

@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + NS * C::STAGE_BYTES);
   __shared__ double red[32];
   const StencilArgs& a = ta.s;
+  pdl_wait();  // the predecessor's results (and the active mask) are visible from here
 
   const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
   if (a.active && !a.active[b]) return;
@@ -401,6 +402,7 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
       }
     }
   }
+  pdl_trigger();
   if (timed_out && ta.status) atomicExch(ta.status, GPW_ETIMEDOUT);
   if constexpr (MODE == MODE_RESIDUAL || MODE == MODE_RESID_DC) {
     if (a.gsum.partial) {

@@ -108,8 +108,8 @@ struct TmaKernel {
     a.nblk_seg = grid.x * grid.y * nc;
     TmaArgs ta{a, device_status_word()};
     const TmaCoefs<S> kc = tma_coefs<S>(sc, R, a.w, a.c0, a.w2);
-    star_tma_kernel<S, R, MODE, VAR><<<grid, dim3(C::NTX, C::NTY), C::smem, st>>>(map_in, map_rho, map_aux, ta, kc);
-    return cudaGetLastError();
+    return launch_pdl(star_tma_kernel<S, R, MODE, VAR>, grid, dim3(C::NTX, C::NTY), C::smem, st, map_in, map_rho,
+                      map_aux, ta, kc);
   }
 };
 

@@ -55,6 +55,7 @@ __device__ __forceinline__ S k2_ld(const S* __restrict__ p, bool ok) {
 
 template <typename S>
 __global__ void __launch_bounds__(K2_TX* K2_TY) restrict_k2_kernel(const TransferArgs a) {
+  pdl_wait();
   const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
   if (a.active && !a.active[b]) return;
   const int I2 = blockIdx.x * K2_TX + threadIdx.x, I1 = blockIdx.y * K2_TY + threadIdx.y;
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(K2_TX* K2_TY) restrict_k2_kernel(const Transfe
 
 template <typename S>
 __global__ void __launch_bounds__(K2_TX* K2_TY) interpolate_k2_kernel(const TransferArgs a) {
+  pdl_wait();
   const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
   if (a.active && !a.active[b]) return;
   const int o2 = blockIdx.x * K2_TX + threadIdx.x, o1 = blockIdx.y * K2_TY + threadIdx.y;
@@ -210,6 +212,7 @@ __device__ __forceinline__ void st4(S* p, const S (&v)[4], int nvalid) {
 
 template <typename S>
 __global__ void __launch_bounds__(K2V_TX* K2V_TY) interpolate_k2_vec_kernel(const TransferArgs a) {
+  pdl_wait();
   const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
   if (a.active && !a.active[b]) return;
   const int o2 = 4 * (blockIdx.x * K2V_TX + threadIdx.x), o1 = blockIdx.y * K2V_TY + threadIdx.y;
@@ -332,6 +335,7 @@ __device__ __forceinline__ void st2(S* p, S v0, S v1, int nvalid) {
 
 template <typename S>
 __global__ void __launch_bounds__(K2V_TX* K2V_TY) restrict_k2_vec_kernel(const TransferArgs a) {
+  pdl_wait();
   const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
   if (a.active && !a.active[b]) return;
   const int I2 = 2 * (blockIdx.x * K2V_TX + threadIdx.x), I1 = blockIdx.y * K2V_TY + threadIdx.y;
@@ -423,6 +427,7 @@ __global__ void __launch_bounds__(RK_TX* RK_TY) restrict_k2_tma_kernel(const __g
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* ring = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + RK_NS * C::STAGE);
+  pdl_wait();
   const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
   if (a.active && !a.active[b]) return;
   const int nc0 = a.vout.n[0];
@@ -481,6 +486,7 @@ __global__ void __launch_bounds__(RK_TX* RK_TY) restrict_k2_tma_kernel(const __g
       if (n1 + 1 < nsteps) issue(n1 + 1);
     }
   }
+  pdl_trigger();
   if (timed_out && status) atomicExch(status, GPW_ETIMEDOUT);
 }
 
@@ -517,6 +523,7 @@ __global__ void __launch_bounds__(IK_TX* IK_NTY) interpolate_k2_tma_kernel(const
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* ring = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + IK_NS * C::STAGE);
+  pdl_wait();
   const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
   if (a.active && !a.active[b]) return;
   const int nf0 = a.vout.n[0];
@@ -608,6 +615,7 @@ __global__ void __launch_bounds__(IK_TX* IK_NTY) interpolate_k2_tma_kernel(const
     __syncthreads();  // plane step i - 1 is consumed
     if (tid == 0 && i + IK_D + 1 < nsteps) issue(i + IK_D + 1);
   }
+  pdl_trigger();
   if (timed_out && status) atomicExch(status, GPW_ETIMEDOUT);
 }
 

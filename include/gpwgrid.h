@@ -244,6 +244,14 @@ int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
  * profilers that cannot look inside conditional graph nodes need it).     */
 int gpw_poisson_set_device_loop(gpw_poisson *ps, int on);
 
+/* Programmatic dependent launch of the V-cycle's kernels (no counterpart in
+ * the reference): on = 1 (default) lets each stencil / transfer / coarse
+ * kernel be dispatched while its predecessor drains (the kernel waits for
+ * the predecessor's results before touching memory); on = 0 launches them
+ * strictly one after another.  Results are identical either way.
+ * Process-wide; takes effect for graphs captured afterwards.              */
+int gpw_set_pdl(int on);
+
 /* Pins the tile variant of the TMA star-stencil kernels (no counterpart in
  * the reference): with variant >= 0 every later TMA stencil launch whose
  * element type and radius have that variant uses it, with `nchunk` axis-0

@@ -237,6 +237,38 @@ def test_solve_stream_equals_batch(cuda, precision):
             want[k]).max()
 
 
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_pdl_off_equals_on(cuda, precision):
+    """Programmatic dependent launch changes when kernels are dispatched,
+    not what they compute: solves with it off equal those with it on."""
+    from gpawdft_b200 import _lib
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    lib = _lib.load()
+    N = 48
+    rhos = []
+    for s in range(2):
+        rho, L = gaussian_density(N, 0.2, 6 + s, 90 + s)
+        rhos.append(rho)
+    rhos = np.array(rhos)
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    eps = 1e-20 * max(float(np.dot(r.ravel(), r.ravel())) for r in rhos)
+    out = []
+    try:
+        for on in (1, 0):
+            _lib.check(lib.gpw_set_pdl(on))
+            ps = PoissonSolver(nn=3, batch=2, precision=precision, maxiter=200)
+            ps.set_grid_descriptor(gd)
+            ps.initialize()
+            phi = np.zeros_like(rhos)
+            n = ps.solve_batch(phi, rhos, eps=eps)
+            out.append((phi, n))
+    finally:
+        _lib.check(lib.gpw_set_pdl(1))
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][0], out[1][0])
+
+
 def test_full_size_127_trajectory(cuda):
     """127^3 (the benchmark grid): the engine's vector transfers, TMA
     stencil variants and one-CTA coarse levels reproduce the reference's
