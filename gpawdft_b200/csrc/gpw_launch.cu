@@ -543,6 +543,23 @@ static bool k2r_tma_ok(const TransferArgs& a, size_t es, int nbatch) {
   return a.vout.n[2] >= 16;
 }
 
+// Chunks of a march of n steps over `tiles` tiles: CTAs run in waves of
+// `slots`, each chunk pays `warm` extra steps; the count (at most maxc) with
+// the least modelled time, waves x steps per chunk.
+static int wave_chunks(int n, int64_t tiles, int warm, int64_t slots, int maxc) {
+  int best = 1;
+  double bestc = 1e300;
+  for (int nc = 1; nc <= std::max(1, maxc); ++nc) {
+    const int64_t waves = (tiles * nc + slots - 1) / slots;
+    const double cost = (double)waves * ((n + nc - 1) / nc + warm);
+    if (cost < bestc * (1 - 1e-9)) {
+      best = nc;
+      bestc = cost;
+    }
+  }
+  return best;
+}
+
 template <typename S>
 static cudaError_t run_restrict_tma(TransferArgs a, int nbatch, cudaStream_t st) {
   using C = RkCfg<S>;
@@ -573,10 +590,8 @@ static cudaError_t run_restrict_tma(TransferArgs a, int nbatch, cudaStream_t st)
     return cudaErrorInvalidValue;
   dim3 grid((a.vout.n[2] + RK_TX - 1) / RK_TX, (a.vout.n[1] + RK_TY - 1) / RK_TY, 1);
   const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
-  const int64_t want = (int64_t)std::max(1, per_sm) * num_sms();
-  int64_t nc = std::max<int64_t>(1, (want + tiles - 1) / tiles);
-  nc = std::min<int64_t>(nc, std::max(1, a.vout.n[0] / 2));
-  a.nchunk = (int)nc;
+  const int64_t slots = (int64_t)std::max(1, per_sm) * num_sms();
+  a.nchunk = wave_chunks(a.vout.n[0], tiles, 1, slots, a.vout.n[0] / 2);
   a.zchunk = (a.vout.n[0] + a.nchunk - 1) / a.nchunk;
   grid.z = a.nchunk * nbatch;
   cudaError_t le = launch_pdl(restrict_k2_tma_kernel<S>, grid, dim3(RK_TX, RK_TY), C::smem, st, map, a,
@@ -634,10 +649,8 @@ static cudaError_t run_interp_tma(TransferArgs a, int nbatch, cudaStream_t st) {
   dim3 grid((a.vout.n[2] + IK_FW - 1) / IK_FW, (a.vout.n[1] + IK_FH - 1) / IK_FH, 1);
   const int nm = a.vout.n[0] / 2 + 1;
   const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
-  const int64_t want = (int64_t)std::max(1, per_sm) * num_sms();
-  int64_t nc = std::max<int64_t>(1, (want + tiles - 1) / tiles);
-  nc = std::min<int64_t>(nc, std::max(1, nm / 2));
-  a.nchunk = (int)nc;
+  const int64_t slots = (int64_t)std::max(1, per_sm) * num_sms();
+  a.nchunk = wave_chunks(nm, tiles, 1, slots, nm / 2);
   a.zchunk = (nm + a.nchunk - 1) / a.nchunk;
   grid.z = a.nchunk * nbatch;
   cudaError_t le = launch_pdl(interpolate_k2_tma_kernel<S>, grid, dim3(IK_TX, IK_NTY), C::smem, st, cmap, bmap, a,
