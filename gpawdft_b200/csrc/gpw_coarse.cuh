@@ -21,6 +21,8 @@
 // same expressions as gpw_transfer_k2.cuh; boundaries are zero or periodic
 // (real data, no Bloch phase).
 #pragma once
+#include <cooperative_groups.h>
+
 #include "gpw_common.cuh"
 #include "gpw_transfer.cuh"
 #include "gpw_transfer_k2.cuh"
@@ -422,6 +424,256 @@ __global__ void __launch_bounds__(CG_THREADS, 1) coarse_vcycle_kernel(const Coar
       g[(int64_t)i0 * a.vphi.s0 + (int64_t)i1 * a.vphi.s1 + i2] = phi[i];
     }
   }
+}
+
+// ---------------------------------------------------------------- cluster top levels
+// The two levels above the one-CTA coarse levels (31^3 and 15^3 at
+// N_c = 128, float32 inner cycles) in a thread-block cluster of CG_NCL CTAs
+// per solve.  CTA r owns a slab of each: the top level's axis-0 planes
+// [r n0 / CG_NCL, (r + 1) n0 / CG_NCL), and of the second level the planes
+// whose restriction centres 2I + 1 lie in that range, each slab padded as
+// above with one halo plane per side.  After every pass the cluster
+// synchronises and each CTA copies its neighbours' boundary planes into its
+// halo planes through distributed shared memory.  Both levels run their
+// pre-sweeps and residual; the second level's residual is restricted into
+// the third level's rho (global memory), CTA 0 runs the coarse kernel's
+// V-cycle from there, and every CTA interpolates back up through its slabs
+// and runs the post-sweeps.  One launch replaces ~18.  Every pass uses the
+// padded functions above on a slab (a level of the CTA's own planes), so
+// the arithmetic is that of the coarse kernel.
+constexpr int CG_NCL = 8;            // CTAs per cluster (one solve)
+constexpr int CG_CLUSTER_THREADS = 256;  // threads per CTA: two CTAs per SM (registers and shared memory)
+
+struct ClusterTop {
+  CoarseLevel L;     // the top level (padded form)
+  CoarseLevel L2;    // the second level (padded form)
+  const void* rho;   // top-level rho, engine layout
+  void* phi;         // top-level phi: in, the first pre-sweep's iterate when first_done; out, the result
+  GridView v;        // engine view of the top level
+  int first_done;
+  int slab_pts;      // padded elements of one top-level slab buffer: (maxp + 2)(n1 + 2)(n2 + 2)
+  int slab2_pts;     // the same for the second level
+  int next_pts;      // padded elements of the third level
+};
+
+struct ClusterArgs {
+  CoarseArgs ca;     // third level .. coarsest (ca.rho: written here; ca.phi: read back)
+  ClusterTop t;
+};
+
+// slab boundaries: the top level's plane r n0 / CG_NCL, the second level's
+// half of it (capped at its extent)
+__device__ __forceinline__ int slab_begin(int rank, int n0) { return rank * n0 / CG_NCL; }
+__device__ __forceinline__ int slab2_begin(int rank, int n0, int m0) {
+  return rank >= CG_NCL ? m0 : min(m0, slab_begin(rank, n0) / 2);
+}
+
+// Fill the halo planes of slab buffer `buf` (np own planes, plane size sz)
+// from the neighbours' boundary planes; npm = the lower neighbour's planes.
+// All of a thread's remote loads (up to 8 per plane and pass) are issued
+// before its stores, so the copy pays the distributed-shared-memory latency
+// about once.
+template <typename S>
+__device__ __forceinline__ void slab_exchange(cooperative_groups::cluster_group& cl, S* buf, int rank, int np,
+                                              int npm, int sz) {
+  constexpr int U = 8;
+  cl.sync();
+  const S* lo = rank > 0 ? cl.map_shared_rank(buf, rank - 1) + npm * sz : nullptr;
+  const S* hi = rank < CG_NCL - 1 ? cl.map_shared_rank(buf, rank + 1) + sz : nullptr;
+  S* dlo = buf;
+  S* dhi = buf + (np + 1) * sz;
+  for (int j0 = 0; j0 < sz; j0 += U * (int)blockDim.x) {
+    S vl[U], vh[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int j = j0 + u * blockDim.x + threadIdx.x;
+      if (j < sz) {
+        if (lo) vl[u] = lo[j];
+        if (hi) vh[u] = hi[j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int j = j0 + u * blockDim.x + threadIdx.x;
+      if (j < sz) {
+        if (lo) dlo[j] = vl[u];
+        if (hi) dhi[j] = vh[u];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// rho_C(I) = R r for the coarse planes I in [Ia, Ib) (centres 2I + 1 in the
+// fine slab starting at plane z0), zero boundaries; written to `out` with
+// plane stride os0, row stride os1 at plane index I - oI0 (padded or engine
+// layout: `padded` adds the halo offset)
+template <typename S>
+__device__ __forceinline__ void slab_restrict(const CoarseLevel& F, const S* __restrict__ r, int z0, int Ia, int Ib,
+                                              const CoarseLevel& C, S* __restrict__ out, int64_t os0, int64_t os1,
+                                              int oI0, bool padded) {
+  const PadGeom f(F);
+  const int cn1 = C.n[1], cn2 = C.n[2];
+  for (int c = threadIdx.x; c < cn1 * cn2; c += blockDim.x) {
+    const int I1 = c / cn2, I2 = c - I1 * cn2;
+    for (int I0 = Ia; I0 < Ib; ++I0) {
+      const int kf = f.at(2 * I0 + 1 - z0, 2 * I1 + 1, 2 * I2 + 1);
+      S y[3];
+#pragma unroll
+      for (int d0 = 0; d0 < 3; ++d0) {
+        S z[3];
+#pragma unroll
+        for (int d1 = 0; d1 < 3; ++d1) {
+          const int q = kf + (d0 - 1) * f.sz + (d1 - 1) * f.sy;
+          z[d1] = r2(r[q - 1], r[q], r[q + 1]);
+        }
+        y[d0] = r2(z[0], z[1], z[2]);
+      }
+      const int p = padded ? 1 : 0;
+      out[(int64_t)(I0 - oI0 + p) * os0 + (int64_t)(I1 + p) * os1 + I2 + p] = r2(y[0], y[1], y[2]);
+    }
+  }
+  __syncthreads();
+}
+
+// dst = base - I e on the fine slab's planes (global planes [z0, z0 + F.n[0]));
+// e holds coarse padded planes from global coarse plane c0 - 1 on (a coarse
+// slab buffer, or the whole padded coarse level with c0 = 0)
+template <typename S>
+__device__ __forceinline__ void slab_interp_sub(const CoarseLevel& F, int z0, const S* __restrict__ base,
+                                                S* __restrict__ dst, const CoarseLevel& C, const S* __restrict__ e,
+                                                int c0) {
+  const PadGeom f(F), g(C);
+  for (int c = threadIdx.x; c < f.n1 * f.n2; c += blockDim.x) {
+    const int o1 = c / f.n2, o2 = c - o1 * f.n2;
+    const int t1 = o1 + 1, t2 = o2 + 1;
+    const int e1 = t1 & 1, e2 = t2 & 1;
+    const int qc = (t1 >> 1) * g.sy + (t2 >> 1);
+    int k = f.at(0, o1, o2);
+    for (int l0 = 0; l0 < f.n0; ++l0, k += f.sz) {
+      const int t0 = z0 + l0 + 1;
+      const int q = ((t0 >> 1) - c0) * g.sz + qc;
+      S v = pg_interp_plane(e, g, q, e1, e2);
+      if (t0 & 1) v = i2h(v, pg_interp_plane(e, g, q + g.sz, e1, e2));
+      dst[k] = base[k] - v;
+    }
+  }
+  __syncthreads();
+}
+
+template <typename S>
+__global__ void __launch_bounds__(CG_CLUSTER_THREADS, 2) cluster_vcycle_kernel(const ClusterArgs a) {
+  namespace cg = cooperative_groups;
+  pdl_wait();
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int b = blockIdx.x / CG_NCL;
+  // the mask is read by every CTA of the cluster alike: all return, or none
+  if (a.ca.active && !a.ca.active[b]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sm = reinterpret_cast<S*>(smem_raw);
+  const ClusterTop& t = a.t;
+  const CoarseLevel& T = t.L;
+  const CoarseLevel& U = t.L2;
+  const int n0 = T.n[0], m0 = U.n[0];
+  // top-level slab
+  const int z0 = slab_begin(rank, n0), z1 = slab_begin(rank + 1, n0), np = z1 - z0;
+  const int npm = rank > 0 ? z0 - slab_begin(rank - 1, n0) : 0;
+  CoarseLevel Ls = T;
+  Ls.n[0] = np;
+  const PadGeom gs(Ls);
+  // second-level slab
+  const int y0 = slab2_begin(rank, n0, m0), y1 = slab2_begin(rank + 1, n0, m0), mp = y1 - y0;
+  const int mpm = rank > 0 ? y0 - slab2_begin(rank - 1, n0, m0) : 0;
+  CoarseLevel Us = U;
+  Us.n[0] = mp;
+  const PadGeom gu(Us);
+  S* P[2] = {sm, sm + t.slab_pts};
+  S* rho = sm + 2 * t.slab_pts;
+  S* Q[2] = {sm + 3 * t.slab_pts, sm + 3 * t.slab_pts + t.slab2_pts};
+  S* rho2 = sm + 3 * t.slab_pts + 2 * t.slab2_pts;
+  S* e = rho2 + t.slab2_pts;        // the third level's phi, padded
+  S* csm = e + t.next_pts;          // CTA 0: the coarse kernel's levels
+  for (int i = threadIdx.x; i < 3 * t.slab_pts + 3 * t.slab2_pts + t.next_pts; i += blockDim.x) sm[i] = S(0);
+  __syncthreads();
+  {
+    const S* gr = static_cast<const S*>(t.rho) + (int64_t)b * t.v.sb;
+    const S* gp = static_cast<const S*>(t.phi) + (int64_t)b * t.v.sb;
+    for (int c = threadIdx.x; c < gs.n1 * gs.n2; c += blockDim.x) {
+      const int i1 = c / gs.n2, i2 = c - i1 * gs.n2;
+      int k = gs.at(0, i1, i2);
+      for (int i0 = 0; i0 < np; ++i0, k += gs.sz) {
+        const int64_t gi = (int64_t)(z0 + i0) * t.v.s0 + (int64_t)i1 * t.v.s1 + i2;
+        rho[k] = gr[gi];
+        if (t.first_done) P[0][k] = gp[gi];
+      }
+    }
+  }
+  // ---- top level: pre-sweeps, residual, restriction into the second level's slab
+  int c = 0;
+  slab_exchange(cl, P[0], rank, np, npm, gs.sz);
+  for (int s = t.first_done; s < T.npre; ++s, c = 1 - c) {
+    pg_jacobi(Ls, P[c], P[1 - c], rho, T.w[s]);
+    slab_exchange(cl, P[1 - c], rank, np, npm, gs.sz);
+  }
+  pg_residual(Ls, P[c], P[1 - c], rho);
+  slab_exchange(cl, P[1 - c], rank, np, npm, gs.sz);
+  slab_restrict(Ls, P[1 - c], z0, y0, y1, U, rho2, gu.sz, gu.sy, y0, true);
+  // ---- second level (phi = 0): pre-sweeps, residual, restriction into the third level (global)
+  int d = 0;
+  slab_exchange(cl, Q[0], rank, mp, mpm, gu.sz);  // (zeros: keeps the barrier sequence uniform)
+  for (int s = 0; s < U.npre; ++s, d = 1 - d) {
+    pg_jacobi(Us, Q[d], Q[1 - d], rho2, U.w[s]);
+    slab_exchange(cl, Q[1 - d], rank, mp, mpm, gu.sz);
+  }
+  pg_residual(Us, Q[d], Q[1 - d], rho2);
+  slab_exchange(cl, Q[1 - d], rank, mp, mpm, gu.sz);
+  const CoarseLevel& C = a.ca.lv[0];
+  slab_restrict(Us, Q[1 - d], y0, y0 / 2, min(C.n[0], y1 / 2), C,
+                static_cast<S*>(const_cast<void*>(a.ca.rho)) + (int64_t)b * a.ca.vrho.sb, a.ca.vrho.s0, a.ca.vrho.s1,
+                0, false);
+  __threadfence();
+  cl.sync();
+  if (rank == 0) coarse_vcycle_padded(a.ca, csm, b);
+  __threadfence();
+  cl.sync();
+  {
+    const PadGeom g(C);
+    const S* gp = static_cast<const S*>(a.ca.phi) + (int64_t)b * a.ca.vphi.sb;
+    for (int q = threadIdx.x; q < g.n1 * g.n2; q += blockDim.x) {
+      const int i1 = q / g.n2, i2 = q - i1 * g.n2;
+      int k = g.at(0, i1, i2);
+      for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz)
+        e[k] = __ldcg(gp + (int64_t)i0 * a.ca.vphi.s0 + (int64_t)i1 * a.ca.vphi.s1 + i2);
+    }
+    __syncthreads();
+  }
+  // ---- second level: interpolation, post-sweeps
+  slab_interp_sub(Us, y0, Q[d], Q[1 - d], C, e, 0);
+  d = 1 - d;
+  slab_exchange(cl, Q[d], rank, mp, mpm, gu.sz);
+  for (int s = 0; s < U.npost; ++s, d = 1 - d) {
+    pg_jacobi(Us, Q[d], Q[1 - d], rho2, U.w[U.npre + s]);
+    slab_exchange(cl, Q[1 - d], rank, mp, mpm, gu.sz);
+  }
+  // ---- top level: interpolation from the second level's slab (its halo planes included), post-sweeps
+  slab_interp_sub(Ls, z0, P[c], P[1 - c], Us, Q[d], y0);
+  c = 1 - c;
+  slab_exchange(cl, P[c], rank, np, npm, gs.sz);
+  for (int s = 0; s < T.npost; ++s, c = 1 - c) {
+    pg_jacobi(Ls, P[c], P[1 - c], rho, T.w[T.npre + s]);
+    if (s + 1 < T.npost) slab_exchange(cl, P[1 - c], rank, np, npm, gs.sz);
+  }
+  {
+    S* gp = static_cast<S*>(t.phi) + (int64_t)b * t.v.sb;
+    for (int q = threadIdx.x; q < gs.n1 * gs.n2; q += blockDim.x) {
+      const int i1 = q / gs.n2, i2 = q - i1 * gs.n2;
+      int k = gs.at(0, i1, i2);
+      for (int i0 = 0; i0 < np; ++i0, k += gs.sz)
+        gp[(int64_t)(z0 + i0) * t.v.s0 + (int64_t)i1 * t.v.s1 + i2] = P[c][k];
+    }
+  }
+  cl.sync();  // no CTA leaves while a neighbour may still read its shared memory
 }
 
 }  // namespace gpw

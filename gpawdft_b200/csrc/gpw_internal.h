@@ -158,6 +158,10 @@ inline cudaError_t smem_optin_bytes(F* kernel, size_t bytes) {
 // smem = the levels' buffer bytes.
 struct CoarseArgs;
 cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatch, cudaStream_t st);
+// The level above the coarse kernel's first level in a cluster of CTAs per
+// solve, then the coarse kernel's levels (float32 only; gpw_coarse.cuh).
+struct ClusterArgs;
+cudaError_t launch_cluster_vcycle(const ClusterArgs& a, size_t smem, int nbatch, cudaStream_t st);
 
 // ---------------------------------------------------------------- blas
 cudaError_t launch_axpy(int dtype, int64_t n, double ar, double ai, const void* x, void* y, cudaStream_t st);

@@ -490,6 +490,33 @@ static cudaError_t dispatch_transfer(const TransferArgs& a, int k, bool interp, 
 }
 
 // ------------------------------------------------------------------ coarse levels
+// The cluster V-cycle (float32): CG_NCL CTAs per solve in one cluster.
+cudaError_t launch_cluster_vcycle(const ClusterArgs& a, size_t smem, int nbatch, cudaStream_t st) {
+  if (nbatch < 1 || smem > 227 * 1024) return cudaErrorInvalidValue;
+  static std::once_flag once;
+  static cudaError_t oe = cudaSuccess;
+  std::call_once(once, [] {
+    oe = cudaFuncSetAttribute(cluster_vcycle_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              227 * 1024);
+  });
+  if (oe != cudaSuccess) return oe;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nbatch * CG_NCL);
+  cfg.blockDim = dim3(CG_CLUSTER_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CG_NCL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 2 : 1;
+  return cudaLaunchKernelEx(&cfg, cluster_vcycle_kernel<float>, a);
+}
+
 cudaError_t launch_coarse(int dtype, const CoarseArgs& a, size_t smem, int nbatch, cudaStream_t st) {
   if (a.nl < 1 || a.nl > CG_MAXL || nbatch < 1 || smem > 200 * 1024) return cudaErrorInvalidValue;
   if (dtype == GPW_F64) {

@@ -154,6 +154,13 @@ struct gpw_poisson {
   int lc[2] = {0, 0};
   CoarseArgs cargs[2];
   size_t csmem[2] = {0, 0};
+  // the two levels lc - 1 and lc in a cluster of CTAs per solve, the coarse
+  // kernel's levels from lc + 1 in its CTA 0 (float32 form; lt = -1: none)
+  int lt = -1;
+  ClusterTop ctop;
+  CoarseArgs ccl;          // the coarse kernel's levels from lc + 1
+  size_t ctsmem = 0;
+  bool use_cluster = true;
   Workspace d_err, d_eps, d_niter, d_active, d_any, d_r64, d_gs_old, d_maxiter, d_tdone, d_t0;
   SumScratch sums;
   int* h_any = nullptr;  // pinned
@@ -300,6 +307,28 @@ int rec_lower(Rec& r, int l, const void* res, bool f32) {
       r.tick("L" + std::to_string(l) + " restrict+zero");
     }
   }
+  if (f32 && l + 1 == ps->lt) {
+    // level l+1 and below in one cluster launch: rho_{l+1} (and its first
+    // sweep) in, phi_{l+1} out in buffer 0
+    if (!r.tune) {
+      ClusterArgs ca;
+      ca.ca = ps->ccl;
+      Level& N = ps->lv[ps->lc[1] + 1];
+      ca.ca.rho = N.rho32.ptr;
+      ca.ca.vrho = N.v;
+      ca.ca.phi = N.phi32[0].ptr;
+      ca.ca.vphi = N.v;
+      ca.ca.active = r.active;
+      ca.t = ps->ctop;
+      ca.t.rho = crho.ptr;
+      ca.t.phi = cphi[0].ptr;
+      ca.t.v = C.v;
+      ca.t.first_done = fuse ? 1 : 0;
+      r.ok(launch_cluster_vcycle(ca, ps->ctsmem, r.nb, r.st));
+      r.tick("L" + std::to_string(l + 1) + "+ cluster kernel");
+    }
+    return 0;
+  }
   // the fused first sweep wrote buffer 0 as the result of sweep 1: the
   // V-cycle continues from there (ping-pong parity counts that sweep)
   if (fuse) return rec_vcycle(r, l + 1, 0, f32, true);
@@ -365,6 +394,78 @@ const TrDesc* transformer_desc(const gpw_transformer* tr);
 // 1 float32) and fill its arguments: the deepest suffix of levels (never
 // level 0) that are real 7-point star Laplacians relaxed by Jacobi and whose
 // buffers (two phi + rho per level) fit the shared-memory budget.
+// The float32 levels lc - 1 and lc (the level above the coarse kernel's
+// first level, and that level) in a cluster of CG_NCL CTAs per solve
+// (gpw_coarse.cuh), the coarse kernel's levels from lc + 1 in its CTA 0:
+// zero boundaries (padded form), 7-point Jacobi, every CTA owning planes of
+// both levels, and everything within one CTA's shared memory at two CTAs per
+// SM (so that all of a batch's clusters are resident together).
+static void setup_cluster_top(gpw_poisson* ps, bool padded, size_t es) {
+  ps->lt = -1;
+  const int lc = ps->lc[1], nl = (int)ps->lv.size();
+  if (!ps->use_cluster || !padded || lc < 2 || lc + 1 >= nl || ps->relax_method != 2 || es != 4) return;
+  const CoarseArgs& ca = ps->cargs[1];
+  if (ca.nl < 2) return;
+  const int lt = lc - 1;
+  const Level& L = ps->lv[lt];
+  const OpDesc& d = *L.op;
+  if (!d.real || !d.star_jacobi || d.R != 1) return;
+  if ((int)(L.wpre[1].size() + L.wpost[1].size()) > CG_MAXW || L.wpre[1].empty()) return;
+  const int n0 = L.v.n[0], m0 = ca.lv[0].n[0];
+  int maxp = 0, maxq = 0;
+  for (int r = 0; r < CG_NCL; ++r) {
+    const int z0 = r * n0 / CG_NCL, z1 = (r + 1) * n0 / CG_NCL;
+    const int y0 = std::min(m0, z0 / 2), y1 = (r + 1 == CG_NCL) ? m0 : std::min(m0, z1 / 2);
+    if (z1 - z0 < 1 || y1 - y0 < 1) return;
+    maxp = std::max(maxp, z1 - z0);
+    maxq = std::max(maxq, y1 - y0);
+  }
+  const CoarseLevel& U = ca.lv[0];
+  const CoarseLevel& N = ca.lv[1];
+  const size_t slab = (size_t)(maxp + 2) * (L.v.n[1] + 2) * (L.v.n[2] + 2);
+  const size_t slab2 = (size_t)(maxq + 2) * (U.n[1] + 2) * (U.n[2] + 2);
+  const size_t next = (size_t)(N.n[0] + 2) * (N.n[1] + 2) * (N.n[2] + 2);
+  // the coarse kernel's levels without its first: bases shifted down
+  CoarseArgs cs = ca;
+  cs.nl = ca.nl - 1;
+  for (int k = 0; k < cs.nl; ++k) {
+    cs.lv[k] = ca.lv[k + 1];
+    cs.lv[k].base -= ca.lv[1].base;
+  }
+  const size_t cbytes = ps->csmem[1] - (size_t)ca.lv[1].base * es;
+  const size_t bytes = (3 * slab + 3 * slab2 + next) * es + cbytes;
+  if (bytes > 110 * 1024) return;
+  ClusterTop& t = ps->ctop;
+  t = ClusterTop{};
+  CoarseLevel& c = t.L;
+  for (int a = 0; a < 3; ++a) {
+    c.n[a] = L.v.n[a];
+    c.periodic[a] = 0;
+    c.rpad0[a] = L.restr->pad[a][0];
+    c.ipad0[a] = L.interp->pad[a][0];
+    c.iskip0[a] = L.interp->skip[a][0];
+  }
+  c.pts = (int)slab;
+  c.cc = d.sc.cc;
+  c.cm[0] = d.sc.cx[0];
+  c.cp[0] = d.sc.cx[2];
+  c.cm[1] = d.sc.cy[0];
+  c.cp[1] = d.sc.cy[2];
+  c.cm[2] = d.sc.cz[0];
+  c.cp[2] = d.sc.cz[2];
+  c.npre = (int)L.wpre[1].size();
+  c.npost = (int)L.wpost[1].size();
+  for (int i = 0; i < c.npre; ++i) c.w[i] = L.wpre[1][i];
+  for (int i = 0; i < c.npost; ++i) c.w[c.npre + i] = L.wpost[1][i];
+  t.L2 = U;
+  t.slab_pts = (int)slab;
+  t.slab2_pts = (int)slab2;
+  t.next_pts = (int)next;
+  ps->ccl = cs;
+  ps->ctsmem = bytes;
+  ps->lt = lt;
+}
+
 static void setup_coarse(gpw_poisson* ps, int p) {
   const int nl = (int)ps->lv.size();
   const size_t es = p ? 4 : 8;
@@ -437,6 +538,7 @@ static void setup_coarse(gpw_poisson* ps, int p) {
   }
   ps->lc[p] = lc;
   ps->csmem[p] = bytes;
+  if (p == 1) setup_cluster_top(ps, padded, es);
 }
 
 int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer* const* restrictors,
@@ -1042,6 +1144,27 @@ extern "C" int gpw_poisson_solve_many(int nengines, gpw_poisson* const* engines,
 // its post-sweeps (its pre-sweep weights are skipped).  The float64 method
 // keeps the reference schedule.  Captured graphs of the float32 form are
 // discarded.
+// Drop the captured graphs of the float32 form (its schedule or launch plan changed).
+static void discard_f32_graphs(gpw_poisson* ps) {
+  for (auto it = ps->graphs.begin(); it != ps->graphs.end();) {
+    if (it->first.prec == 1) {
+      cudaGraphExecDestroy(it->second);
+      ps->graph_kernels.erase(it->first);
+      it = ps->graphs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  for (auto it = ps->loops.begin(); it != ps->loops.end();) {
+    if (it->first.prec == 1) {
+      if (it->second) cudaGraphExecDestroy(it->second);
+      it = ps->loops.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
 extern "C" int gpw_poisson_set_inner_schedule(gpw_poisson* ps, const int* npre, const int* npost,
                                               const double* weights, int nweights) {
   if (!ps || !npre || !npost || !weights) return fail(GPW_EINVAL, "null argument");
@@ -1066,15 +1189,18 @@ extern "C" int gpw_poisson_set_inner_schedule(gpw_poisson* ps, const int* npre, 
     k += npost[l];
   }
   setup_coarse(ps, 1);
-  for (auto it = ps->graphs.begin(); it != ps->graphs.end();) {
-    if (it->first.prec == 1) {
-      cudaGraphExecDestroy(it->second);
-      ps->graph_kernels.erase(it->first);
-      it = ps->graphs.erase(it);
-    } else {
-      ++it;
-    }
-  }
+  discard_f32_graphs(ps);
+  return GPW_OK;
+}
+
+// Cluster launch of the level above the coarse kernel's first level (float32
+// form; on by default where it applies): on = 0 runs that level as separate
+// stencil and transfer launches again.  Captured float32 graphs are discarded.
+extern "C" int gpw_poisson_set_cluster(gpw_poisson* ps, int on) {
+  if (!ps) return fail(GPW_EINVAL, "null argument");
+  ps->use_cluster = on != 0;
+  setup_coarse(ps, 1);
+  discard_f32_graphs(ps);
   return GPW_OK;
 }
 

@@ -244,6 +244,14 @@ int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
  * profilers that cannot look inside conditional graph nodes need it).     */
 int gpw_poisson_set_device_loop(gpw_poisson *ps, int on);
 
+/* Launch plan of the float32 form's inner V-cycles (no counterpart in the
+ * reference): on = 1 (default) runs the level above the one-CTA coarse
+ * levels (31^3 at N_c = 128) together with them as one launch of a
+ * thread-block cluster per solve; on = 0 runs that level as separate
+ * stencil and transfer launches.  The two plans sum the stencil terms in a
+ * different order (results within float32 rounding of each other).       */
+int gpw_poisson_set_cluster(gpw_poisson *ps, int on);
+
 /* Programmatic dependent launch of the V-cycle's kernels (no counterpart in
  * the reference): on = 1 (default) lets each stencil / transfer / coarse
  * kernel be dispatched while its predecessor drains (the kernel waits for
