@@ -42,6 +42,8 @@ template <> struct TmaVariant<4> { using T = TmaShape<32, 2, 8, 2, 3, 2>; };  //
 // float32 only: 4 points per thread (16-byte shared-memory reads)
 template <> struct TmaVariant<5> { using T = TmaShape<16, 4, 8, 2, 2, 3>; };  // 64 x 16 tile, 128 threads
 template <> struct TmaVariant<6> { using T = TmaShape<16, 4, 8, 1, 2, 4>; };  // 64 x 8 tile, 128 threads
+template <> struct TmaVariant<7> { using T = TmaShape<16, 4, 8, 2, 3, 3>; };  // 64 x 16 tile, 3 planes ahead
+template <> struct TmaVariant<8> { using T = TmaShape<16, 4, 16, 1, 2, 2>; };  // 64 x 16 tile, 256 threads
 
 // VEC elements of S moved as one vector load / store
 template <typename S, int N> struct VecT;

@@ -39,7 +39,7 @@ namespace gpw {
 enum StencilMode { MODE_APPLY = 0, MODE_RESIDUAL = 1, MODE_JACOBI = 2, MODE_RESID_DC = 3, MODE_JACOBI_ADD64 = 4 };
 
 // Number of tile-shape variants of the TMA star kernel (gpw_star_tma.cuh).
-constexpr int TMA_NVARIANT = 7;  // 5 and 6: float32 only
+constexpr int TMA_NVARIANT = 9;  // 5 - 8: float32 only
 
 constexpr int PMAX = 80;  // GUC n<=6 with 6 directions needs 73
 

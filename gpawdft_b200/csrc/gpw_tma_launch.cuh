@@ -17,7 +17,7 @@ namespace gpw {
 // Every variant is compiled for radius 1 (coarse multigrid levels) and 3
 // (the nn=3 Laplacian of level 0); radius 2 uses variant 2 only and radius 4
 // variant 1 (128 threads: its float64 accumulators do not fit the register
-// share of two 256-thread CTAs per SM).  The 4-point variants (5, 6) are
+// share of two 256-thread CTAs per SM).  The 4-point variants (5 - 8) are
 // float32 only.
 __host__ __device__ constexpr int tma_default_variant(int R) { return R == 4 ? 1 : 2; }
 template <typename S>
@@ -129,6 +129,8 @@ cudaError_t tma_run_variant(int var, const StencilArgs& a, int nbatch, const Sta
       switch (var) {
         case 5: return TmaKernel<S, R, MODE, 5>::run(a, nbatch, sc, nchunk, st);
         case 6: return TmaKernel<S, R, MODE, 6>::run(a, nbatch, sc, nchunk, st);
+        case 7: return TmaKernel<S, R, MODE, 7>::run(a, nbatch, sc, nchunk, st);
+        case 8: return TmaKernel<S, R, MODE, 8>::run(a, nbatch, sc, nchunk, st);
       }
     }
     return cudaErrorInvalidValue;

@@ -265,8 +265,8 @@ int gpw_set_pdl(int on);
  * element type and radius have that variant uses it, with `nchunk` axis-0
  * chunks (0 = the wave model, < 0 = the model's count times -nchunk);
  * variant -1 returns to the autotuned choice.  Variants 0-4 exist for both
- * element types, 5-6 (4 points per thread) for float32 only.  Process-wide;
- * meant for tests and tuning studies.  GPW_EINVAL outside [-1, 6].        */
+ * element types, 5-8 (4 points per thread) for float32 only.  Process-wide;
+ * meant for tests and tuning studies.  GPW_EINVAL outside [-1, 8].        */
 int gpw_set_tma_variant(int variant, int nchunk);
 
 /* Pins the tile layout of the star-stencil kernel that serves applies on
