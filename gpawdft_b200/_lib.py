@@ -32,6 +32,7 @@ EXPORTS = [
     'gpw_poisson_time_level0', 'gpw_poisson_set_inner_schedule',
     'gpw_set_tma_variant', 'gpw_set_bloch_layout', 'gpw_bloch_launch_count',
     'gpw_poisson_set_device_loop', 'gpw_set_pdl', 'gpw_poisson_set_cluster',
+    'gpw_poisson_set_fusion',
     'gpw_poisson_solve_many', 'gpw_poisson_last_latency',
     'gpw_poisson_profile_iteration', 'gpw_poisson_free',
     'gpw_nn_conv3', 'gpw_nn_wgrad_scratch', 'gpw_nn_conv3_wgrad',
@@ -94,6 +95,7 @@ _SIGS = {
     'gpw_poisson_set_device_loop': (ctypes.c_int, [_vp, ctypes.c_int]),
     'gpw_set_pdl': (ctypes.c_int, [ctypes.c_int]),
     'gpw_poisson_set_cluster': (ctypes.c_int, [_vp, ctypes.c_int]),
+    'gpw_poisson_set_fusion': (ctypes.c_int, [_vp, ctypes.c_int]),
     'gpw_bloch_launch_count': (ctypes.c_int64, []),
     'gpw_poisson_time_level0': (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int,
                                                ctypes.c_int, _vp, _vp, _vp]),

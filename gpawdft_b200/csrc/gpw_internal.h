@@ -224,6 +224,15 @@ inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
   return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// The float32 level-0 residual restricted (K = 2, zero boundaries) into the
+// next level's rho and first Jacobi iterate in one TMA launch
+// (MODE_RESID_RESTRICT); `tune` times its tile variants instead.
+bool resid_restrict_ok(const OpDesc& d, const void* in, const void* rho, const GridView& v, const void* out,
+                       const void* out2, const GridView& vco, int nbatch);
+cudaError_t launch_resid_restrict(const OpDesc& d, const void* in, const void* rho, const GridView& v, void* out,
+                                  void* out2, const GridView& vco, int nbatch, double w2, double c02,
+                                  const unsigned char* active, bool tune, cudaStream_t st);
+
 // Periodic / Bloch (or mixed-boundary) star applies on the TMA row kernel
 // (gpw_bloch.cu): eligibility and launch.
 bool bloch_path_ok(const OpDesc& d, int dtype, const void* in, const GridView& vin, const void* out,

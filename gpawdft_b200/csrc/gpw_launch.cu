@@ -367,6 +367,39 @@ cudaError_t launch_stencil_dc(const OpDesc& d, int mode, const void* in, const G
   return tma_launch(dtype, mode, d.R, ch, a, nbatch, d.sc, st);
 }
 
+static cudaError_t tune_stencil_args(const OpDesc& d, int ldtype, int mode, const StencilArgs& a, int nbatch,
+                                     cudaStream_t st);
+
+bool resid_restrict_ok(const OpDesc& d, const void* in, const void* rho, const GridView& v, const void* out,
+                       const void* out2, const GridView& vco, int nbatch) {
+  if (!dc_fusable(d) || d.R != 3 || !tensor_map_encoder()) return false;
+  if (!aligned16(in) || !aligned16(rho) || !aligned16(out) || !aligned16(out2)) return false;
+  if (!view_tma_ok(v, 4, nbatch)) return false;
+  for (int c = 0; c < 3; ++c)
+    if (v.n[c] != 2 * vco.n[c] + 1) return false;  // zero boundaries, fine centre 2I + 1
+  return true;
+}
+
+cudaError_t launch_resid_restrict(const OpDesc& d, const void* in, const void* rho, const GridView& v, void* out,
+                                  void* out2, const GridView& vco, int nbatch, double w2, double c02,
+                                  const unsigned char* active, bool tune, cudaStream_t st) {
+  if (!resid_restrict_ok(d, in, rho, v, out, out2, vco, nbatch)) return cudaErrorNotSupported;
+  StencilArgs a{};
+  a.in = in;
+  a.out = out;
+  a.out2 = out2;
+  a.rho = rho;
+  a.vin = a.vout = a.vrho = v;
+  a.vco = vco;
+  a.w = 1.0;
+  a.w2 = w2;
+  a.c0 = c02;  // the next level's diagonal: the first coarse sweep's w2 / c0
+  a.active = active;
+  if (tune) return tune_stencil_args(d, GPW_F32, MODE_RESID_RESTRICT, a, nbatch, st);
+  const TmaChoice ch = tma_choice(GPW_F32, d.R, MODE_RESID_RESTRICT, v, nbatch);
+  return tma_launch(GPW_F32, MODE_RESID_RESTRICT, d.R, ch, a, nbatch, d.sc, st);
+}
+
 cudaError_t tune_stencil(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, void* out,
                          const GridView& vout, const void* rho, const GridView& vrho, void* out2, int nbatch,
                          double w, const GridSum& gs, cudaStream_t st) {
@@ -393,6 +426,13 @@ cudaError_t tune_stencil(const OpDesc& d, int dtype, int mode, const void* in, c
   } else if (!tma_path_ok(d, dtype, mode, in, vin, out, vout, rho, vrho, nbatch)) {
     return cudaSuccess;  // not the TMA path: nothing to tune
   }
+  return tune_stencil_args(d, ldtype, mode, a, nbatch, st);
+}
+
+// The tuning loop proper, on prepared arguments (element type ldtype).
+static cudaError_t tune_stencil_args(const OpDesc& d, int ldtype, int mode, const StencilArgs& a, int nbatch,
+                                     cudaStream_t st) {
+  const GridView& vout = a.vout;
   const TuneKey key{ldtype, d.R, mode, vout.n[0], vout.n[1], vout.n[2], nbatch};
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);

@@ -161,6 +161,7 @@ struct gpw_poisson {
   CoarseArgs ccl;          // the coarse kernel's levels from lc + 1
   size_t ctsmem = 0;
   bool use_cluster = true;
+  bool use_rr = true;  // float32 form: level-0 residual restricted in the same launch
   Workspace d_err, d_eps, d_niter, d_active, d_any, d_r64, d_gs_old, d_maxiter, d_tdone, d_t0;
   SumScratch sums;
   int* h_any = nullptr;  // pinned
@@ -760,9 +761,25 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStrea
     const std::vector<double>& wpre = L0.wpre[1];
     const std::vector<double>& wpost = L0.wpost[1];
     int cur = rec_relax(r, 0, 0, wpre.data() + 1, (int)wpre.size() - 1, true);
-    r.stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[cur].ptr, L0.res32.ptr, L0.rho32.ptr, L0.v, 1.0, GridSum{});
-    r.tick("L0 f32 residual");
-    const int ccur = rec_lower(r, 0, L0.res32.ptr, true);
+    int ccur;
+    const int nl = (int)ps->lv.size();
+    const bool rr = ps->use_rr && nl > 2 && ps->lc[1] > 1 && ps->lt != 1 && L0.restr->k == 2 &&
+                    L0.restr->pad[0][0] == 0 && L0.restr->pad[1][0] == 0 && L0.restr->pad[2][0] == 0 &&
+                    !C.wpre[1].empty() && !C.op->coefs.empty() &&
+                    resid_restrict_ok(*L0.op, L0.phi32[cur].ptr, L0.rho32.ptr, L0.v, C.rho32.ptr, C.phi32[0].ptr,
+                                      C.v, nb);
+    if (rr) {
+      // the residual restricted straight into level 1's rho and first sweep
+      r.ok(launch_resid_restrict(*L0.op, L0.phi32[cur].ptr, L0.rho32.ptr, L0.v, C.rho32.ptr, C.phi32[0].ptr, C.v,
+                                 nb, C.wpre[1][0], C.op->coefs[0], r.active, tune, st));
+      r.tick("L0 f32 residual + restriction");
+      ccur = rec_vcycle(r, 1, 0, true, true);
+    } else {
+      r.stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[cur].ptr, L0.res32.ptr, L0.rho32.ptr, L0.v, 1.0,
+                GridSum{});
+      r.tick("L0 f32 residual");
+      ccur = rec_lower(r, 0, L0.res32.ptr, true);
+    }
     Boundary cbc = make_boundary(C.op->periodic, GPW_F32, nullptr);
     if (!tune) {
       r.ok(launch_transfer(*L0.interp, GPW_F32, C.phi32[ccur].ptr, C.v, L0.phi32[1 - cur].ptr, L0.v, nb, cbc, 1,
@@ -1189,6 +1206,16 @@ extern "C" int gpw_poisson_set_inner_schedule(gpw_poisson* ps, const int* npre, 
     k += npost[l];
   }
   setup_coarse(ps, 1);
+  discard_f32_graphs(ps);
+  return GPW_OK;
+}
+
+// Level-0 residual and restriction in one launch (float32 form; on by
+// default where it applies): on = 0 launches them separately.  Both plans
+// compute the same values.  Captured float32 graphs are discarded.
+extern "C" int gpw_poisson_set_fusion(gpw_poisson* ps, int on) {
+  if (!ps) return fail(GPW_EINVAL, "null argument");
+  ps->use_rr = on != 0;
   discard_f32_graphs(ps);
   return GPW_OK;
 }

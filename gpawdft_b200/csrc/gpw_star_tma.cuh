@@ -21,6 +21,7 @@
 #include "gpw_common.cuh"
 #include "gpw_reduce.cuh"
 #include "gpw_stencil.cuh"
+#include "gpw_transfer.cuh"
 
 namespace gpw {
 
@@ -44,6 +45,9 @@ template <> struct TmaVariant<5> { using T = TmaShape<16, 4, 8, 2, 2, 3>; };  //
 template <> struct TmaVariant<6> { using T = TmaShape<16, 4, 8, 1, 2, 4>; };  // 64 x 8 tile, 128 threads
 template <> struct TmaVariant<7> { using T = TmaShape<16, 4, 8, 2, 3, 3>; };  // 64 x 16 tile, 3 planes ahead
 template <> struct TmaVariant<8> { using T = TmaShape<16, 4, 16, 1, 2, 2>; };  // 64 x 16 tile, 256 threads
+// 68 x 16 tile: with the residual restricted in-kernel, 32 coarse columns a
+// tile at a 64-column stride
+template <> struct TmaVariant<9> { using T = TmaShape<17, 4, 8, 2, 2, 3>; };
 
 // VEC elements of S moved as one vector load / store
 template <typename S, int N> struct VecT;
@@ -124,7 +128,13 @@ struct TmaCfg {
   static constexpr int RHO_OFF = tma_align128(IN_BYTES);
   static constexpr int AUX_OFF = RHO_OFF + tma_align128(RHO_BYTES);
   static constexpr int NR = 2 * R + 1;
-  static constexpr size_t smem = (size_t)NS * STAGE_BYTES + (size_t)NS * 8 + 128;
+  // RESID_RESTRICT: the residual plane of the tile, and the coarse points a
+  // tile restricts (centres 2I + 1 in the tile's first TZ - 4 columns and
+  // TY - 2 rows; tiles advance by those and overlap by the rest)
+  static constexpr bool RR = MODE == MODE_RESID_RESTRICT;
+  static constexpr int CX = (TZ - 4) / 2, CY = (TY - 2) / 2;
+  static constexpr int RT_BYTES = RR ? TY * TZ * (int)sizeof(S) : 0;
+  static constexpr size_t smem = (size_t)NS * STAGE_BYTES + (size_t)NS * 8 + (size_t)RT_BYTES + 128;
 };
 
 // Coefficients and relaxation weights in the kernel's element type, rounded
@@ -203,18 +213,28 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
   // 128-byte aligned ring of stages (TMA destinations), then the mbarriers;
   // the launch reserves 128 bytes for the alignment shift
   unsigned char* ring = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + NS * C::STAGE_BYTES);
+  S* rtile = reinterpret_cast<S*>(ring + NS * C::STAGE_BYTES);  // RESID_RESTRICT (128-byte aligned)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + NS * C::STAGE_BYTES + C::RT_BYTES);
   __shared__ double red[32];
   const StencilArgs& a = ta.s;
   pdl_wait();  // the predecessor's results (and the active mask) are visible from here
 
   const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
   if (a.active && !a.active[b]) return;
-  const int x0 = blockIdx.x * C::TZ, y0 = blockIdx.y * C::TY;
+  const int x0 = blockIdx.x * (C::RR ? 2 * C::CX : C::TZ), y0 = blockIdx.y * (C::RR ? 2 * C::CY : C::TY);
   const int n0 = a.vout.n[0];
-  // balanced chunks of axis 0 (lengths differ by at most one plane)
-  const int z0 = (int)((int64_t)chunk * n0 / a.nchunk);
-  const int z1 = (int)((int64_t)(chunk + 1) * n0 / a.nchunk);
+  // balanced chunks of axis 0 (lengths differ by at most one plane); for
+  // RESID_RESTRICT chunks of coarse planes [C0, C1), i.e. fine planes
+  // 2 C0 .. 2 C1 (consecutive chunks share one fine plane)
+  int z0, z1;
+  if constexpr (C::RR) {
+    const int nc0 = a.vco.n[0];
+    z0 = 2 * (int)((int64_t)chunk * nc0 / a.nchunk);
+    z1 = min(n0, 2 * (int)((int64_t)(chunk + 1) * nc0 / a.nchunk) + 1);
+  } else {
+    z0 = (int)((int64_t)chunk * n0 / a.nchunk);
+    z1 = (int)((int64_t)(chunk + 1) * n0 / a.nchunk);
+  }
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + C::NTX * ty;
   const int xl = XL + VEC * tx;       // local column of this thread's first point
@@ -257,6 +277,12 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
       for (int m = 0; m < NR; ++m)
 #pragma unroll
         for (int e = 0; e < VEC; ++e) acc[j][m].v[e] = S(0);
+    // RESID_RESTRICT: this thread's coarse points of the tile (tid + u NT)
+    // and the in-plane restricted values of their last two fine planes
+    constexpr int RK = C::RR ? (C::CX * C::CY + C::NT - 1) / C::NT : 1;
+    S rq0[RK], rq1[RK];
+#pragma unroll
+    for (int u = 0; u < RK; ++u) rq0[u] = rq1[u] = S(0);
 
     for (int sb = 0; sb < nsteps; sb += NR) {
 #pragma unroll
@@ -334,6 +360,9 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
                   (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
               if constexpr (MODE == MODE_APPLY) {
                 res = av;
+              } else if constexpr (C::RR) {
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) res.v[e] = av.v[e] - rho.v[e];
               } else if constexpr (MODE == MODE_RESIDUAL || MODE == MODE_RESID_DC) {
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) res.v[e] = av.v[e] - rho.v[e];
@@ -385,12 +414,46 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
                   else
                     stv_part<double, 2>(pp + h, pv, nx - h);
                 }
+              } else if constexpr (C::RR) {
+                stv<S, VEC>(rtile + (yb + j) * C::TZ + VEC * tx, res);
               } else if (MODE != MODE_RESIDUAL || a.out) {
                 S* op = static_cast<S*>(a.out) + oidx;
                 if (nx == VEC)
                   stv<S, VEC>(op, res);
                 else
                   stv_part<S, VEC>(op, res, nx);
+              }
+            }
+          }
+          if constexpr (C::RR) {
+            // restriction of the residual plane o (c/bmgs/restrict.c: axis 2,
+            // then axis 1, then axis 0 over fine planes 2 I0, 2 I0 + 1, 2 I0 + 2)
+            __syncthreads();  // the tile's residual plane is complete in rtile
+#pragma unroll
+            for (int u = 0; u < RK; ++u) {
+              const int t = tid + u * C::NT;
+              const int rci1 = t / C::CX, rci2 = t - (t / C::CX) * C::CX;
+              const int rI1 = blockIdx.y * C::CY + rci1, rI2 = blockIdx.x * C::CX + rci2;
+              if (t < C::CX * C::CY && rI1 < a.vco.n[1] && rI2 < a.vco.n[2]) {
+                const S* rr = rtile + (2 * rci1) * C::TZ + 2 * rci2;
+                S zr[3];
+#pragma unroll
+                for (int d1 = 0; d1 < 3; ++d1)
+                  zr[d1] = r2(rr[d1 * C::TZ], rr[d1 * C::TZ + 1], rr[d1 * C::TZ + 2]);
+                const S yv = r2(zr[0], zr[1], zr[2]);
+                const int ol = o - z0;  // z0 is even
+                if ((ol & 1) == 0) {
+                  if (ol >= 2) {
+                    const S v = r2(rq0[u], rq1[u], yv);
+                    const int64_t ci = (int64_t)b * a.vco.sb + (int64_t)((o - 2) / 2) * a.vco.s0 +
+                                       (int64_t)rI1 * a.vco.s1 + rI2;
+                    static_cast<S*>(a.out)[ci] = v;
+                    static_cast<S*>(a.out2)[ci] = (S)k.wc2 * v;
+                  }
+                  rq0[u] = yv;
+                } else {
+                  rq1[u] = yv;
+                }
               }
             }
           }

@@ -35,11 +35,22 @@ namespace gpw {
 // and writes the float32 defect rhs = -(A phi - rho) to `out` and the first
 // inner Jacobi iterate from zero, (w2 / c0) rhs, to `out2`, plus sum r^2;
 // JACOBI_ADD64 is a float32 Jacobi sweep whose result is added to the float64
-// array `out2` (phi += e) instead of being stored.
-enum StencilMode { MODE_APPLY = 0, MODE_RESIDUAL = 1, MODE_JACOBI = 2, MODE_RESID_DC = 3, MODE_JACOBI_ADD64 = 4 };
+// array `out2` (phi += e) instead of being stored.  RESID_RESTRICT is a
+// float32 residual that is not stored but restricted (K = 2, zero
+// boundaries) into the next level: rho_c to `out` and that level's first
+// Jacobi iterate from zero, (w2 / c0) rho_c with c0 the next level's
+// diagonal, to `out2`, both in the coarse view `vco`.
+enum StencilMode {
+  MODE_APPLY = 0,
+  MODE_RESIDUAL = 1,
+  MODE_JACOBI = 2,
+  MODE_RESID_DC = 3,
+  MODE_JACOBI_ADD64 = 4,
+  MODE_RESID_RESTRICT = 5
+};
 
 // Number of tile-shape variants of the TMA star kernel (gpw_star_tma.cuh).
-constexpr int TMA_NVARIANT = 9;  // 5 - 8: float32 only
+constexpr int TMA_NVARIANT = 10;  // 5 - 9: float32 only
 
 constexpr int PMAX = 80;  // GUC n<=6 with 6 directions needs 73
 
@@ -58,6 +69,7 @@ struct StencilArgs {
   int nblk_seg;     // CTAs per batch member
   void* out2;       // RESID_DC: first inner iterate (float); JACOBI_ADD64: float64 phi
   double w2;        // RESID_DC: Jacobi weight of that first inner sweep
+  GridView vco;     // RESID_RESTRICT: the next level's view (out, out2)
 };
 
 struct GeneralCoefs {

@@ -1,5 +1,6 @@
-// TMA star-stencil launches for float32 grids (apply, residual, Jacobi and
-// the Jacobi sweep that adds its result into float64 phi).
+// TMA star-stencil launches for float32 grids (apply, residual, Jacobi, the
+// Jacobi sweep that adds its result into float64 phi, and the residual
+// restricted into the next level).
 #include "gpw_tma_launch.cuh"
 
 namespace gpw {
@@ -11,6 +12,9 @@ cudaError_t tma_stencil_f32(int mode, int R, int var, const StencilArgs& a, int 
     case MODE_RESIDUAL: return tma_run_radius<float, MODE_RESIDUAL>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_JACOBI: return tma_run_radius<float, MODE_JACOBI>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_JACOBI_ADD64: return tma_run_radius<float, MODE_JACOBI_ADD64>(R, var, a, nbatch, sc, nchunk, st);
+    case MODE_RESID_RESTRICT:  // the float32 form's level 0 (nn = 3) only
+      if (R == 3) return tma_run_variant<float, 3, MODE_RESID_RESTRICT>(var, a, nbatch, sc, nchunk, st);
+      return cudaErrorInvalidValue;
   }
   return cudaErrorInvalidValue;
 }

@@ -17,7 +17,7 @@ namespace gpw {
 // Every variant is compiled for radius 1 (coarse multigrid levels) and 3
 // (the nn=3 Laplacian of level 0); radius 2 uses variant 2 only and radius 4
 // variant 1 (128 threads: its float64 accumulators do not fit the register
-// share of two 256-thread CTAs per SM).  The 4-point variants (5 - 8) are
+// share of two 256-thread CTAs per SM).  The 4-point variants (5 - 9) are
 // float32 only.
 __host__ __device__ constexpr int tma_default_variant(int R) { return R == 4 ? 1 : 2; }
 template <typename S>
@@ -98,10 +98,15 @@ struct TmaKernel {
       return cudaErrorInvalidValue;
     const GridView& v = a.vout;
     dim3 grid((v.n[2] + C::TZ - 1) / C::TZ, (v.n[1] + C::TY - 1) / C::TY, 1);
+    if (C::RR) {  // tiles of CX x CY coarse points
+      if (C::CY < 1) return cudaErrorInvalidValue;
+      grid = dim3((a.vco.n[2] + C::CX - 1) / C::CX, (a.vco.n[1] + C::CY - 1) / C::CY, 1);
+    }
     const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
     int nc = nchunk > 0 ? nchunk
                         : tma_model_chunks(v.n[0], tiles, R, (int64_t)spm * num_sms()) * std::max(1, -nchunk);
     nc = std::max(1, std::min(nc, tma_max_chunks(v.n[0], R)));
+    if (C::RR) nc = std::max(1, std::min(nc, a.vco.n[0] / 2));  // chunks of at least two coarse planes
     a.nchunk = nc;
     a.zchunk = (v.n[0] + nc - 1) / nc;
     grid.z = nc * nbatch;
@@ -131,6 +136,7 @@ cudaError_t tma_run_variant(int var, const StencilArgs& a, int nbatch, const Sta
         case 6: return TmaKernel<S, R, MODE, 6>::run(a, nbatch, sc, nchunk, st);
         case 7: return TmaKernel<S, R, MODE, 7>::run(a, nbatch, sc, nchunk, st);
         case 8: return TmaKernel<S, R, MODE, 8>::run(a, nbatch, sc, nchunk, st);
+        case 9: return TmaKernel<S, R, MODE, 9>::run(a, nbatch, sc, nchunk, st);
       }
     }
     return cudaErrorInvalidValue;

@@ -129,6 +129,17 @@ __device__ __forceinline__ float2 rmul(float c, float2 a) {
   return make_float2(__fmul_rn(c, a.x), __fmul_rn(c, a.y));
 }
 
+// K = 2 rules: 0.5 * (a0 + 0.5 * (a1 + a_1))   (c/bmgs/restrict.c:38-39)
+template <typename S>
+__device__ __forceinline__ S r2(S am, S a0, S ap) {
+  return rmul(S(0.5), radd(a0, rmul(S(0.5), radd(ap, am))));
+}
+// 0.5 * (a0 + a1)                 (c/bmgs/interpolate.c:33)
+template <typename S>
+__device__ __forceinline__ S i2h(S a0, S a1) {
+  return rmul(S(0.5), radd(a0, a1));
+}
+
 template <int K> struct TW;
 template <> struct TW<2> { static __device__ __forceinline__ double w(int) { return 0.5; } };
 template <> struct TW<4> {

@@ -25,17 +25,6 @@ namespace gpw {
 
 constexpr int K2_TX = 32, K2_TY = 8;
 
-// 0.5 * (a0 + 0.5 * (a1 + a_1))   (c/bmgs/restrict.c:38-39)
-template <typename S>
-__device__ __forceinline__ S r2(S am, S a0, S ap) {
-  return rmul(S(0.5), radd(a0, rmul(S(0.5), radd(ap, am))));
-}
-// 0.5 * (a0 + a1)                 (c/bmgs/interpolate.c:33)
-template <typename S>
-__device__ __forceinline__ S i2h(S a0, S a1) {
-  return rmul(S(0.5), radd(a0, a1));
-}
-
 // Resolve index i along an axis: element offset (times stride) and a
 // validity flag (false: zero-boundary halo, value 0).
 __device__ __forceinline__ bool k2_axis(int i, int n, int periodic, int64_t stride, int64_t& off) {

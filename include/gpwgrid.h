@@ -252,6 +252,13 @@ int gpw_poisson_set_device_loop(gpw_poisson *ps, int on);
  * different order (results within float32 rounding of each other).       */
 int gpw_poisson_set_cluster(gpw_poisson *ps, int on);
 
+/* Level-0 launch plan of the float32 form (no counterpart in the
+ * reference): on = 1 (default) computes the level-0 residual and restricts
+ * it into level 1 (its rho and first Jacobi sweep) in one launch, without
+ * storing the residual; on = 0 launches the residual and the restriction
+ * separately.  The two plans compute identical values.                    */
+int gpw_poisson_set_fusion(gpw_poisson *ps, int on);
+
 /* Programmatic dependent launch of the V-cycle's kernels (no counterpart in
  * the reference): on = 1 (default) lets each stencil / transfer / coarse
  * kernel be dispatched while its predecessor drains (the kernel waits for
@@ -265,8 +272,8 @@ int gpw_set_pdl(int on);
  * element type and radius have that variant uses it, with `nchunk` axis-0
  * chunks (0 = the wave model, < 0 = the model's count times -nchunk);
  * variant -1 returns to the autotuned choice.  Variants 0-4 exist for both
- * element types, 5-8 (4 points per thread) for float32 only.  Process-wide;
- * meant for tests and tuning studies.  GPW_EINVAL outside [-1, 8].        */
+ * element types, 5-9 (4 points per thread) for float32 only.  Process-wide;
+ * meant for tests and tuning studies.  GPW_EINVAL outside [-1, 9].        */
 int gpw_set_tma_variant(int variant, int nchunk);
 
 /* Pins the tile layout of the star-stencil kernel that serves applies on

@@ -270,6 +270,36 @@ def test_pdl_off_equals_on(cuda, precision):
 
 
 @pytest.mark.parametrize('N', [64, 128, 192])
+def test_fused_residual_restriction(cuda, N):
+    """The float32 form's level-0 residual restricted in the same launch
+    (no residual stored) and in two launches: identical iteration counts and
+    bit-identical potentials (the same values in the same order)."""
+    from gpawdft_b200 import _lib
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    lib = _lib.load()
+    rhos = []
+    for s in range(2):
+        rho, L = gaussian_density(N, 0.2, 8, 140 + s)
+        rhos.append(rho)
+    rhos = np.array(rhos)
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    eps = [1e-20 * float(np.dot(r.ravel(), r.ravel())) * gd.dv for r in rhos]
+    out = []
+    for on in (1, 0):
+        ps = PoissonSolver(nn=3, batch=2, precision='fp32', maxiter=100)
+        ps.set_grid_descriptor(gd)
+        ps.initialize()
+        _lib.check(lib.gpw_poisson_set_fusion(ps._engine[0], on))
+        phi = np.zeros_like(rhos)
+        n = ps.solve_batch(phi, rhos, eps=eps)
+        assert (ps.last_errors <= eps).all()
+        out.append((phi, n))
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][0], out[1][0])
+
+
+@pytest.mark.parametrize('N', [64, 128, 192])
 def test_cluster_level_plan(cuda, N):
     """The float32 form with the two levels above the one-CTA coarse levels
     in one cluster launch (31^3 and 15^3 at N_c = 64 and 128, 23^3 and 11^3
