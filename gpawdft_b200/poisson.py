@@ -45,7 +45,7 @@ def create_poisson_solver(name='fd', **kwargs):
 
 def PoissonSolver(dipolelayer=None, **kwargs):
     if dipolelayer is not None:
-        raise NotImplementedError('DipoleCorrection is not part of this build')
+        raise NotImplementedError('DipoleCorrection is not implemented by this package')
     return FDPoissonSolver(**kwargs)
 
 

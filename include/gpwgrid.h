@@ -41,7 +41,7 @@ extern "C" {
 #define GPW_OK 0
 #define GPW_ENOMEM 12     /* device allocation failed */
 #define GPW_EINVAL 22     /* bad shape / dtype / argument */
-#define GPW_ENOTSUP 95    /* valid request this build does not implement */
+#define GPW_ENOTSUP 95    /* valid request the library does not implement */
 #define GPW_ETIMEDOUT 110 /* a bounded device-side wait gave up */
 #define GPW_ECONV 1001    /* Poisson V-cycles reached maxiter (PoissonConvergenceError) */
 #define GPW_ECUDA 1002    /* a CUDA runtime call failed */
