@@ -102,6 +102,23 @@ def test_null_and_dtype_checks():
                                  None) == _lib.GPW_EINVAL
 
 
+def test_launch_plan_switches_validate():
+    """The tuning / launch-plan switches check their arguments on the host:
+    TMA variant range, Bloch layout index, and a null engine."""
+    lib = _lib.load()
+    assert lib.gpw_set_tma_variant(-2, 0) == _lib.GPW_EINVAL
+    assert lib.gpw_set_tma_variant(10, 0) == _lib.GPW_EINVAL
+    assert lib.gpw_set_tma_variant(-1, 0) == _lib.GPW_OK   # back to the tuned choice
+    assert lib.gpw_set_bloch_layout(-1) == _lib.GPW_EINVAL
+    assert lib.gpw_set_bloch_layout(17) == _lib.GPW_EINVAL
+    assert lib.gpw_set_bloch_layout(0) == _lib.GPW_OK
+    assert lib.gpw_set_pdl(1) == _lib.GPW_OK
+    for f in (lib.gpw_poisson_set_device_loop, lib.gpw_poisson_set_cluster,
+              lib.gpw_poisson_set_fusion):
+        assert f(None, 1) == _lib.GPW_EINVAL
+    assert lib.gpw_bloch_launch_count() >= 0
+
+
 def test_product_fails_loudly_without_cuda():
     torch = pytest.importorskip('torch')
     if torch.cuda.is_available():
