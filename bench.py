@@ -342,17 +342,29 @@ def run_ours(args, rank, world, dist):
              2: 'star_tma_kernel<float,3,JACOBI> level-0 sweep',
              3: 'star_tma_kernel<float,3,JACOBI_ADD64> level-0 sweep + phi64 update',
              4: 'star_tma_kernel<double,3,RESID_DC> level-0 fp64 defect',
-             5: 'star_tma_kernel<float,3,RESIDUAL> level-0 residual'}
+             5: 'star_tma_kernel<float,3,RESIDUAL> level-0 residual',
+             6: 'star_tma_kernel<float,3,RESID_RESTRICT> level-0 residual '
+                '+ restriction into level 1'}
     # launches of each per outer iteration: float64 method 3 sweeps + 2
     # residuals; float32 form (2 + 2 Chebyshev sweeps on level 0) 2 plain
     # sweeps, 1 residual, 1 defect, 1 update
+    # (the float32 form's level-0 residual is restricted in the same launch
+    # where the grid allows it: which 6, else the plain residual, which 5)
     per_iter = ({0: 3, 1: 2} if args.precision == 'fp64' else
-                {2: 2, 5: 1, 4: 1, 3: 1})
-    for which in per_iter:
+                {2: 2, 6: 1, 4: 1, 3: 1})
+    for which in list(per_iter):
         ms, nbytes = ctypes.c_double(), ctypes.c_double()
-        _lib.check(lib.gpw_poisson_time_level0(
+        rc = lib.gpw_poisson_time_level0(
             ps._engine[0], B, which, 20, ctypes.byref(ms), ctypes.byref(nbytes),
-            stream.cuda_stream))
+            stream.cuda_stream)
+        if rc == _lib.GPW_ENOTSUP and which == 6:
+            del per_iter[6]
+            per_iter[5] = 1
+            which = 5
+            rc = lib.gpw_poisson_time_level0(
+                ps._engine[0], B, which, 20, ctypes.byref(ms),
+                ctypes.byref(nbytes), stream.cuda_stream)
+        _lib.check(rc)
         kernels[which] = (ms.value / 1e3, nbytes.value)
     # the dominant kernel: the largest time per outer iteration
     dom = max(per_iter, key=lambda w: kernels[w][0] * per_iter[w])

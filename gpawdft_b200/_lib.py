@@ -29,6 +29,7 @@ EXPORTS = [
     'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
     'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_add_scalar',
     'gpw_poisson_new', 'gpw_poisson_solve', 'gpw_poisson_last_stats',
+    'gpw_poisson_solve_async', 'gpw_poisson_collect',
     'gpw_poisson_time_level0', 'gpw_poisson_set_inner_schedule',
     'gpw_set_tma_variant', 'gpw_set_bloch_layout', 'gpw_bloch_launch_count',
     'gpw_poisson_set_device_loop', 'gpw_set_pdl', 'gpw_poisson_set_cluster',
@@ -90,6 +91,11 @@ _SIGS = {
                                          ctypes.c_int, ctypes.c_int, _vp, _vp,
                                          _vp]),
     'gpw_poisson_last_stats': (ctypes.c_int, [_vp, _vp, _vp]),
+    'gpw_poisson_solve_async': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int64, _vp,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               _vp]),
+    'gpw_poisson_collect': (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, _vp, _vp]),
     'gpw_set_tma_variant': (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     'gpw_set_bloch_layout': (ctypes.c_int, [ctypes.c_int]),
     'gpw_poisson_set_device_loop': (ctypes.c_int, [_vp, ctypes.c_int]),

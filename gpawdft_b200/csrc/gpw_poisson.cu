@@ -166,13 +166,15 @@ struct gpw_poisson {
   SumScratch sums;
   int* h_any = nullptr;  // pinned
   // mapped pinned mailbox: eps in, niter / error out (nbmax each)
+  // two slots, so an asynchronous solve can be enqueued while the previous
+  // one's results are still to be collected
   void* h_io = nullptr;
-  double* h_eps = nullptr;
-  double* h_err = nullptr;
-  int* h_niter = nullptr;
-  double* m_eps = nullptr;  // the same three, as device pointers
-  double* m_err = nullptr;
-  int* m_niter = nullptr;
+  double* h_eps[2] = {nullptr, nullptr};
+  double* h_err[2] = {nullptr, nullptr};
+  int* h_niter[2] = {nullptr, nullptr};
+  double* m_eps[2] = {nullptr, nullptr};  // the same, as device pointers
+  double* m_err[2] = {nullptr, nullptr};
+  int* m_niter[2] = {nullptr, nullptr};
   struct GraphKey {
     int64_t nb;
     int prec;
@@ -613,17 +615,20 @@ int gpw_poisson_new(int nlevels, gpw_operator* const* operators, gpw_transformer
   if (!device_status_word()) return fail(GPW_ENOMEM, "status word allocation");
   cudaError_t e = cudaMallocHost(&ps->h_any, sizeof(int));
   if (e != cudaSuccess) return cuda_fail(e, "pinned alloc");
-  e = cudaHostAlloc(&ps->h_io, (size_t)nbatch_max * 20 + 64, cudaHostAllocMapped | cudaHostAllocPortable);
+  const size_t slot_bytes = ((size_t)nbatch_max * 20 + 15) / 16 * 16;
+  e = cudaHostAlloc(&ps->h_io, 2 * slot_bytes + 64, cudaHostAllocMapped | cudaHostAllocPortable);
   if (e != cudaSuccess) return cuda_fail(e, "pinned mailbox");
-  ps->h_eps = (double*)ps->h_io;
-  ps->h_err = ps->h_eps + nbatch_max;
-  ps->h_niter = (int*)(ps->h_err + nbatch_max);
   void* dio = nullptr;
   e = cudaHostGetDevicePointer(&dio, ps->h_io, 0);
   if (e != cudaSuccess) return cuda_fail(e, "pinned mailbox mapping");
-  ps->m_eps = (double*)dio;
-  ps->m_err = ps->m_eps + nbatch_max;
-  ps->m_niter = (int*)(ps->m_err + nbatch_max);
+  for (int k = 0; k < 2; ++k) {
+    ps->h_eps[k] = (double*)((char*)ps->h_io + k * slot_bytes);
+    ps->h_err[k] = ps->h_eps[k] + nbatch_max;
+    ps->h_niter[k] = (int*)(ps->h_err[k] + nbatch_max);
+    ps->m_eps[k] = (double*)((char*)dio + k * slot_bytes);
+    ps->m_err[k] = ps->m_eps[k] + nbatch_max;
+    ps->m_niter[k] = (int*)(ps->m_err[k] + nbatch_max);
+  }
   *out = ps.release();
   return GPW_OK;
 }
@@ -636,7 +641,7 @@ static bool fused_dc(const gpw_poisson* ps);
 extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int which, int reps, double* ms_per_launch,
                                        double* bytes_per_launch, gpw_stream stream) {
   if (!ps || !ms_per_launch || !bytes_per_launch) return fail(GPW_EINVAL, "null argument");
-  if (nbatch < 1 || nbatch > ps->nbmax || reps < 1 || which < 0 || which > 5)
+  if (nbatch < 1 || nbatch > ps->nbmax || reps < 1 || which < 0 || which > 6)
     return fail(GPW_EINVAL, "time_level0: bad arguments");
   if (which >= 2) {
     int rc = ensure_f32(ps);
@@ -647,6 +652,10 @@ extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int whic
   Level& L0 = ps->lv[0];
   const int nb = (int)nbatch;
   const double pts = (double)view_points(L0.v) * nb;
+  if (which == 6 && (ps->lv.size() < 2 || ps->lv[1].wpre[1].empty() ||
+                     !resid_restrict_ok(*L0.op, L0.phi32[0].ptr, L0.rho32.ptr, L0.v, ps->lv[1].rho32.ptr,
+                                        ps->lv[1].phi32[0].ptr, ps->lv[1].v, nb)))
+    return fail(GPW_ENOTSUP, "time_level0: no fused residual-restriction here");
   const unsigned char* act = nullptr;
   auto launch = [&]() -> cudaError_t {
     switch (which) {
@@ -666,13 +675,20 @@ extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int whic
       case 4:
         return launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[1].ptr,
                                  L0.rho.ptr, nb, 1.0, L0.w, act, ps->sums.gs(), st);
+      case 6: {
+        Level& C = ps->lv[1];
+        return launch_resid_restrict(*L0.op, L0.phi32[0].ptr, L0.rho32.ptr, L0.v, C.rho32.ptr, C.phi32[0].ptr, C.v,
+                                     nb, C.wpre[1][0], C.op->coefs[0], act, false, st);
+      }
       default:
         return launch_stencil(*L0.op, GPW_F32, MODE_RESIDUAL, L0.phi32[0].ptr, L0.v, L0.res32.ptr, L0.v,
                               L0.rho32.ptr, L0.v, nb, make_boundary(L0.op->periodic, GPW_F32, nullptr), 1.0, act,
                               GridSum{}, st);
     }
   };
-  static const double bytes_pp[6] = {24.0, 16.0, 12.0, 24.0, 24.0, 12.0};
+  // which 6: reads phi and rho (8 B per fine point), writes the next level's
+  // rho and first sweep (8 B per coarse point)
+  static const double bytes_pp[7] = {24.0, 16.0, 12.0, 24.0, 24.0, 12.0, 8.0};
   cudaError_t e = launch();  // warm-up (and lazy kernel setup)
   if (e != cudaSuccess) return cuda_fail(e, "time_level0 launch");
   cudaEvent_t e0, e1;
@@ -689,7 +705,7 @@ extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int whic
   if (e != cudaSuccess) return cuda_fail(e, "time_level0 launch");
   if (se != cudaSuccess) return cuda_fail(se, "time_level0 sync");
   *ms_per_launch = ms / reps;
-  *bytes_per_launch = bytes_pp[which] * pts;
+  *bytes_per_launch = bytes_pp[which] * pts + (which == 6 ? 8.0 * (double)view_points(ps->lv[1].v) * nb : 0.0);
   return GPW_OK;
 }
 
@@ -948,10 +964,10 @@ static cudaError_t pitch_copy(const GridView& v, int nb, const double* src, int6
 // which the previous solve on this engine has finished with (solves end in
 // a stream synchronisation).
 static int solve_prologue(gpw_poisson* ps, double* phi, const double* rho, int nb, const double* eps, int maxiter,
-                          int precision, cudaStream_t st) {
+                          int precision, cudaStream_t st, int slot = 0) {
   Level& L0 = ps->lv[0];
-  std::memcpy(ps->h_eps, eps, (size_t)nb * 8);
-  solve_setup_kernel<<<1, 128, 0, st>>>(nb, ps->m_eps, maxiter, (double*)ps->d_eps.ptr, (int*)ps->d_niter.ptr,
+  std::memcpy(ps->h_eps[slot], eps, (size_t)nb * 8);
+  solve_setup_kernel<<<1, 128, 0, st>>>(nb, ps->m_eps[slot], maxiter, (double*)ps->d_eps.ptr, (int*)ps->d_niter.ptr,
                                         (unsigned char*)ps->d_active.ptr, (int*)ps->d_maxiter.ptr);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = pitch_copy(L0.v, nb, phi, L0.v.n[2], (double*)L0.phi[0].ptr, L0.v.s1, st);
@@ -974,24 +990,36 @@ static int solve_prologue(gpw_poisson* ps, double* phi, const double* rho, int n
   return GPW_OK;
 }
 
-// Result copy and per-solve statistics (kernels on `st`), then the one
-// stream synchronisation of a solve.
-static int solve_epilogue(gpw_poisson* ps, double* phi, int nb, int maxiter, int* niter, double* error,
-                          cudaStream_t st) {
+// Result copy and per-solve statistics into mailbox `slot` (kernels on
+// `st`, nothing waited for).
+static cudaError_t solve_finish(gpw_poisson* ps, double* phi, int nb, cudaStream_t st, int slot) {
   Level& L0 = ps->lv[0];
   cudaError_t e = pitch_copy(L0.v, nb, (const double*)L0.phi[0].ptr, L0.v.s1, phi, L0.v.n[2], st);
   if (e == cudaSuccess) {
     solve_readback_kernel<<<1, 128, 0, st>>>(nb, (const int*)ps->d_niter.ptr, (const double*)ps->d_err.ptr,
-                                             ps->m_niter, ps->m_err);
+                                             ps->m_niter[slot], ps->m_err[slot]);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return cuda_fail(e, "poisson result copies");
-  std::memcpy(niter, ps->h_niter, (size_t)nb * 4);
-  std::memcpy(error, ps->h_err, (size_t)nb * 8);
+  return e;
+}
+
+// The per-solve statistics of a finished solve from mailbox `slot`.
+static int solve_collect(gpw_poisson* ps, int nb, int maxiter, int* niter, double* error, int slot) {
+  std::memcpy(niter, ps->h_niter[slot], (size_t)nb * 4);
+  std::memcpy(error, ps->h_err[slot], (size_t)nb * 8);
   for (int b = 0; b < nb; ++b)
     if (niter[b] >= maxiter) return fail(GPW_ECONV, "Poisson solver did not converge in maxiter iterations");
   return GPW_OK;
+}
+
+// Result copy and per-solve statistics, then the one stream synchronisation
+// of a synchronous solve.
+static int solve_epilogue(gpw_poisson* ps, double* phi, int nb, int maxiter, int* niter, double* error,
+                          cudaStream_t st) {
+  cudaError_t e = solve_finish(ps, phi, nb, st, 0);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "poisson result copies");
+  return solve_collect(ps, nb, maxiter, niter, error, 0);
 }
 
 static int check_solve_args(gpw_poisson* ps, int64_t nbatch, int precision, int maxiter) {
@@ -1053,6 +1081,41 @@ extern "C" int gpw_poisson_set_device_loop(gpw_poisson* ps, int on) {
   if (!ps) return fail(GPW_EINVAL, "null argument");
   ps->device_loop = on != 0;
   return GPW_OK;
+}
+
+// A solve enqueued on `stream` without waiting for it (the device-side
+// loop only): results go to mailbox `slot` (0 or 1) and are read by
+// gpw_poisson_collect once the caller has seen the stream's work finish.  A
+// slot is not reused before its solve has been collected.
+int gpw_poisson_solve_async(gpw_poisson* ps, double* phi, const double* rho, int64_t nbatch, const double* eps,
+                            int maxiter, int precision, int slot, gpw_stream stream) {
+  if (!ps || !phi || !rho || !eps) return fail(GPW_EINVAL, "null argument");
+  if (slot < 0 || slot > 1) return fail(GPW_EINVAL, "poisson: slot must be 0 or 1");
+  int rc = check_solve_args(ps, nbatch, precision, maxiter);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = (int)nbatch;
+  cudaGraphExec_t iter = nullptr;
+  if ((rc = iteration_graph(ps, nb, precision, st, &iter))) return rc;
+  cudaGraphExec_t loop = ps->device_loop ? loop_graph(ps, nb, precision) : nullptr;
+  if (!loop) return fail(GPW_ENOTSUP, "poisson: asynchronous solves need the device-side loop");
+  if ((rc = solve_prologue(ps, phi, rho, nb, eps, maxiter, precision, st, slot))) return rc;
+  cudaError_t e = cudaGraphLaunch(loop, st);
+  if (e != cudaSuccess) return cuda_fail(e, "loop graph launch");
+  if ((e = solve_finish(ps, phi, nb, st, slot)) != cudaSuccess) return cuda_fail(e, "poisson result copies");
+  return GPW_OK;
+}
+
+int gpw_poisson_collect(gpw_poisson* ps, int64_t nbatch, int maxiter, int precision, int slot, int* niter,
+                        double* error) {
+  if (!ps || !niter || !error) return fail(GPW_EINVAL, "null argument");
+  if (slot < 0 || slot > 1 || nbatch < 1 || nbatch > ps->nbmax) return fail(GPW_EINVAL, "poisson: bad arguments");
+  const int rc = solve_collect(ps, (int)nbatch, maxiter, niter, error, slot);
+  int64_t mx = 0;
+  for (int b = 0; b < nbatch; ++b) mx = std::max<int64_t>(mx, niter[b]);
+  ps->last_graphs = mx;
+  ps->last_kernels = (precision == 1 ? 2 : 1) + mx * ps->graph_kernels[gpw_poisson::GraphKey{nbatch, precision}];
+  return rc;
 }
 
 // Per-solve latency of the last solve: device time from the start of the

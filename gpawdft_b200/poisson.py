@@ -522,7 +522,20 @@ class FDPoissonSolver:
                 ev.record(up)
             arrived[k] = ev
 
-        niters = []
+        niters = [None] * n
+        eps_a = np.ascontiguousarray(np.broadcast_to(np.asarray(eps, float),
+                                                     (nb,)))
+        # solves are enqueued without waiting (results collected two batches
+        # later, before their mailbox slot is reused) where the solve needs no
+        # host step after its loop
+        use_async = self.B is None and not self.gd.pbc_c.all()
+        pending = {}
+
+        def collect(k):
+            ev, slot = pending.pop(k)
+            ev.synchronize()
+            niters[k] = self._collect(nb, slot)
+
         upload(0)
         if n > 1:
             upload(1)
@@ -533,10 +546,18 @@ class FDPoissonSolver:
                 if phi_free[s] is not None:
                     compute.wait_event(phi_free[s])
                 phi_d[s].zero_()
-            niters.append(self.solve_batch(phi_d[s], rho_d[s], eps=eps))
+            if k - 2 in pending:
+                collect(k - 2)
+            if use_async and not self._solve_async(phi_d[s], rho_d[s], nb,
+                                                   eps_a, s):
+                use_async = False   # no device-side loop here: solve in turn
+            if not use_async:
+                niters[k] = self.solve_batch(phi_d[s], rho_d[s], eps=eps)
             done = torch.cuda.Event()
             done.record(compute)
             rho_free[s] = done
+            if use_async:
+                pending[k] = (done, s)
             with torch.cuda.stream(down):
                 down.wait_event(done)
                 out[k].copy_(phi_d[s], non_blocking=True)
@@ -545,8 +566,37 @@ class FDPoissonSolver:
             phi_free[s] = ev
             if k + 2 < n:
                 upload(k + 2)
+        for k in sorted(pending):
+            collect(k)
         down.synchronize()   # every copy and solve has finished
         return out, niters
+
+    def _solve_async(self, phi_d, rho_d, nb, eps_a, slot):
+        """Enqueue a solve on the current stream (results to mailbox `slot`);
+        False where asynchronous solves are unavailable."""
+        self._make_engine(nb)
+        rc = self._lib.gpw_poisson_solve_async(
+            self._engine[0], arrays.ptr(phi_d), arrays.ptr(rho_d), nb,
+            eps_a.ctypes.data, int(self.maxiter), _PREC[self.precision],
+            int(slot), arrays.stream())
+        if rc == _lib.GPW_ENOTSUP:
+            return False
+        _lib.check(rc)
+        return True
+
+    def _collect(self, nb, slot):
+        niter = np.zeros(nb, np.int32)
+        err = np.zeros(nb, float)
+        rc = self._lib.gpw_poisson_collect(
+            self._engine[0], nb, int(self.maxiter), _PREC[self.precision],
+            int(slot), niter.ctypes.data, err.ctypes.data)
+        self.last_errors = err
+        if rc == _lib.GPW_ECONV:
+            raise PoissonConvergenceError(
+                'Poisson solver did not converge in %d iterations!' %
+                self.maxiter)
+        _lib.check(rc)
+        return niter
 
     def estimate_memory(self, mem=None):
         gdbytes = int(np.prod(self.gd.n_c)) * 8

@@ -200,6 +200,22 @@ int gpw_poisson_solve(gpw_poisson *ps, double *phi, const double *rho,
                       int precision, int *niter, double *error,
                       gpw_stream stream);
 
+/* The same solve enqueued on `stream` without waiting for it (no
+ * counterpart in the reference): for callers that overlap host transfers
+ * or other work with solves.  The per-solve results land in mailbox `slot`
+ * (0 or 1) and are read by gpw_poisson_collect after the caller has seen
+ * the stream's work finish (an event or a stream synchronisation); a slot
+ * is not reused before its solve has been collected.  Needs the device-side
+ * loop (GPW_ENOTSUP where conditional graph nodes are unavailable).        */
+int gpw_poisson_solve_async(gpw_poisson *ps, double *phi, const double *rho,
+                            int64_t nbatch, const double *eps, int maxiter,
+                            int precision, int slot, gpw_stream stream);
+
+/* Reads the per-solve results of a finished asynchronous solve from mailbox
+ * `slot`: niter[b], error[b]; GPW_ECONV if any solve reached maxiter.       */
+int gpw_poisson_collect(gpw_poisson *ps, int64_t nbatch, int maxiter,
+                        int precision, int slot, int *niter, double *error);
+
 /* Several engines (e.g. one per grid size) solved by ONE graph launch (no
  * counterpart in the reference, which solves one grid per call): each
  * engine's convergence loop runs on the device as a conditional while node
@@ -230,7 +246,9 @@ int gpw_poisson_last_stats(const gpw_poisson *ps, int64_t *kernel_launches,
  * overwritten; call between solves): `which` 0 = float64 Jacobi sweep,
  * 1 = float64 residual + norm, 2 = float32 Jacobi sweep, 3 = float32 sweep
  * adding into float64 phi (defect-correction update), 4 = float64 defect
- * (float32 rhs + first sweep + norm), 5 = float32 residual (no norm).  `reps` launches between CUDA events
+ * (float32 rhs + first sweep + norm), 5 = float32 residual (no norm),
+ * 6 = float32 residual restricted into level 1 (rho and first sweep; the
+ * float32 form's level-0 residual launch).  `reps` launches between CUDA events
  * on `stream`; writes the mean milliseconds per launch and the algorithmic
  * bytes per launch (each compulsory read and write counted once).          */
 int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
