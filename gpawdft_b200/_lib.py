@@ -32,6 +32,7 @@ EXPORTS = [
     'gpw_poisson_solve_async', 'gpw_poisson_collect',
     'gpw_poisson_time_level0', 'gpw_poisson_set_inner_schedule',
     'gpw_set_tma_variant', 'gpw_set_bloch_layout', 'gpw_bloch_launch_count',
+    'gpw_set_restrict_layout', 'gpw_restrict_rows_launch_count',
     'gpw_poisson_set_device_loop', 'gpw_set_pdl', 'gpw_poisson_set_cluster',
     'gpw_poisson_set_fusion',
     'gpw_poisson_solve_many', 'gpw_poisson_last_latency',
@@ -103,6 +104,8 @@ _SIGS = {
     'gpw_poisson_set_cluster': (ctypes.c_int, [_vp, ctypes.c_int]),
     'gpw_poisson_set_fusion': (ctypes.c_int, [_vp, ctypes.c_int]),
     'gpw_bloch_launch_count': (ctypes.c_int64, []),
+    'gpw_set_restrict_layout': (ctypes.c_int, [ctypes.c_int]),
+    'gpw_restrict_rows_launch_count': (ctypes.c_int64, []),
     'gpw_poisson_time_level0': (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int,
                                                ctypes.c_int, _vp, _vp, _vp]),
     'gpw_poisson_set_inner_schedule': (ctypes.c_int, [_vp, _vp, _vp, _vp,

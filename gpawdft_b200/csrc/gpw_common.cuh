@@ -101,9 +101,12 @@ __device__ __forceinline__ double2 phase_mul(double2 p, double2 v) {
   return make_double2(__dsub_rn(__dmul_rn(p.x, v.x), __dmul_rn(p.y, v.y)),
                       __dadd_rn(__dmul_rn(p.x, v.y), __dmul_rn(p.y, v.x)));
 }
+// (complex64: the same formula in float, rounded after every operation, so
+// that every kernel computes the same bits whatever the compiler contracts)
 __device__ __forceinline__ float2 phase_mul(double2 p, float2 v) {
-  float px = (float)p.x, py = (float)p.y;
-  return make_float2(px * v.x - py * v.y, px * v.y + py * v.x);
+  const float px = (float)p.x, py = (float)p.y;
+  return make_float2(__fsub_rn(__fmul_rn(px, v.x), __fmul_rn(py, v.y)),
+                     __fadd_rn(__fmul_rn(px, v.y), __fmul_rn(py, v.x)));
 }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),

@@ -13,6 +13,7 @@
 #include "gpw_stencil.cuh"
 #include "gpw_transfer.cuh"
 #include "gpw_transfer_k2.cuh"
+#include "gpw_transfer_rows.cuh"
 
 namespace gpw {
 
@@ -509,8 +510,151 @@ static cudaError_t run_interp(TransferArgs a, int nbatch, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Restriction layout: 0 = the launcher's choice, 1 = the tile kernel
+// (restrict_kernel), 2 / 3 = the row kernel with 384 / 192 threads (up to
+// 8 / 4 coarse rows per CTA).  Process-wide; for tests and tuning studies.
+static std::atomic<int> g_restrict_force{0};
+static std::atomic<long long> g_restrict_rows_launches{0};
+
+struct RowsPlan {
+  RowRestrictArgs ra;
+  size_t smem;
+};
+
+// Launch plan of restrict_rows_kernel with `nt` threads, or false where the
+// kernel does not apply: 8- or 16-byte elements, rows and strides in whole
+// 16-byte units (TMA and bulk copies), at most 32 staged rows (no more than
+// the rows of a periodic axis 1) and one axis-1 item a thread, a tensor box
+// row of at most 256 scalars, stages that fit in shared memory.
+static bool rows_plan(const TransferArgs& a, int k, size_t es, bool cpx, int nt, int mo, RowsPlan& p) {
+  const int n1 = a.vin.n[1], n2 = a.vin.n[2], nout2 = a.vout.n[2];
+  if (es < 8 || k < 2 || k > 8 || !tensor_map_encoder()) return false;
+  if ((n2 * es) % 16 || (a.vin.s1 * (int64_t)es) % 16 || (a.vin.s0 * (int64_t)es) % 16 ||
+      (a.vin.sb * (int64_t)es) % 16 || !aligned16(a.in))
+    return false;
+  RowRestrictArgs& r = p.ra;
+  r.t = a;
+  r.ty = std::min(std::min(8, nt / std::max(nout2, 1)), a.vout.n[1]);
+  if (r.ty < 1) return false;
+  r.h = 2 * r.ty + 2 * k - 3;
+  if (r.h > 32 || (a.bc.periodic[1] && n1 < r.h)) return false;
+  // halo columns: at least K - 1, in whole 16-byte units
+  const int unit = (int)(16 / es);
+  r.L = (k - 1 + unit - 1) / unit * unit;
+  if (n2 < r.L) return false;
+  // every tap inside the staged row: fine columns -pad .. -pad + 2 (nout2 - 1) + 2K - 2
+  const int lo = -a.pad0[2], hi = -a.pad0[2] + 2 * (nout2 - 1) + 2 * k - 2;
+  if (lo < -r.L || hi >= n2 + r.L) return false;
+  // row pitches 16 bytes past a multiple of 128: lanes on consecutive rows
+  // read distinct banks
+  auto pitch_for = [&](int n) {
+    int q = n;
+    while ((q * (int64_t)es) % 128 != 16) ++q;
+    return q;
+  };
+  r.pitch = pitch_for(n2 + 2 * r.L);
+  if (r.pitch * (cpx ? 2 : 1) > 256) return false;
+  r.pitchz = pitch_for(nout2);
+  r.nseg = (nout2 + mo - 1) / mo;
+  const int per128 = (int)(128 / es);
+  r.stage_elems = (r.h * r.pitch + per128 - 1) / per128 * per128;
+  // the most rows any tile wraps along a periodic axis 1
+  int wmax = 0;
+  if (a.bc.periodic[1]) {
+    const int ntile = (a.vout.n[1] + r.ty - 1) / r.ty;
+    for (int t = 0; t < ntile; ++t) {
+      const int y0 = 2 * t * r.ty - a.pad0[1];
+      const int w = std::min(r.h, std::max(0, -y0) + std::max(0, y0 + r.h - n1));
+      wmax = std::max(wmax, w);
+    }
+  }
+  r.wrap_elems = (wmax * n2 + per128 - 1) / per128 * per128;
+  r.status = device_status_word();
+  p.smem = 128 + (size_t)RR_NS * (r.stage_elems + r.wrap_elems) * es + 2 * (size_t)r.h * r.pitchz * es +
+           RR_NS * 8 + 33 * 4;
+  return p.smem <= 227 * 1024 && r.status != nullptr;
+}
+
+// 4D tensor map of the restriction's input (scalars of complex elements
+// counted separately): box = one staged plane, `pitch` elements by h rows.
+static bool encode_plane_box(CUtensorMap* map, size_t es, bool cpx, const void* base, const GridView& v, int nbatch,
+                             int pitch, int rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const size_t ses = cpx ? es / 2 : es;
+  const int m = cpx ? 2 : 1;
+  cuuint64_t dims[4] = {(cuuint64_t)(v.n[2] * m), (cuuint64_t)v.n[1], (cuuint64_t)v.n[0], (cuuint64_t)nbatch};
+  cuuint64_t strides[3] = {(cuuint64_t)(v.s1 * es), (cuuint64_t)(v.s0 * es),
+                           (cuuint64_t)(std::max<int64_t>(v.sb, v.s0 * v.n[0]) * es)};
+  cuuint32_t box[4] = {(cuuint32_t)(pitch * m), (cuuint32_t)rows, 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(map, ses == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <typename T, int K, int NT>
+static cudaError_t run_restrict_rows(RowsPlan p, int nbatch, cudaStream_t st) {
+  TransferArgs& a = p.ra.t;
+  CUtensorMap map;
+  if (!encode_plane_box(&map, sizeof(T), EltTraits<T>::cpx, a.in, a.vin, nbatch, p.ra.pitch, p.ra.h))
+    return cudaErrorInvalidValue;
+  dim3 grid(1, (a.vout.n[1] + p.ra.ty - 1) / p.ra.ty, 1);
+  choose_chunks(a.vout.n[0], (int64_t)grid.y * nbatch, 2 * K, a.zchunk, a.nchunk);
+  grid.z = a.nchunk * nbatch;
+  auto kern = restrict_rows_kernel<T, K, NT>;
+  static std::once_flag once;
+  cudaError_t e = cudaSuccess;
+  std::call_once(once, [&] { e = smem_optin(kern, 227 * 1024); });
+  if (e != cudaSuccess) return e;
+  kern<<<grid, NT, p.smem, st>>>(map, p.ra);
+  g_restrict_rows_launches.fetch_add(1);
+  return cudaGetLastError();
+}
+
+// The row kernel where it applies (complex and float64 data), else false.
+template <typename T, int K>
+static bool try_restrict_rows(const TransferArgs& a, int nbatch, cudaStream_t st, cudaError_t& e) {
+  if constexpr (sizeof(T) < 8) {
+    return false;
+  } else {
+    const int force = g_restrict_force.load();
+    if (force == 1) return false;
+    RowsPlan p;
+    if (force == 3) {
+      if (!rows_plan(a, K, sizeof(T), EltTraits<T>::cpx, 192, RowRestrictCfg<192>::MO, p)) return false;
+      e = run_restrict_rows<T, K, 192>(p, nbatch, st);
+      return true;
+    }
+    if (!rows_plan(a, K, sizeof(T), EltTraits<T>::cpx, 384, RowRestrictCfg<384>::MO, p)) return false;
+    e = run_restrict_rows<T, K, 384>(p, nbatch, st);
+    return true;
+  }
+}
+
+extern "C" int gpw_set_restrict_layout(int k) {
+  if (k < 0 || k > 3) return fail(GPW_EINVAL, "restriction layout must be 0-3");
+  g_restrict_force.store(k);
+  return GPW_OK;
+}
+
+// Launches of the row restriction kernel so far in this process.
+extern "C" int64_t gpw_restrict_rows_launch_count(void) { return (int64_t)g_restrict_rows_launches.load(); }
+
 template <typename T>
 static cudaError_t dispatch_transfer(const TransferArgs& a, int k, bool interp, int nbatch, cudaStream_t st) {
+  if (!interp && a.out2 == nullptr) {
+    cudaError_t e = cudaSuccess;
+    bool done = false;
+    switch (k) {
+      case 2: done = try_restrict_rows<T, 2>(a, nbatch, st, e); break;
+      case 4: done = try_restrict_rows<T, 4>(a, nbatch, st, e); break;
+      case 6: done = try_restrict_rows<T, 6>(a, nbatch, st, e); break;
+      case 8: done = try_restrict_rows<T, 8>(a, nbatch, st, e); break;
+    }
+    if (done) return e;
+  }
   if (interp) {
     switch (k) {
       case 2: return run_interp<T, 2>(a, nbatch, st);

@@ -307,6 +307,18 @@ int gpw_set_bloch_layout(int k);
  * a shape took the kernel rather than the general one).                   */
 int64_t gpw_bloch_launch_count(void);
 
+/* Pins the kernel that serves restrictions (no counterpart in the
+ * reference): 1 = the tile kernel (2D tiles with halos on both in-plane
+ * axes), 2 / 3 = the row kernel (whole fine rows per plane, 384 / 192
+ * threads a CTA; 8- or 16-byte elements with 16-byte rows and strides, else
+ * the tile kernel), 0 = the launcher's choice.  Results are identical
+ * either way.  Process-wide; for tests and tuning studies.  GPW_EINVAL
+ * outside [0, 3].                                                          */
+int gpw_set_restrict_layout(int k);
+
+/* Launches of the row restriction kernel so far in this process.         */
+int64_t gpw_restrict_rows_launch_count(void);
+
 /* Inner V-cycle schedule of the float32 defect-correction form
  * (precision 1; no counterpart in the reference, whose only schedule is the
  * float64 one of gpaw/poisson.py:111-128, 191-192, which precision 0 keeps).

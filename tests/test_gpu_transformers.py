@@ -86,3 +86,73 @@ def test_band_config_shapes(cuda):
     bb = ol.Transformer(ocoarse, ofine, 3, complex).apply(rr, None, ph)
     assert np.array_equal(r[:1].cpu().numpy(), rr)
     assert np.array_equal(back[:1].cpu().numpy(), bb)
+
+
+@pytest.fixture
+def restrict_layout():
+    from gpawdft_b200 import _lib
+    lib = _lib.load()
+
+    def pin(k):
+        _lib.check(lib.gpw_set_restrict_layout(k))
+    yield pin, lib
+    _lib.check(lib.gpw_set_restrict_layout(0))
+
+
+@pytest.mark.parametrize('layout', [1, 2, 3])
+@pytest.mark.parametrize('pbc', [0, 1])
+@pytest.mark.parametrize('nn', [1, 3, 4])
+@pytest.mark.parametrize('dtype', [np.float64, np.complex128, np.complex64])
+def test_restrict_layouts(cuda, restrict_layout, layout, pbc, nn, dtype):
+    """Each restriction kernel pinned in turn (the tile kernel; the row
+    kernel with 384 and with 192 threads) against the oracle: bit-identical
+    for float64 / complex128.  Rows of 44 points (pbc) take the row kernel;
+    rows of 43 complex64 / float64 points are not whole 16-byte units and
+    keep the tile kernel, as real K = 2 restrictions keep theirs.  36 rows:
+    the last tile of 8 coarse rows wraps 18 of its fine rows when periodic
+    (nn = 4)."""
+    from gpawdft_b200.transformers import Transformer
+    pin, lib = restrict_layout
+    pin(layout)
+    fine, ofine = pair((36, 36, 44), pbc)
+    coarse, ocoarse = fine.coarsen(), ofine.coarsen()
+    a = rand((3,) + tuple(fine.n_c), dtype, 31)
+    ph = None
+    if np.dtype(dtype).kind == 'c':
+        ph = phase_cd_for_k(ofine, np.random.default_rng(6).uniform(-.5, .5, 3))
+    n0 = lib.gpw_restrict_rows_launch_count()
+    out = Transformer(fine, coarse, nn, dtype).apply(a, None, ph)
+    rows = lib.gpw_restrict_rows_launch_count() - n0
+    ref = ol.Transformer(ofine, ocoarse, nn, oracle_dtype(dtype)).apply(
+        a.astype(oracle_dtype(dtype)), None, ph)
+    if np.dtype(dtype) == np.dtype(np.complex64):
+        assert relerr(out, ref) < TOL[np.dtype(dtype)]
+    else:
+        assert np.array_equal(out, ref), relerr(out, ref)
+    whole = fine.n_c[2] * np.dtype(dtype).itemsize % 16 == 0
+    # real K = 2 restrictions keep their own kernels
+    served = whole and (np.dtype(dtype).kind == 'c' or nn > 1)
+    assert rows == (1 if layout > 1 and served else 0)
+
+
+def test_restrict_rows_bands_equal_tile(cuda, restrict_layout):
+    """96^3 -> 48^3 complex128 / complex64 Bloch bands, K = 6: both row
+    layouts equal the tile kernel bit for bit (same operations, same order)."""
+    import torch
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.transformers import Transformer
+    pin, lib = restrict_layout
+    h = 0.18 / 0.52917721
+    fine = GridDescriptor((96,) * 3, (96 * h,) * 3, 1)
+    ofine = OGD((96,) * 3, (96 * h,) * 3, 1)
+    ph = phase_cd_for_k(ofine, [0.21, -0.44, 0.05])
+    for dt, tdt in ((complex, torch.complex128), (np.complex64, torch.complex64)):
+        g = torch.Generator(device='cuda').manual_seed(7)
+        a = torch.randn((5, 96, 96, 96), dtype=tdt, device='cuda', generator=g)
+        R = Transformer(fine, fine.coarsen(), 3, dt)
+        outs = []
+        for layout in (1, 2, 3):
+            pin(layout)
+            outs.append(R.apply(a, None, ph).cpu().numpy())
+        assert np.array_equal(outs[0], outs[1])
+        assert np.array_equal(outs[0], outs[2])
