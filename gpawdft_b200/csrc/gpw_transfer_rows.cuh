@@ -67,6 +67,40 @@ struct RowRestrictCfg {
   static constexpr int MO = NT >= 384 ? 4 : 6;  // axis-2 outputs per item
 };
 
+// Axis-0 restriction over a ring of the last 2K - 1 axis-1 results whose
+// newest entry is q[NEW]: the centre is K - 1 entries back; the sums run in
+// restrict_1d's order.  Compile-time indices keep the ring in registers.
+template <int K, int NEW, typename T>
+__device__ __forceinline__ T restrict_ring(const T (&q)[2 * K - 1]) {
+  using S = typename EltTraits<T>::S;
+  constexpr int NQ = 2 * K - 1;
+  constexpr int C = (NEW - (K - 1) + NQ) % NQ;
+  if constexpr (K == 2) {
+    return rmul(S(0.5), radd(q[C], rmul(S(0.5), radd(q[(C + 1) % NQ], q[(C + NQ - 1) % NQ]))));
+  } else {
+    T s = q[C];
+#pragma unroll
+    for (int j = 0; j < K / 2; ++j)
+      s = radd(s, rmul((S)TW<K>::w(j), radd(q[(C + 2 * j + 1) % NQ], q[(C + NQ - 2 * j - 1) % NQ])));
+    return rmul(S(0.5), s);
+  }
+}
+
+// Write v into ring slot k (runtime) and, when `emit`, return the output it
+// completes; one case per slot.
+template <int K, int I = 0, typename T>
+__device__ __forceinline__ T ring_push(T (&q)[2 * K - 1], int k, const T& v, bool emit) {
+  if constexpr (I == 2 * K - 1) {
+    return v;
+  } else {
+    if (k == I) {
+      q[I] = v;
+      return emit ? restrict_ring<K, I>(q) : v;
+    }
+    return ring_push<K, I + 1>(q, k, v, emit);
+  }
+}
+
 // Stage layout: the tensor box of a plane, h rows of `pitch` elements taken
 // from fine column -L on: L halo columns (out of range, zero-filled; on a
 // periodic axis 2 the fix-up writes the row's last L values there), the n2
@@ -131,6 +165,17 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 1 : 2)
 
   const unsigned rowbytes = (unsigned)(n2 * sizeof(T));
   const unsigned boxbytes = (unsigned)(h * pitch * sizeof(T));
+  // this thread's first halo value of a periodic axis 2 (stage offsets)
+  int hsrc = -1, hdst = 0, hside = 0;
+  if (per2 && tid < h * 2 * L) {
+    const int r = tid / (2 * L), k = tid - r * (2 * L);
+    int j1, s1;
+    if (!(wrap_axis(yfirst + r, n1, bc.periodic[1], j1, s1) && s1 >= 0)) {
+      hsrc = r * pitch + (k < L ? L + n2 - L + k : L + (k - L));
+      hdst = r * pitch + (k < L ? k : L + n2 + (k - L));
+      hside = k < L ? 1 : 0;
+    }
+  }
   // warp 0 streams the planes: lane 0 the tensor box, the lanes of wrapped
   // rows their bulk copies
   auto issue = [&](int i) {
@@ -192,7 +237,12 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 1 : 2)
         put(row, c, phase_mul(bc.ph[0][s0], row[L + c]));
       }
     } else if (per2) {
-      for (int idx = tid; idx < h * 2 * L; idx += NT) {
+      // this thread's first halo value is precomputed (hsrc < 0: none)
+      if (hsrc >= 0) {
+        const T v = st[hsrc];
+        st[hdst] = cpx_phase ? phase_mul(bc.ph[2][hside], v) : v;
+      }
+      for (int idx = tid + NT; idx < h * 2 * L; idx += NT) {
         const int r = idx / (2 * L), k = idx - r * (2 * L);
         int j1, s1;
         if (wrap_axis(yfirst + r, n1, bc.periodic[1], j1, s1) && s1 >= 0) continue;  // wrapped: done above
@@ -219,12 +269,14 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 1 : 2)
   const int Yl = tid / nout2, J = tid - Yl * nout2;
   const bool yitem = tid < yitems;
   const bool ystore = yitem && Y0 + Yl < a.vout.n[1];
-  T q[NQ];
+  T q[NQ];  // ring of the last NQ axis-1 results; the next goes to q[qk]
 #pragma unroll
   for (int i = 0; i < NQ; ++i) q[i] = zero<T>();
+  int qk = 0;
   // stage column of the first odd-offset tap of output 0
   const int cx0 = L + (K - 1 - a.pad0[2]) - (K - 1);
   const int xitems = h * ra.nseg;
+  const int xr = tid % h, xJa = (tid / h) * MO;  // this thread's first axis-2 item
 
   for (int s = 0; s <= nsteps; ++s) {
     if (s < nsteps) {
@@ -234,8 +286,13 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 1 : 2)
       const T* stg = ring + (s % NS) * ra.stage_elems;
       T* zbuf = zb + (s & 1) * h * pitchz;
       for (int it = tid; it < xitems; it += NT) {
-        const int seg = it / h, r = it - seg * h;
-        const int Ja = seg * MO, nJ = min(MO, nout2 - Ja);
+        int r = xr, Ja = xJa;
+        if (it != tid) {
+          const int seg = it / h;
+          r = it - seg * h;
+          Ja = seg * MO;
+        }
+        const int nJ = min(MO, nout2 - Ja);
         const T* rp = stg + r * pitch + cx0 + 2 * Ja;
         T* zrow = zbuf + r * pitchz + Ja;
         T w[MO + K - 1];
@@ -257,14 +314,13 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 1 : 2)
       // ---- axis-1 pass of plane s - 1, axis-0 queue, output
       const T* zbuf = zb + ((s - 1) & 1) * h * pitchz;
       const T v = restrict_1d<K>(zbuf + (K - 1 + 2 * Yl) * pitchz + J, pitchz);
-#pragma unroll
-      for (int i = 0; i < NQ - 1; ++i) q[i] = q[i + 1];
-      q[NQ - 1] = v;
       // step s - 1 completes output I0 + (s - 1 - (NQ - 1)) / 2 when even
       const int t = s - 1 - (NQ - 1);
-      if (t >= 0 && (t & 1) == 0 && ystore) {
+      const bool emit = t >= 0 && (t & 1) == 0 && ystore;
+      const T o = ring_push<K>(q, qk, v, emit);
+      qk = qk + 1 == NQ ? 0 : qk + 1;
+      if (emit) {
         const int I = I0 + (t >> 1);
-        const T o = restrict_1d<K>(q + (K - 1), 1);
         static_cast<T*>(a.out)[(int64_t)b * a.vout.sb + (int64_t)I * a.vout.s0 + (int64_t)(Y0 + Yl) * a.vout.s1 +
                                J] = o;
       }
