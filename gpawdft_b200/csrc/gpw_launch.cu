@@ -150,8 +150,9 @@ int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& v, int 
   choose_chunks(v.n[0], (int64_t)gx * gy * nbatch, minz, zc, nc);
   int nblk = gx * gy * nc;
   if (use_star) {  // a TMA tile variant may be chosen instead: bound its CTA count
-    // (tiles of at least 64 x 8 points, at most n0 / (2R + 2) axis-0 chunks)
-    const int tx2 = (v.n[2] + 63) / 64, ty2 = (v.n[1] + 7) / 8;
+    // (tiles at least 48 points wide and 8 rows high, at most n0 / (2R + 2)
+    // axis-0 chunks)
+    const int tx2 = (v.n[2] + 47) / 48, ty2 = (v.n[1] + 7) / 8;
     nblk = std::max(nblk, tx2 * ty2 * std::max(1, v.n[0] / (2 * d.R + 2)));
   }
   return nblk;

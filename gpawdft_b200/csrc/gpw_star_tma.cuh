@@ -48,6 +48,9 @@ template <> struct TmaVariant<8> { using T = TmaShape<16, 4, 16, 1, 2, 2>; };  /
 // 68 x 16 tile: with the residual restricted in-kernel, 32 coarse columns a
 // tile at a 64-column stride
 template <> struct TmaVariant<9> { using T = TmaShape<17, 4, 8, 2, 2, 3>; };
+// both element types: 48 x 16 tile (192 threads), whole rows of 48-point
+// grids with no idle columns
+template <> struct TmaVariant<10> { using T = TmaShape<24, 2, 8, 2, 2, 2>; };
 
 // VEC elements of S moved as one vector load / store
 template <typename S, int N> struct VecT;

@@ -50,7 +50,7 @@ enum StencilMode {
 };
 
 // Number of tile-shape variants of the TMA star kernel (gpw_star_tma.cuh).
-constexpr int TMA_NVARIANT = 10;  // 5 - 9: float32 only
+constexpr int TMA_NVARIANT = 11;  // 5 - 9: float32 only
 
 constexpr int PMAX = 80;  // GUC n<=6 with 6 directions needs 73
 

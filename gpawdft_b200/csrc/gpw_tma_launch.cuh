@@ -18,11 +18,11 @@ namespace gpw {
 // (the nn=3 Laplacian of level 0); radius 2 uses variant 2 only and radius 4
 // variant 1 (128 threads: its float64 accumulators do not fit the register
 // share of two 256-thread CTAs per SM).  The 4-point variants (5 - 9) are
-// float32 only.
+// float32 only; variant 10 (48-wide tiles) exists for both.
 __host__ __device__ constexpr int tma_default_variant(int R) { return R == 4 ? 1 : 2; }
 template <typename S>
 __host__ __device__ constexpr bool tma_variant_compiled(int R, int v) {
-  if (v >= 5 && sizeof(S) != 4) return false;
+  if (v >= 5 && v <= 9 && sizeof(S) != 4) return false;
   return (R == 1 || R == 3) ? (v >= 0 && v < TMA_NVARIANT) : v == tma_default_variant(R);
 }
 
@@ -129,6 +129,7 @@ cudaError_t tma_run_variant(int var, const StencilArgs& a, int nbatch, const Sta
       case 2: return TmaKernel<S, R, MODE, 2>::run(a, nbatch, sc, nchunk, st);
       case 3: return TmaKernel<S, R, MODE, 3>::run(a, nbatch, sc, nchunk, st);
       case 4: return TmaKernel<S, R, MODE, 4>::run(a, nbatch, sc, nchunk, st);
+      case 10: return TmaKernel<S, R, MODE, 10>::run(a, nbatch, sc, nchunk, st);
     }
     if constexpr (sizeof(S) == 4) {
       switch (var) {

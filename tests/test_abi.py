@@ -107,7 +107,7 @@ def test_launch_plan_switches_validate():
     TMA variant range, Bloch layout index, and a null engine."""
     lib = _lib.load()
     assert lib.gpw_set_tma_variant(-2, 0) == _lib.GPW_EINVAL
-    assert lib.gpw_set_tma_variant(10, 0) == _lib.GPW_EINVAL
+    assert lib.gpw_set_tma_variant(11, 0) == _lib.GPW_EINVAL
     assert lib.gpw_set_tma_variant(-1, 0) == _lib.GPW_OK   # back to the tuned choice
     assert lib.gpw_set_bloch_layout(-1) == _lib.GPW_EINVAL
     assert lib.gpw_set_bloch_layout(17) == _lib.GPW_EINVAL

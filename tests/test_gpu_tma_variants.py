@@ -18,7 +18,7 @@ from gpawdft_b200.workloads import gaussian_density
 
 pytestmark = pytest.mark.gpu
 
-NVARIANT = 10           # 0-4 both element types, 5-9 float32 only
+NVARIANT = 11           # 0-4 and 10 both element types, 5-9 float32 only
 CHUNKS = [0, 1, -2]     # wave model, one chunk, twice the model's count
 
 
