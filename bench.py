@@ -775,6 +775,19 @@ def run_bands(args):
                                          'frac': gbs / peak}
         del a, c
         torch.cuda.empty_cache()
+    # eigensolver preconditioner (gpaw/preconditioner.py:34-60): a block of
+    # 32 complex128 residuals, the caller's nn=3 kinetic operator, the same
+    # Bloch phases; its three grids and nine launches per band are timed
+    # whole, so the line reports time, not a roofline fraction
+    from gpawdft_b200.preconditioner import Preconditioner
+    nbp = min(NB, 32)
+    g = torch.Generator(device='cuda').manual_seed(4)
+    r = torch.randn((nbp, 96, 96, 96), dtype=torch.complex128, device='cuda', generator=g)
+    P = Preconditioner(gd, Laplace(gd, -0.5, 3, complex), complex, block=nbp)
+    t = timeit(lambda: P(r, ph), args.steps)
+    res['c128_preconditioner'] = {'ms': t * 1e3, 'bands_per_s': nbp / t, 'block': nbp}
+    del r, P
+    torch.cuda.empty_cache()
     line = {'metric': 'band_stencil_GBps_256x96^3_bloch', 'value':
             res['c128_laplace']['GB/s'], 'unit': 'GB/s',
             'higher_is_better': True, 'n_gpus': 1, 'steps': args.steps,
