@@ -344,19 +344,27 @@ def run_ours(args, rank, world, dist):
              4: 'star_tma_kernel<double,3,RESID_DC> level-0 fp64 defect',
              5: 'star_tma_kernel<float,3,RESIDUAL> level-0 residual',
              6: 'star_tma_kernel<float,3,RESID_RESTRICT> level-0 residual '
-                '+ restriction into level 1'}
+                '+ restriction into level 1',
+             7: 'star_tma_kernel<float,3,JACOBI_SCALED_IN> level-0 sweep '
+                'reading the defect alone'}
     # launches of each per outer iteration: float64 method 3 sweeps + 2
     # residuals; float32 form (2 + 2 Chebyshev sweeps on level 0) 2 plain
     # sweeps, 1 residual, 1 defect, 1 update
     # (the float32 form's level-0 residual is restricted in the same launch
-    # where the grid allows it: which 6, else the plain residual, which 5)
+    # where the grid allows it: which 6, else the plain residual, which 5;
+    # its second pre-sweep reads the defect alone where the plan allows it:
+    # which 7 and one plain sweep, else two plain sweeps)
     per_iter = ({0: 3, 1: 2} if args.precision == 'fp64' else
-                {2: 2, 6: 1, 4: 1, 3: 1})
+                {2: 1, 7: 1, 6: 1, 4: 1, 3: 1})
     for which in list(per_iter):
         ms, nbytes = ctypes.c_double(), ctypes.c_double()
         rc = lib.gpw_poisson_time_level0(
             ps._engine[0], B, which, 20, ctypes.byref(ms), ctypes.byref(nbytes),
             stream.cuda_stream)
+        if rc == _lib.GPW_ENOTSUP and which == 7:
+            del per_iter[7]
+            per_iter[2] = 2
+            continue
         if rc == _lib.GPW_ENOTSUP and which == 6:
             del per_iter[6]
             per_iter[5] = 1
@@ -375,6 +383,8 @@ def run_ours(args, rank, world, dist):
     ncu_bytes_per_point = {2: (139.83e6 + 40.00e6) / 16387064,
                            4: (292.3e6 + 103.9e6) / 16387064,
                            3: (268.9e6 + 90.9e6) / 16387064}
+    if 7 in per_iter:  # the defect's capture stored the first iterate too
+        del ncu_bytes_per_point[4]
     t_sweep, sweep_bytes = kernels[dom]
     achieved = sweep_bytes / t_sweep / 1e9
     peak, peak_src = measured_peak()

@@ -363,7 +363,7 @@ cudaError_t launch_stencil_dc(const OpDesc& d, int mode, const void* in, const G
   a.c0 = d.coefs[0];
   a.active = active;
   a.gsum = gs;
-  if (mode != MODE_RESID_DC && mode != MODE_JACOBI_ADD64) return cudaErrorInvalidValue;
+  if (mode != MODE_RESID_DC && mode != MODE_JACOBI_ADD64 && mode != MODE_JACOBI_SCALED_IN) return cudaErrorInvalidValue;
   const int dtype = (mode == MODE_RESID_DC) ? GPW_F64 : GPW_F32;
   const TmaChoice ch = tma_choice(dtype, d.R, mode, v, nbatch);
   return tma_launch(dtype, mode, d.R, ch, a, nbatch, d.sc, st);
@@ -418,7 +418,7 @@ cudaError_t tune_stencil(const OpDesc& d, int dtype, int mode, const void* in, c
   a.c0 = d.coefs.empty() ? 1.0 : d.coefs[0];
   a.gsum = gs;
   int ldtype = dtype;
-  if (mode == MODE_RESID_DC || mode == MODE_JACOBI_ADD64) {
+  if (mode == MODE_RESID_DC || mode == MODE_JACOBI_ADD64 || mode == MODE_JACOBI_SCALED_IN) {
     const size_t es_in = (mode == MODE_RESID_DC) ? 8 : 4;
     if (!dc_fusable(d) || !aligned16(in) || !aligned16(rho) || !aligned16(out2) || (out && !aligned16(out)) ||
         !view_tma_ok(vout, es_in, nbatch) || !view_tma_ok(vout, 4, nbatch))

@@ -637,17 +637,20 @@ void gpw_poisson_free(gpw_poisson* ps) { delete ps; }
 
 static int ensure_f32(gpw_poisson* ps);
 static bool fused_dc(const gpw_poisson* ps);
+static bool scaled_first(const gpw_poisson* ps);
 
 extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int which, int reps, double* ms_per_launch,
                                        double* bytes_per_launch, gpw_stream stream) {
   if (!ps || !ms_per_launch || !bytes_per_launch) return fail(GPW_EINVAL, "null argument");
-  if (nbatch < 1 || nbatch > ps->nbmax || reps < 1 || which < 0 || which > 6)
+  if (nbatch < 1 || nbatch > ps->nbmax || reps < 1 || which < 0 || which > 7)
     return fail(GPW_EINVAL, "time_level0: bad arguments");
   if (which >= 2) {
     int rc = ensure_f32(ps);
     if (rc) return rc;
   }
   if ((which == 3 || which == 4) && !fused_dc(ps)) return fail(GPW_ENOTSUP, "time_level0: no fused path here");
+  if (which == 7 && !scaled_first(ps)) return fail(GPW_ENOTSUP, "time_level0: no scaled first sweep here");
+  const bool scaled = scaled_first(ps);
   cudaStream_t st = (cudaStream_t)stream;
   Level& L0 = ps->lv[0];
   const int nb = (int)nbatch;
@@ -672,9 +675,12 @@ extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int whic
       case 3:
         return launch_stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[0].ptr, L0.v, nullptr, L0.phi[1].ptr,
                                  L0.rho32.ptr, nb, L0.w, 0.0, act, GridSum{}, st);
-      case 4:
-        return launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[1].ptr,
-                                 L0.rho.ptr, nb, 1.0, L0.w, act, ps->sums.gs(), st);
+      case 4:  // as the iteration launches it (no stored iterate when the next sweep forms it)
+        return launch_stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr,
+                                 scaled ? nullptr : L0.phi32[1].ptr, L0.rho.ptr, nb, 1.0, L0.w, act, ps->sums.gs(), st);
+      case 7:
+        return launch_stencil_dc(*L0.op, MODE_JACOBI_SCALED_IN, L0.rho32.ptr, L0.v, L0.phi32[1].ptr, nullptr,
+                                 nullptr, nb, L0.wpre[1][1], L0.wpre[1][0], act, GridSum{}, st);
       case 6: {
         Level& C = ps->lv[1];
         return launch_resid_restrict(*L0.op, L0.phi32[0].ptr, L0.rho32.ptr, L0.v, C.rho32.ptr, C.phi32[0].ptr, C.v,
@@ -687,8 +693,9 @@ extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int whic
     }
   };
   // which 6: reads phi and rho (8 B per fine point), writes the next level's
-  // rho and first sweep (8 B per coarse point)
-  static const double bytes_pp[7] = {24.0, 16.0, 12.0, 24.0, 24.0, 12.0, 8.0};
+  // rho and first sweep (8 B per coarse point); 4 without the stored iterate:
+  // 20 B; 7: reads rhs, writes phi (8 B)
+  static const double bytes_pp[8] = {24.0, 16.0, 12.0, 24.0, 24.0, 12.0, 8.0, 8.0};
   cudaError_t e = launch();  // warm-up (and lazy kernel setup)
   if (e != cudaSuccess) return cuda_fail(e, "time_level0 launch");
   cudaEvent_t e0, e1;
@@ -705,7 +712,8 @@ extern "C" int gpw_poisson_time_level0(gpw_poisson* ps, int64_t nbatch, int whic
   if (e != cudaSuccess) return cuda_fail(e, "time_level0 launch");
   if (se != cudaSuccess) return cuda_fail(se, "time_level0 sync");
   *ms_per_launch = ms / reps;
-  *bytes_per_launch = bytes_pp[which] * pts + (which == 6 ? 8.0 * (double)view_points(ps->lv[1].v) * nb : 0.0);
+  *bytes_per_launch = (which == 4 && scaled ? 20.0 : bytes_pp[which]) * pts +
+                      (which == 6 ? 8.0 * (double)view_points(ps->lv[1].v) * nb : 0.0);
   return GPW_OK;
 }
 
@@ -737,6 +745,12 @@ static bool fused_dc(const gpw_poisson* ps) {
   return ps->relax_method == 2 && ps->lv.size() >= 2 && !L0.wpre[1].empty() && !L0.wpost[1].empty() &&
          dc_fusable(*L0.op);
 }
+
+// The float32 form's second level-0 pre-sweep reads the defect alone and
+// forms the first sweep's iterate itself (MODE_JACOBI_SCALED_IN), so the
+// float64 defect stores no iterate: with the fusions on and at least two
+// level-0 pre-sweeps.
+static bool scaled_first(const gpw_poisson* ps) { return fused_dc(ps) && ps->use_rr && ps->lv[0].wpre[1].size() >= 2; }
 
 // tune = true: the autotuner's pass over the same stencil launches (before
 // capture, on the engine's buffers); nothing else is launched.
@@ -776,7 +790,17 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStrea
     Level& C = ps->lv[1];
     const std::vector<double>& wpre = L0.wpre[1];
     const std::vector<double>& wpost = L0.wpost[1];
-    int cur = rec_relax(r, 0, 0, wpre.data() + 1, (int)wpre.size() - 1, true);
+    int cur;
+    if (scaled_first(ps)) {
+      // the second pre-sweep reads rhs alone and forms the first sweep's
+      // iterate (w2 / c0) rhs itself, so RESID_DC stores no iterate
+      r.stencil_dc(*L0.op, MODE_JACOBI_SCALED_IN, L0.rho32.ptr, L0.v, L0.phi32[1].ptr, nullptr, nullptr, wpre[1],
+                   wpre[0], GridSum{});
+      r.tick("L0 f32 jacobi from rhs");
+      cur = rec_relax(r, 0, 1, wpre.data() + 2, (int)wpre.size() - 2, true);
+    } else {
+      cur = rec_relax(r, 0, 0, wpre.data() + 1, (int)wpre.size() - 1, true);
+    }
     int ccur;
     const int nl = (int)ps->lv.size();
     const bool rr = ps->use_rr && nl > 2 && ps->lc[1] > 1 && ps->lt != 1 && L0.restr->k == 2 &&
@@ -807,9 +831,9 @@ static cudaError_t record_iteration(gpw_poisson* ps, int nb, int prec, cudaStrea
     r.stencil_dc(*L0.op, MODE_JACOBI_ADD64, L0.phi32[cur].ptr, L0.v, nullptr, L0.phi[0].ptr, L0.rho32.ptr,
                  wpost.back(), 0.0, GridSum{});
     r.tick("L0 f32 jacobi + phi64 update");
-    r.stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr, L0.phi32[0].ptr, L0.rho.ptr, 1.0,
-                 wpre[0], ps->sums.gs());
-    r.tick("L0 f64 defect + first sweep");
+    r.stencil_dc(*L0.op, MODE_RESID_DC, L0.phi[0].ptr, L0.v, L0.rho32.ptr,
+                 scaled_first(ps) ? nullptr : L0.phi32[0].ptr, L0.rho.ptr, 1.0, wpre[0], ps->sums.gs());
+    r.tick(scaled_first(ps) ? "L0 f64 defect" : "L0 f64 defect + first sweep");
     converge();
     return r.err;
   } else {

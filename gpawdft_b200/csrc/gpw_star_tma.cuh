@@ -118,11 +118,11 @@ struct TmaCfg {
   static constexpr int D = Sh::D;                      // planes prefetched beyond the current one
   // ring stages: a Jacobi sweep re-reads its centre value R planes behind;
   // the other epilogues read each plane once, at arrival
-  static constexpr bool KEEP_CENTRE = MODE == MODE_JACOBI || MODE == MODE_JACOBI_ADD64;
+  static constexpr bool KEEP_CENTRE = MODE == MODE_JACOBI || MODE == MODE_JACOBI_ADD64 || MODE == MODE_JACOBI_SCALED_IN;
   static constexpr int NS = KEEP_CENTRE ? R + D + 1 : D + 1;
   // per stage: the input plane (with halo), the rho plane of the output
   // completed at that step, and (JACOBI_ADD64) the float64 phi plane
-  static constexpr bool HAS_RHO = MODE != MODE_APPLY;
+  static constexpr bool HAS_RHO = MODE != MODE_APPLY && MODE != MODE_JACOBI_SCALED_IN;  // (scaled: rho is the input)
   static constexpr bool HAS_AUX = MODE == MODE_JACOBI_ADD64;
   static constexpr int IN_BYTES = H * W * (int)sizeof(S);
   static constexpr int RHO_BYTES = HAS_RHO ? TY * TZ * (int)sizeof(S) : 0;
@@ -302,6 +302,13 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
         P col[PY + 2 * R];
 #pragma unroll
         for (int i = 0; i < PY + 2 * R; ++i) col[i] = ldv<S, VEC>(sl + (yb + i) * W + xl);
+        if constexpr (MODE == MODE_JACOBI_SCALED_IN) {
+          // phi = (w2 / c0) rhs, rounded as RESID_DC rounds the stored iterate
+#pragma unroll
+          for (int i = 0; i < PY + 2 * R; ++i)
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) col[i].v[e] = k.wc2 * col[i].v[e];
+        }
 #pragma unroll
         for (int j = 0; j < PY; ++j) {
           const S* row = sl + (yb + j + R) * W + xl;
@@ -313,14 +320,19 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
             const P hi = ldv<S, VEC>(row + VEC + q);
 #pragma unroll
             for (int e = 0; e < VEC; ++e) {
-              nb[q + e] = lo.v[e];
-              nb[XL + VEC + q + e] = hi.v[e];
+              if constexpr (MODE == MODE_JACOBI_SCALED_IN) {
+                nb[q + e] = k.wc2 * lo.v[e];
+                nb[XL + VEC + q + e] = k.wc2 * hi.v[e];
+              } else {
+                nb[q + e] = lo.v[e];
+                nb[XL + VEC + q + e] = hi.v[e];
+              }
             }
           }
           const P c = col[j + R];
 #pragma unroll
           for (int e = 0; e < VEC; ++e) nb[XL + e] = c.v[e];
-          constexpr bool sweep = (MODE == MODE_JACOBI || MODE == MODE_JACOBI_ADD64);
+          constexpr bool sweep = (MODE == MODE_JACOBI || MODE == MODE_JACOBI_ADD64 || MODE == MODE_JACOBI_SCALED_IN);
           S p[VEC];
 #pragma unroll
           for (int e = 0; e < VEC; ++e) p[e] = sweep ? S(0) : k.cc * c.v[e];
@@ -382,7 +394,15 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
               } else {
                 // the centre value, R planes behind in the ring
                 const S* osl = reinterpret_cast<const S*>(ring + ((s + NS - R) % NS) * C::STAGE_BYTES);
-                const P cur = ldv<S, VEC>(osl + (yb + j + R) * W + xl);
+                P cur = ldv<S, VEC>(osl + (yb + j + R) * W + xl);
+                if constexpr (MODE == MODE_JACOBI_SCALED_IN) {
+                  // the ring holds rhs: rho = rhs, phi = (w2 / c0) rhs
+#pragma unroll
+                  for (int e = 0; e < VEC; ++e) {
+                    rho.v[e] = cur.v[e];
+                    cur.v[e] = k.wc2 * cur.v[e];
+                  }
+                }
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) res.v[e] = k.w1 * cur.v[e] + k.wc * (rho.v[e] - av.v[e]);
               }
@@ -395,13 +415,13 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
                   e1.v[e] = k.wc2 * rhs.v[e];
                 }
                 float* rp = static_cast<float*>(a.out) + oidx;
-                float* ep = static_cast<float*>(a.out2) + oidx;
+                float* ep = static_cast<float*>(a.out2) + oidx;  // null: the next sweep forms e1 itself
                 if (nx == VEC) {
                   stv<float, VEC>(rp, rhs);
-                  stv<float, VEC>(ep, e1);
+                  if (a.out2) stv<float, VEC>(ep, e1);
                 } else {
                   stv_part<float, VEC>(rp, rhs, nx);
-                  stv_part<float, VEC>(ep, e1, nx);
+                  if (a.out2) stv_part<float, VEC>(ep, e1, nx);
                 }
               } else if constexpr (MODE == MODE_JACOBI_ADD64) {
                 // phi64 += e (the inner correction), e never stored

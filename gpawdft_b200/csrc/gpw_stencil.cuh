@@ -39,14 +39,18 @@ namespace gpw {
 // float32 residual that is not stored but restricted (K = 2, zero
 // boundaries) into the next level: rho_c to `out` and that level's first
 // Jacobi iterate from zero, (w2 / c0) rho_c with c0 the next level's
-// diagonal, to `out2`, both in the coarse view `vco`.
+// diagonal, to `out2`, both in the coarse view `vco`.  JACOBI_SCALED_IN is a
+// float32 Jacobi sweep whose iterate is never stored: it reads only the
+// defect rhs (`in`) and takes phi = (w2 / c0) rhs -- the first inner sweep
+// from zero, rounded exactly as RESID_DC rounds it -- with rho = rhs.
 enum StencilMode {
   MODE_APPLY = 0,
   MODE_RESIDUAL = 1,
   MODE_JACOBI = 2,
   MODE_RESID_DC = 3,
   MODE_JACOBI_ADD64 = 4,
-  MODE_RESID_RESTRICT = 5
+  MODE_RESID_RESTRICT = 5,
+  MODE_JACOBI_SCALED_IN = 6
 };
 
 // Number of tile-shape variants of the TMA star kernel (gpw_star_tma.cuh).

@@ -12,6 +12,8 @@ cudaError_t tma_stencil_f32(int mode, int R, int var, const StencilArgs& a, int 
     case MODE_RESIDUAL: return tma_run_radius<float, MODE_RESIDUAL>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_JACOBI: return tma_run_radius<float, MODE_JACOBI>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_JACOBI_ADD64: return tma_run_radius<float, MODE_JACOBI_ADD64>(R, var, a, nbatch, sc, nchunk, st);
+    case MODE_JACOBI_SCALED_IN:
+      return tma_run_radius<float, MODE_JACOBI_SCALED_IN>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_RESID_RESTRICT:  // the float32 form's level 0 (nn = 3) only
       if (R == 3) return tma_run_variant<float, 3, MODE_RESID_RESTRICT>(var, a, nbatch, sc, nchunk, st);
       return cudaErrorInvalidValue;

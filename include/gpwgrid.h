@@ -246,9 +246,12 @@ int gpw_poisson_last_stats(const gpw_poisson *ps, int64_t *kernel_launches,
  * overwritten; call between solves): `which` 0 = float64 Jacobi sweep,
  * 1 = float64 residual + norm, 2 = float32 Jacobi sweep, 3 = float32 sweep
  * adding into float64 phi (defect-correction update), 4 = float64 defect
- * (float32 rhs + first sweep + norm), 5 = float32 residual (no norm),
- * 6 = float32 residual restricted into level 1 (rho and first sweep; the
- * float32 form's level-0 residual launch).  `reps` launches between CUDA events
+ * (float32 rhs + norm, and the first sweep unless the next sweep forms it),
+ * 5 = float32 residual (no norm), 6 = float32 residual restricted into
+ * level 1 (rho and first sweep; the float32 form's level-0 residual
+ * launch), 7 = float32 sweep reading the defect alone and forming the first
+ * sweep's iterate itself (GPW_ENOTSUP where the plan does not use it).
+ * `reps` launches between CUDA events
  * on `stream`; writes the mean milliseconds per launch and the algorithmic
  * bytes per launch (each compulsory read and write counted once).          */
 int gpw_poisson_time_level0(gpw_poisson *ps, int64_t nbatch, int which,
@@ -273,8 +276,11 @@ int gpw_poisson_set_cluster(gpw_poisson *ps, int on);
 /* Level-0 launch plan of the float32 form (no counterpart in the
  * reference): on = 1 (default) computes the level-0 residual and restricts
  * it into level 1 (its rho and first Jacobi sweep) in one launch, without
- * storing the residual; on = 0 launches the residual and the restriction
- * separately.  The two plans compute identical values.                    */
+ * storing the residual, and (with two or more level-0 pre-sweeps) lets the
+ * second pre-sweep read the float32 defect alone and form the first
+ * sweep's iterate itself, so the float64 defect stores no iterate; on = 0
+ * launches the residual and the restriction separately and stores the
+ * first iterate.  The two plans compute identical values.                 */
 int gpw_poisson_set_fusion(gpw_poisson *ps, int on);
 
 /* Programmatic dependent launch of the V-cycle's kernels (no counterpart in
