@@ -104,7 +104,8 @@ def test_null_and_dtype_checks():
 
 def test_launch_plan_switches_validate():
     """The tuning / launch-plan switches check their arguments on the host:
-    TMA variant range, Bloch layout index, and a null engine."""
+    TMA variant range, Bloch and restriction layout indices, and a null
+    engine."""
     lib = _lib.load()
     assert lib.gpw_set_tma_variant(-2, 0) == _lib.GPW_EINVAL
     assert lib.gpw_set_tma_variant(11, 0) == _lib.GPW_EINVAL
@@ -117,6 +118,10 @@ def test_launch_plan_switches_validate():
               lib.gpw_poisson_set_fusion):
         assert f(None, 1) == _lib.GPW_EINVAL
     assert lib.gpw_bloch_launch_count() >= 0
+    assert lib.gpw_set_restrict_layout(-1) == _lib.GPW_EINVAL
+    assert lib.gpw_set_restrict_layout(4) == _lib.GPW_EINVAL
+    assert lib.gpw_set_restrict_layout(0) == _lib.GPW_OK
+    assert lib.gpw_restrict_rows_launch_count() >= 0
 
 
 def test_product_fails_loudly_without_cuda():
