@@ -21,9 +21,17 @@ sum(r^2) dv <= eps with eps = 1e-20 sum(rho^2) dv.
   cpu_baseline  the reference's own C (oracle/_ref) driven by the restated
          solver, one solve per host core in parallel, rank 0 only
 
+  single_solve  latency of the drop-in PoissonSolver.solve(phi, rho) on one
+         grid with NumPy arrays (GPAW's once-per-SCF-step call)
+
+Every timed solve runs solve()'s charge integral and branch (background shift
+or Gaussian compensation) on the device before its V-cycles.
+
 --impl reference times that CPU implementation alone, as its own arm.
-Multi-GPU (torchrun): every rank solves its own batch (weak scaling); the
-only collective is the max-over-ranks of the timings.
+Multi-GPU (one process per GPU; --gpus N without a launcher relaunches under
+torchrun): every rank solves its own batch (weak scaling) with no exchange in
+the timed region; after it, the per-solve results (V-cycles, final error,
+E_H) are all-gathered to rank 0 and the timings reduced by max.
 """
 import argparse
 import json
@@ -84,6 +92,37 @@ def reduce_max(x, dist, device):
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+RESULT_COLUMNS = ('seed', 'vcycles', 'error', 'E_H')
+
+
+def gather_results(table, dist, device):
+    """All-gather each rank's per-solve table (rows: seed, V-cycles, final
+    error sum(r^2) dv, Hartree energy) into the whole job's table, ordered by
+    rank.  Every rank has the same number of rows."""
+    table = np.ascontiguousarray(table, np.float64)
+    if dist is None:
+        return table
+    import torch
+    t = torch.from_numpy(table).to(device)
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size())]
+    dist.all_gather(parts, t)
+    return torch.cat(parts).cpu().numpy()
+
+
+def results_summary(table, rho_norms):
+    """Whole-job summary of the gathered per-solve table."""
+    rel = np.sqrt(table[:, 2] / rho_norms) if rho_norms is not None else None
+    return {'solves': int(len(table)),
+            'columns': list(RESULT_COLUMNS),
+            'vcycles_min': int(table[:, 1].min()),
+            'vcycles_max': int(table[:, 1].max()),
+            'max_rel_residual': (float(rel.max()) if rel is not None
+                                 else None),
+            'E_H_sum_Ha': float(table[:, 3].sum()),
+            'seeds_distinct': bool(len(np.unique(table[:, 0])) ==
+                                   len(table))}
 
 
 # ------------------------------------------------------------------ clocks
@@ -217,15 +256,18 @@ def run_reference(args, rank, world):
     # one round (a solve per host core) takes ~10 s on a 16-core host: the
     # sample is capped at 6 timed rounds and 1 warm-up round so that the
     # reference arm ends within a couple of minutes whatever K and W are
+    # (a step here is one such round; the line reports the rounds it timed)
     rounds, warm = max(1, min(args.steps, 6)), min(args.warmup, 1)
     r = cpu_arm(rounds, warm)
     v = float(np.mean(r['rates']))
     line = {'metric': METRIC, 'value': v, 'unit': 'solves/s', 'n_gpus': world,
-            'steps': args.steps, 'warmup': args.warmup,
+            'steps': rounds, 'warmup': warm,
+            'steps_requested': args.steps, 'warmup_requested': args.warmup,
+            'step': 'one round: a solve per host core, run concurrently',
             'ms_per_step': 1000.0 * r['cores'] / v,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
             'dtype': 'f64', 'data': 'synthetic', 'impl': 'reference',
-            'config': config_dict(args, world, r['cores']),
+            'config': config_dict(args, world, r['cores'], 'fp64'),
             'cpu_baseline': {'value': v, 'unit': 'solves/s',
                              'cores': r['cores'], 'kind': r['kind'],
                              'sample': r['sample']},
@@ -236,13 +278,14 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def config_dict(args, world, batch):
+def config_dict(args, world, batch, precision=None):
     return {'workload': 'Poisson FD multigrid, N_c=%d zero boundary (%d^3 '
                         'unknowns), h=%.2f A, nn=3 Jacobi, %d Gaussians, '
                         'relative residual %g' % (N_GRID, N_GRID - 1, H_ANG,
                                                   N_GAUSS, REL_TOL),
             'batch_per_gpu': batch, 'grid': [N_GRID - 1] * 3,
-            'precision': args.precision, 'parallelism': 'dp%d' % world,
+            'precision': precision or args.precision,
+            'parallelism': 'dp%d' % world,
             'l2': 'inputs larger than L2 (%d grids x %.1f MB per array)' %
                   (batch, (N_GRID - 1) ** 3 * 8 / 1e6)}
 
@@ -306,12 +349,27 @@ def run_ours(args, rank, world, dist):
     for _ in range(args.steps):
         phi_d.zero_()
         niters = ps.solve_batch(phi_d, rho_d, eps=eps)
-        launches += stats()[0]
+        # the engine's launches plus the charge branch's: sum, shift and
+        # (zero boundary) the Gaussian finish
+        launches += stats()[0] + 3
     e1.record(stream)
     barrier()
     clocks = clk.stop(w0, time.time())
     t_dev = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
     value = world * B * args.steps / t_dev
+
+    # ---- per-solve results of the last timed step, gathered from every rank
+    # (the path's one data collective, after the timed region)
+    from gpawdft_b200 import blas
+    seeds = shard_seed0(rank) + np.arange(B)
+    e_h = 0.5 * gd.dv * blas.vector_dots(phi_d, rho_d, B)
+    table = np.stack([seeds, np.asarray(niters, float),
+                      np.asarray(ps.last_errors, float), e_h], axis=1)
+    rho_sq = np.array([float(np.dot(r.ravel(), r.ravel())) * gd.dv
+                       for r in rho_h])
+    all_table = gather_results(table, dist, dev)
+    all_rho_sq = gather_results(rho_sq[:, None], dist, dev)[:, 0]
+    results = results_summary(all_table, all_rho_sq)
 
     # ---- end to end through the public API from pinned host memory: every
     # step's densities go host -> device and its potentials device -> host;
@@ -417,6 +475,11 @@ def run_ours(args, rank, world, dist):
                       'unit': 'solves/s', 'vcycles_mean': float(np.mean(n64))}
         del ps64
 
+    # ---- one grid per call through the drop-in PoissonSolver.solve(phi, rho)
+    # with NumPy host arrays (GPAW's once-per-SCF-step call): host wall-clock
+    # latency per call, the copies in and out included
+    single = single_solve(args, gd, rho_h[0], eps[0])
+
     # ---- live per-launch breakdown of one outer iteration (eager launches)
     breakdown = [{'launch': n, 'ms': t}
                  for n, t in ps.profile_iteration(B, reps=5)]
@@ -449,6 +512,8 @@ def run_ours(args, rank, world, dist):
            'gpu_launches': int(launches),
            'clocks': clocks,
            'vcycles': [int(x) for x in niters],
+           'results': results,
+           'single_solve': single,
            'iteration_breakdown': breakdown,
            'stencil_config_a': stencil}
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -458,6 +523,37 @@ def run_ours(args, rank, world, dist):
                                'kind': r['kind'], 'sample': r['sample']}
     if rank == 0:
         print(json.dumps(out, default=_plain), flush=True)
+
+
+def single_solve(args, gd, rho, eps, calls=10):
+    """Latency of PoissonSolver.solve(phi, rho) on one 127^3 grid with NumPy
+    arrays: each call copies rho in, runs the charge integral, the branch and
+    the device-side V-cycle loop, and copies phi back."""
+    from gpawdft_b200.poisson import PoissonSolver
+    ps1 = PoissonSolver(nn=3, relax='J', maxiter=1000,
+                        precision=args.precision, batch=1)
+    ps1.set_grid_descriptor(gd)
+    ps1.initialize()
+    phi = np.zeros_like(rho)
+    for _ in range(3):
+        phi[:] = 0.0
+        ps1.solve(phi, rho, eps=eps)
+    ts = []
+    n = None
+    for _ in range(calls):
+        phi[:] = 0.0
+        t = time.perf_counter()
+        n = ps1.solve(phi, rho, eps=eps)
+        ts.append(time.perf_counter() - t)
+    ts = np.array(ts) * 1e3
+    return {'call': 'PoissonSolver.solve(phi, rho), NumPy float64 arrays, '
+                    'one %d^3 grid, zero start' % (N_GRID - 1),
+            'precision': args.precision, 'vcycles': int(n),
+            'latency_ms_p50': float(np.median(ts)),
+            'latency_ms_max': float(ts.max()),
+            'solves_per_s': float(1e3 / ts.mean()),
+            'timer': 'host wall clock around each call (%d calls)' % calls,
+            'h2d_bytes': int(rho.nbytes), 'd2h_bytes': int(rho.nbytes)}
 
 
 def measured_peak():
@@ -833,7 +929,24 @@ def main():
          'bands96': run_bands, 'learned128': run_learned}[args.workload](args)
         return
     args.warmup = max(args.warmup, 3) if args.impl == 'ours' else args.warmup
+    if 'WORLD_SIZE' not in os.environ and args.gpus > 1:
+        # one process per GPU: relaunch this command under torchrun
+        import socket
+        so = socket.socket()
+        so.bind(('127.0.0.1', 0))
+        port = so.getsockname()[1]
+        so.close()
+        cmd = [sys.executable, '-m', 'torch.distributed.run', '--nnodes=1',
+               '--nproc-per-node', str(args.gpus), '--master-addr',
+               '127.0.0.1', '--master-port', str(port),
+               os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
     world = int(os.environ.get('WORLD_SIZE', '1'))
+    if world != args.gpus:
+        print('bench.py: --gpus %d but WORLD_SIZE=%d; launch one process per '
+              'GPU with --nproc-per-node %d' % (args.gpus, world, args.gpus),
+              file=sys.stderr)
+        sys.exit(2)
     rank = int(os.environ.get('RANK', '0'))
     dist = None
     if world > 1 and args.impl == 'ours':

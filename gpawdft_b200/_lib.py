@@ -27,7 +27,9 @@ EXPORTS = [
     'gpw_operator_get_diagonal_element', 'gpw_operator_residual',
     'gpw_operator_residual_noalloc', 'gpw_operator_free',
     'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
-    'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_add_scalar',
+    'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_dotc_pairs',
+    'gpw_add_scalar',
+    'gpw_poisson_charge_prepare', 'gpw_poisson_charge_finish',
     'gpw_poisson_new', 'gpw_poisson_solve', 'gpw_poisson_last_stats',
     'gpw_poisson_solve_async', 'gpw_poisson_collect',
     'gpw_poisson_time_level0', 'gpw_poisson_set_inner_schedule',
@@ -83,8 +85,17 @@ _SIGS = {
                                _vp, _vp, _vp]),
     'gpw_dot': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
                                _vp, _vp, _vp, _vp]),
+    'gpw_dotc_pairs': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64,
+                                      ctypes.c_int64, ctypes.c_int64, _vp,
+                                      _vp, _vp, _vp]),
     'gpw_add_scalar': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64,
                                       ctypes.c_double, _vp, _vp, _vp]),
+    'gpw_poisson_charge_prepare': (ctypes.c_int, [
+        ctypes.c_int64, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp,
+        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+        ctypes.c_int, _vp, _vp]),
+    'gpw_poisson_charge_finish': (ctypes.c_int, [
+        ctypes.c_int64, ctypes.c_int64, _vp, _vp, _vp, _vp]),
     'gpw_poisson_new': (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
                                        _vp, ctypes.c_int, ctypes.c_double,
                                        ctypes.c_int64, ctypes.POINTER(_vp)]),

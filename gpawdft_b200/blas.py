@@ -59,15 +59,50 @@ def vector_dots(x, y, nvec):
     return out.cpu().numpy()
 
 
+def pair_dots(x, nx, y, ny):
+    """out[ix, iy] = sum(conj(x[ix]) y[iy]) over (nx, n) / (ny, n) views."""
+    import torch
+    lib = _lib.load()
+    code = arrays.code_of(x)
+    if arrays.code_of(y) != code:
+        raise TypeError('integrate: both arrays need the same dtype')
+    cplx = code in (_lib.GPW_C128, _lib.GPW_C64)
+    ncomp = 2 if cplx else 1
+    n = x.numel() // nx
+    if y.numel() != ny * n:
+        raise ValueError('integrate: grid shapes differ')
+    out = torch.empty(nx * ny * ncomp, dtype=torch.float64, device='cuda')
+    _lib.check(lib.gpw_dotc_pairs(code, nx, ny, n, arrays.ptr(x),
+                                  arrays.ptr(y), arrays.ptr(out),
+                                  arrays.stream()))
+    out = out.cpu().numpy()
+    if cplx:
+        out = out[0::2] + 1j * out[1::2]
+    return out.reshape(nx, ny)
+
+
 def integrate_device(gd, a_xg, b_yg=None):
+    """gpaw/grid_descriptor.py:263-319 on the device.
+
+    ``integrate(a)`` is ``sum(a) dv`` per leading index; ``integrate(a, b)``
+    is the matrix ``sum(conj(a_x) b_y) dv`` over every pair of leading indices
+    (shape ``xshape + yshape``), a Python scalar when both are single grids.
+    When ``a is b`` the reference's rank-k update fills only one triangle; the
+    full Hermitian matrix returned here agrees with it there.
+    """
     a = arrays.to_device(a_xg)
     xshape = tuple(a.shape[:-3])
-    nvec = int(np.prod(xshape)) if xshape else 1
+    nx = int(np.prod(xshape)) if xshape else 1
     if b_yg is None:
-        r = vector_sums(a, nvec) * gd.dv
-    else:
-        b = arrays.to_device(b_yg)
-        r = vector_dots(a, b, nvec) * gd.dv
-    if not xshape:
-        return r[0].item()
-    return r.reshape(xshape)
+        r = vector_sums(a, nx) * gd.dv
+        if not xshape:
+            return r[0].item()
+        return r.reshape(xshape)
+    b = a if b_yg is a_xg else arrays.to_device(b_yg)
+    yshape = tuple(b.shape[:-3])
+    ny = int(np.prod(yshape)) if yshape else 1
+    r = pair_dots(a, nx, b, ny) * gd.dv
+    r = r.reshape(xshape + yshape)
+    if r.ndim == 0:
+        return r.item()
+    return r

@@ -404,17 +404,17 @@ int gpw_add_scalar(int dtype, int64_t n, double c, const void* x, void* y, gpw_s
 }
 
 static int reduce_common(int dtype, int op, int64_t nvec, int64_t n, const void* x, const void* y, double* out,
-                         gpw_stream stream) {
+                         gpw_stream stream, int ny = 1) {
   if (!valid_dtype(dtype) || nvec <= 0 || n <= 0 || !x || !out || nvec > 65535)
     return fail(GPW_EINVAL, "reduction: bad arguments");
   static thread_local SumScratch scratch;
   const int nblk = reduce_blocks(n);
-  const int ncomp = (op == 0 && is_complex(dtype)) ? 2 : 1;
+  const int ncomp = (op != 1 && is_complex(dtype)) ? 2 : 1;
   int rc = scratch.ensure(nvec * ncomp, nblk);
   if (rc) return rc;
   GridSum gs = scratch.gs();
   cudaStream_t st = (cudaStream_t)stream;
-  cudaError_t e = launch_reduce(dtype, op, nvec, n, x, y, gs, nblk, st);
+  cudaError_t e = launch_reduce(dtype, op, nvec, n, x, y, gs, nblk, st, ny);
   if (e != cudaSuccess) return cuda_fail(e, "reduction launch");
   e = cudaMemcpyAsync(out, gs.result, sizeof(double) * nvec * ncomp, cudaMemcpyDeviceToDevice, st);
   return e == cudaSuccess ? GPW_OK : cuda_fail(e, "reduction copy");
@@ -427,6 +427,44 @@ int gpw_sum(int dtype, int64_t nvec, int64_t n, const void* x, double* out_dev, 
 int gpw_dot(int dtype, int64_t nvec, int64_t n, const void* x, const void* y, double* out_dev, gpw_stream stream) {
   if (!y) return fail(GPW_EINVAL, "null argument");
   return reduce_common(dtype, 1, nvec, n, x, y, out_dev, stream);
+}
+
+int gpw_poisson_charge_prepare(int64_t nb, int64_t n, const double* rho, double* rho_out, double* phi,
+                               const double* rho_gauss, const double* phi_gauss, double dv, double npts_global,
+                               double maxcharge, int pbc_mask, int zero_initial_phi, double* q_dev,
+                               gpw_stream stream) {
+  if (nb <= 0 || nb > 65535 || n <= 0 || !rho || !rho_out || !phi || !q_dev || !(dv > 0) || !(npts_global > 0))
+    return fail(GPW_EINVAL, "charge_prepare: bad arguments");
+  if (rho_out == rho) return fail(GPW_EINVAL, "charge_prepare: rho_out must not alias rho");
+  if ((rho_gauss == nullptr) != (phi_gauss == nullptr))
+    return fail(GPW_EINVAL, "charge_prepare: give both Gaussian arrays or neither");
+  static thread_local SumScratch scratch;
+  const int nblk = reduce_blocks(n);
+  int rc = scratch.ensure(nb, nblk);
+  if (rc) return rc;
+  GridSum gs = scratch.gs();
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = launch_reduce(GPW_F64, 0, nb, n, rho, nullptr, gs, nblk, st);
+  if (e != cudaSuccess) return cuda_fail(e, "charge_prepare: reduction");
+  const int all_p = (pbc_mask & 7) == 7, any_p = (pbc_mask & 7) != 0;
+  e = launch_charge_prepare(nb, n, rho, rho_out, phi, rho_gauss, phi_gauss, gs.result, dv, npts_global, maxcharge,
+                            all_p, any_p, zero_initial_phi, q_dev, st);
+  return e == cudaSuccess ? GPW_OK : cuda_fail(e, "charge_prepare");
+}
+
+int gpw_poisson_charge_finish(int64_t nb, int64_t n, double* phi, const double* phi_gauss, const double* q_dev,
+                              gpw_stream stream) {
+  if (nb <= 0 || nb > 65535 || n <= 0 || !phi || !q_dev) return fail(GPW_EINVAL, "charge_finish: bad arguments");
+  if (!phi_gauss) return GPW_OK;
+  cudaError_t e = launch_charge_finish(nb, n, phi, phi_gauss, q_dev, (cudaStream_t)stream);
+  return e == cudaSuccess ? GPW_OK : cuda_fail(e, "charge_finish");
+}
+
+int gpw_dotc_pairs(int dtype, int64_t nx, int64_t ny, int64_t n, const void* x, const void* y, double* out_dev,
+                   gpw_stream stream) {
+  if (!y) return fail(GPW_EINVAL, "null argument");
+  if (nx <= 0 || ny <= 0 || nx * ny > 65535) return fail(GPW_EINVAL, "dotc_pairs: 1 <= nx * ny <= 65535");
+  return reduce_common(dtype, 2, nx * ny, n, x, y, out_dev, stream, (int)ny);
 }
 
 }  // extern "C"

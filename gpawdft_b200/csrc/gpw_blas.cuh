@@ -56,16 +56,19 @@ __global__ void add_scalar_kernel(int64_t n, double c, const S* __restrict__ x, 
   for (; i < n; i += stride) y[i] = x[i] + (S)c;
 }
 
-// Segmented sum / dot: vector m = blockIdx.y, CTAs of one vector = gridDim.x.
-// OP 0: sum(x) (real; complex -> real and imaginary in two segments),
-// OP 1: sum(conj(x) y) real part.
+// Segmented sum / dot: segment m = blockIdx.y, CTAs of one segment = gridDim.x.
+// OP 0: sum(x[m]) (real; complex -> real and imaginary in two segments),
+// OP 1: real part of sum(conj(x[m]) y[m]),
+// OP 2: sum(conj(x[m / ny]) y[m % ny]) over every (x, y) vector pair; complex
+//       results take two segments (real, imaginary).
 template <typename T, int OP>
 __global__ void __launch_bounds__(256) reduce_kernel(int64_t n, const T* __restrict__ x,
-                                                     const T* __restrict__ y, GridSum gs, int ncomp) {
+                                                     const T* __restrict__ y, GridSum gs, int ncomp,
+                                                     int ny) {
   __shared__ double red[32];
   const int m = blockIdx.y;
-  const T* xv = x + (int64_t)m * n;
-  const T* yv = y ? y + (int64_t)m * n : nullptr;
+  const T* xv = x + (int64_t)(OP == 2 ? m / ny : m) * n;
+  const T* yv = y ? y + (int64_t)(OP == 2 ? m % ny : m) * n : nullptr;
   double s0 = 0.0, s1 = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     if constexpr (OP == 0) {
@@ -77,7 +80,9 @@ __global__ void __launch_bounds__(256) reduce_kernel(int64_t n, const T* __restr
       }
     } else {
       if constexpr (EltTraits<T>::cpx) {
-        s0 += (double)xv[i].x * yv[i].x + (double)xv[i].y * yv[i].y;
+        const double xr = xv[i].x, xi = xv[i].y, yr = yv[i].x, yi = yv[i].y;
+        s0 += xr * yr + xi * yi;
+        if constexpr (OP == 2) s1 += xr * yi - xi * yr;
       } else {
         s0 += (double)xv[i] * (double)yv[i];
       }
@@ -90,6 +95,63 @@ __global__ void __launch_bounds__(256) reduce_kernel(int64_t n, const T* __restr
     double t1 = block_sum(s1, red);
     grid_sum_finish(gs, m * ncomp + 1, blockIdx.x, gridDim.x, t1, red);
   }
+}
+
+// The charge branches of PoissonSolver.solve (gpaw/poisson.py:209-299) for
+// a batch of float64 densities, member b = blockIdx.y, after its sum(rho) is
+// in sums[b]:
+//   |charge| <= maxcharge, or every axis periodic:
+//        rho_out = rho - charge / dv / npts            (the background shift)
+//        (charged periodic with zero_phi: phi = 0)
+//   charged, no periodic axis, Gaussians given:
+//        q = charge / sqrt(4 pi); rho_out = rho - q rho_gauss;
+//        phi = 0 (zero_phi) or phi - q phi_gauss       (poisson.py:286-293)
+//   charged with mixed boundaries: q = NaN, rho_out = rho (the caller raises).
+// charge = sums[b] dv; q_out[b] receives q (0 outside the Gaussian branch).
+// The NumPy expressions are rounded as NumPy rounds them (no contraction);
+// the axpy on phi fuses, as the BLAS axpy it replaces may.
+__global__ void charge_prepare_kernel(int64_t n, const double* __restrict__ rho, double* __restrict__ rho_out,
+                                      double* __restrict__ phi, const double* __restrict__ rho_g,
+                                      const double* __restrict__ phi_g, const double* __restrict__ sums,
+                                      double dv, double npts, double maxcharge, int all_periodic,
+                                      int any_periodic, int zero_phi, double* __restrict__ q_out) {
+  const int b = blockIdx.y;
+  const double charge = __dmul_rn(sums[b], dv);
+  int mode;  // 0 background shift, 1 Gaussian, 2 unsupported
+  if (fabs(charge) <= maxcharge || all_periodic) mode = 0;
+  else if (!any_periodic && rho_g && phi_g) mode = 1;
+  else mode = 2;
+  const double bg = __ddiv_rn(__ddiv_rn(charge, dv), npts);
+  const double q = __ddiv_rn(charge, sqrt(4.0 * 3.14159265358979323846));
+  const bool clear_phi = zero_phi && fabs(charge) > maxcharge && mode != 2;
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    q_out[b] = mode == 1 ? q : (mode == 2 ? __longlong_as_double(0x7ff8000000000000LL) : 0.0);
+  const double* r = rho + (int64_t)b * n;
+  double* ro = rho_out + (int64_t)b * n;
+  double* ph = phi + (int64_t)b * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (mode == 0) {
+      ro[i] = __dsub_rn(r[i], bg);
+      if (clear_phi) ph[i] = 0.0;
+    } else if (mode == 1) {
+      ro[i] = __dsub_rn(r[i], __dmul_rn(q, rho_g[i]));
+      ph[i] = clear_phi ? 0.0 : fma(-q, phi_g[i], ph[i]);
+    } else {
+      ro[i] = r[i];
+    }
+  }
+}
+
+// phi[b] += q[b] phi_gauss for the members of the Gaussian branch
+// (gpaw/poisson.py:298-299).
+__global__ void charge_finish_kernel(int64_t n, double* __restrict__ phi, const double* __restrict__ phi_g,
+                                     const double* __restrict__ q_in) {
+  const int b = blockIdx.y;
+  const double q = q_in[b];
+  if (!(q != 0.0) || isnan(q)) return;
+  double* ph = phi + (int64_t)b * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    ph[i] = fma(q, phi_g[i], ph[i]);
 }
 
 // Fill `n` elements with zero (used for phi_{l+1} = 0 inside captured graphs

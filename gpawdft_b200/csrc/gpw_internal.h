@@ -167,8 +167,14 @@ cudaError_t launch_cluster_vcycle(const ClusterArgs& a, size_t smem, int nbatch,
 cudaError_t launch_axpy(int dtype, int64_t n, double ar, double ai, const void* x, void* y, cudaStream_t st);
 cudaError_t launch_scal(int dtype, int64_t n, double ar, double ai, void* x, cudaStream_t st);
 cudaError_t launch_reduce(int dtype, int op, int64_t nvec, int64_t n, const void* x, const void* y,
-                          const GridSum& gs, int nblk, cudaStream_t st);
+                          const GridSum& gs, int nblk, cudaStream_t st, int ny = 1);
 int reduce_blocks(int64_t n);
+cudaError_t launch_charge_prepare(int64_t nb, int64_t n, const double* rho, double* rho_out, double* phi,
+                                  const double* rho_g, const double* phi_g, const double* sums, double dv,
+                                  double npts, double maxcharge, int all_periodic, int any_periodic, int zero_phi,
+                                  double* q_out, cudaStream_t st);
+cudaError_t launch_charge_finish(int64_t nb, int64_t n, double* phi, const double* phi_g, const double* q,
+                                 cudaStream_t st);
 cudaError_t launch_add_scalar(int dtype, int64_t n, double c, const void* x, void* y, cudaStream_t st);
 cudaError_t launch_zero(int dtype, const GridView& v, void* x, int nbatch, const unsigned char* active,
                         cudaStream_t st);

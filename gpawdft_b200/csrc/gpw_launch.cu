@@ -1016,28 +1016,39 @@ int reduce_blocks(int64_t n) {
 }
 
 cudaError_t launch_reduce(int dtype, int op, int64_t nvec, int64_t n, const void* x, const void* y,
-                          const GridSum& gs, int nblk, cudaStream_t st) {
+                          const GridSum& gs, int nblk, cudaStream_t st, int ny) {
   dim3 grid(nblk, (unsigned)nvec);
-  const int ncomp = (op == 0 && is_complex(dtype)) ? 2 : 1;
+  const int ncomp = (op != 1 && is_complex(dtype)) ? 2 : 1;
+#define GPW_REDUCE_CASE(T)                                                                              \
+  if (op == 0) reduce_kernel<T, 0><<<grid, 256, 0, st>>>(n, (const T*)x, nullptr, gs, ncomp, ny);       \
+  else if (op == 1) reduce_kernel<T, 1><<<grid, 256, 0, st>>>(n, (const T*)x, (const T*)y, gs, ncomp, ny); \
+  else reduce_kernel<T, 2><<<grid, 256, 0, st>>>(n, (const T*)x, (const T*)y, gs, ncomp, ny);
   switch (dtype) {
-    case GPW_F64:
-      if (op == 0) reduce_kernel<double, 0><<<grid, 256, 0, st>>>(n, (const double*)x, nullptr, gs, ncomp);
-      else reduce_kernel<double, 1><<<grid, 256, 0, st>>>(n, (const double*)x, (const double*)y, gs, ncomp);
-      break;
-    case GPW_F32:
-      if (op == 0) reduce_kernel<float, 0><<<grid, 256, 0, st>>>(n, (const float*)x, nullptr, gs, ncomp);
-      else reduce_kernel<float, 1><<<grid, 256, 0, st>>>(n, (const float*)x, (const float*)y, gs, ncomp);
-      break;
-    case GPW_C128:
-      if (op == 0) reduce_kernel<double2, 0><<<grid, 256, 0, st>>>(n, (const double2*)x, nullptr, gs, ncomp);
-      else reduce_kernel<double2, 1><<<grid, 256, 0, st>>>(n, (const double2*)x, (const double2*)y, gs, ncomp);
-      break;
-    case GPW_C64:
-      if (op == 0) reduce_kernel<float2, 0><<<grid, 256, 0, st>>>(n, (const float2*)x, nullptr, gs, ncomp);
-      else reduce_kernel<float2, 1><<<grid, 256, 0, st>>>(n, (const float2*)x, (const float2*)y, gs, ncomp);
-      break;
+    case GPW_F64: GPW_REDUCE_CASE(double) break;
+    case GPW_F32: GPW_REDUCE_CASE(float) break;
+    case GPW_C128: GPW_REDUCE_CASE(double2) break;
+    case GPW_C64: GPW_REDUCE_CASE(float2) break;
     default: return cudaErrorInvalidValue;
   }
+#undef GPW_REDUCE_CASE
+  return cudaGetLastError();
+}
+
+cudaError_t launch_charge_prepare(int64_t nb, int64_t n, const double* rho, double* rho_out, double* phi,
+                                  const double* rho_g, const double* phi_g, const double* sums, double dv,
+                                  double npts, double maxcharge, int all_periodic, int any_periodic, int zero_phi,
+                                  double* q_out, cudaStream_t st) {
+  const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 2LL * num_sms()));
+  charge_prepare_kernel<<<dim3(gx, (unsigned)nb), 256, 0, st>>>(n, rho, rho_out, phi, rho_g, phi_g, sums, dv, npts,
+                                                                 maxcharge, all_periodic, any_periodic, zero_phi,
+                                                                 q_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_charge_finish(int64_t nb, int64_t n, double* phi, const double* phi_g, const double* q,
+                                 cudaStream_t st) {
+  const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 2LL * num_sms()));
+  charge_finish_kernel<<<dim3(gx, (unsigned)nb), 256, 0, st>>>(n, phi, phi_g, q);
   return cudaGetLastError();
 }
 

@@ -9,7 +9,8 @@
 // variant keeps those partial sums in a fixed array compiled into the
 // library instead, so a call allocates nothing.
 //
-// The array (g_noalloc_scratch, NOALLOC_BYTES bytes, ~272 KB) exists once per
+// The array (g_noalloc_scratch, NOALLOC_BYTES = 540,672 bytes, about 528 KB:
+// 65,536 double partial sums plus 4,096 unsigned counters) exists once per
 // GPU that loads the library and stays resident until the process exits.
 // Its device address is looked up with cudaGetSymbolAddress the first time
 // the entry point runs on a device (with that device current); that first
@@ -34,10 +35,11 @@ using namespace gpw;
 namespace {
 
 // Limits of one call: CTAs of the reduction over all `nin` grids, and nin.
-constexpr int64_t NOALLOC_MAX_PARTIALS = 1 << 16;  // doubles (512 KB of blocks x grids)
+constexpr int64_t NOALLOC_MAX_PARTIALS = 1 << 16;  // doubles: 512 KiB of partial sums (blocks x grids)
 constexpr int64_t NOALLOC_MAX_NIN = 4096;          // grids per call (one counter each)
 constexpr size_t NOALLOC_BYTES =
     (size_t)NOALLOC_MAX_PARTIALS * sizeof(double) + (size_t)NOALLOC_MAX_NIN * sizeof(unsigned);
+static_assert(NOALLOC_BYTES == 540672, "the documented size of the fixed scratch is 540,672 bytes");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 

@@ -105,7 +105,7 @@ class GridDescriptor:
         return arrays.empty_like_device(self._shape(n), dtype)
 
     def integrate(self, a_xg, b_yg=None, global_integral=True):
-        """gpaw/grid_descriptor.py:263-319: sum(a) dv, or Re sum(conj(a) b) dv.
+        """gpaw/grid_descriptor.py:263-319: sum(a) dv, or sum(conj(a_x) b_y) dv.
 
         Reduced on the device by the library's deterministic kernels (NumPy
         inputs are copied there first).

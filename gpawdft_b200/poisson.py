@@ -298,12 +298,24 @@ class FDPoissonSolver:
             eps = self.eps
         phi_d = arrays.to_device(phi)
         rho_d = arrays.to_device(rho)
-        actual_charge = self.gd.integrate(rho_d)
-        background = (actual_charge / self.gd.dv /
-                      self.gd.get_size_of_global_array().prod())
         if self.remove_moment:
             raise NotImplementedError('remove_moment is not part of this '
                                       'build')
+        if charge is None and not (self.use_charge_center and
+                                   not self.gd.pbc_c.any()):
+            # the charge integral and the branch run on the device: no host
+            # round trip before the solve
+            phi_b, rho_b = phi_d.unsqueeze(0), rho_d.unsqueeze(0)
+            rho_n, q = self._charge_prepare(phi_b, rho_b, 1, maxcharge,
+                                            zero_initial_phi, 0)
+            niter = int(self._run(phi_b, rho_n, 1, [eps])[0])
+            self._charge_finish(phi_b, 1, q)
+            if not arrays.is_device(phi):
+                arrays.writeback(phi, phi_d)
+            return niter
+        actual_charge = self.gd.integrate(rho_d)
+        background = (actual_charge / self.gd.dv /
+                      self.gd.get_size_of_global_array().prod())
         if charge is None:
             charge = actual_charge
         if abs(charge) <= maxcharge:
@@ -438,29 +450,84 @@ class FDPoissonSolver:
             self._engine[0], nb, ms.ctypes.data, arrays.stream()))
         return ms
 
-    def solve_batch(self, phi_b, rho_b, eps=None):
-        """Independent neutral solves of a batch (nb, *n_c) on one grid.
+    def solve_batch(self, phi_b, rho_b, eps=None, maxcharge=1e-6,
+                    zero_initial_phi=False):
+        """``solve(phi, rho)`` of every member of a batch (nb, *n_c) on one grid.
 
-        Each solve stops at its own ``error <= eps``; results and V-cycle
-        counts equal those of solving each grid alone.  Returns the per-solve
-        iteration counts.
+        Each member goes through the charge branches of ``solve``
+        (gpaw/poisson.py:209-299: the charge integral, then the background
+        shift or the Gaussian compensation), on the device with no host
+        round trip, and stops at its own ``error <= eps``; results and
+        V-cycle counts equal those of solving each grid alone.  Returns the
+        per-solve iteration counts.
         """
         if self._engine is None:
             self.initialize()
         nb = int(phi_b.shape[0])
         if eps is None:
             eps = self.eps
+        if self.use_charge_center and not self.gd.pbc_c.any():
+            # the Gaussian's centre depends on each member's charge
+            return np.array([self.solve(phi_b[b], rho_b[b], eps=np.broadcast_to(
+                np.asarray(eps, float), (nb,))[b], maxcharge=maxcharge,
+                zero_initial_phi=zero_initial_phi) for b in range(nb)])
         eps_list = np.broadcast_to(np.asarray(eps, float), (nb,))
         phi_d = arrays.to_device(phi_b)
         rho_d = arrays.to_device(rho_b)
-        niter = self._run(phi_d, rho_d, nb, eps_list)
+        rho_n, q = self._charge_prepare(phi_d, rho_d, nb, maxcharge,
+                                        zero_initial_phi, 0)
+        niter = self._run(phi_d, rho_n, nb, eps_list)
+        self._charge_finish(phi_d, nb, q)
         if not arrays.is_device(phi_b):
             arrays.writeback(phi_b, phi_d)
         return niter
 
+    def _charge_prepare(self, phi_d, rho_d, nb, maxcharge, zero_initial_phi,
+                        slot):
+        """Device charge branches of ``solve`` for a batch: returns the
+        density the neutral solve uses and the per-member Gaussian moments."""
+        import torch
+        if not self.gd.pbc_c.any():
+            self.load_gauss()
+            rg, pg = arrays.ptr(self.rho_gauss), arrays.ptr(self.phi_gauss)
+        else:
+            rg = pg = None
+        shape = (nb,) + tuple(int(x) for x in self.gd.n_c)
+        bufs = getattr(self, '_charge_bufs', None)
+        if bufs is None or bufs[0].shape[0] < nb:
+            rows = max(nb, self._engine[1] if self._engine else 1)
+            bufs = (torch.empty((rows,) + shape[1:], dtype=torch.float64,
+                                device=rho_d.device),
+                    torch.empty((2, rows), dtype=torch.float64,
+                                device=rho_d.device))
+            self._charge_bufs = bufs
+        rho_n = bufs[0][:nb]
+        q = bufs[1][slot, :nb]
+        pbc = sum(1 << c for c in range(3) if self.gd.pbc_c[c])
+        npts = float(np.prod(self.gd.get_size_of_global_array()))
+        _lib.check(self._lib.gpw_poisson_charge_prepare(
+            nb, int(np.prod(shape[1:])), arrays.ptr(rho_d), arrays.ptr(rho_n),
+            arrays.ptr(phi_d), rg, pg, float(self.gd.dv), npts,
+            float(maxcharge), pbc, int(bool(zero_initial_phi)), arrays.ptr(q),
+            arrays.stream()))
+        if self.gd.pbc_c.any() and not self.gd.pbc_c.all():
+            # only a mixed-boundary grid can meet the unsupported branch
+            if torch.isnan(q).any().item():
+                raise NotImplementedError('Charged systems with mixed '
+                                          'periodic/zero boundary conditions')
+        return rho_n, q
+
+    def _charge_finish(self, phi_d, nb, q):
+        if self.gd.pbc_c.any():
+            return
+        _lib.check(self._lib.gpw_poisson_charge_finish(
+            nb, int(np.prod(self.gd.n_c)), arrays.ptr(phi_d),
+            arrays.ptr(self.phi_gauss), arrays.ptr(q), arrays.stream()))
+
     def solve_stream(self, rhos, phis=None, eps=None, out=None):
-        """Independent neutral solves of a sequence of host batches, each
-        (nb, *n_c) float64, with the host<->device transfers overlapped with
+        """``solve_batch`` of a sequence of host batches, each (nb, *n_c)
+        float64 (charge branches included), with the host<->device transfers
+        overlapped with
         the solves: while batch k is solved, batch k+1's densities travel to
         the device and batch k-1's potentials back (two device slots, one
         copy stream per direction).
@@ -548,15 +615,21 @@ class FDPoissonSolver:
                 phi_d[s].zero_()
             if k - 2 in pending:
                 collect(k - 2)
-            if use_async and not self._solve_async(phi_d[s], rho_d[s], nb,
-                                                   eps_a, s):
-                use_async = False   # no device-side loop here: solve in turn
-            if not use_async:
+            if use_async:
+                rho_n, q = self._charge_prepare(phi_d[s], rho_d[s], nb, 1e-6,
+                                                False, s)
+                if not self._solve_async(phi_d[s], rho_n, nb, eps_a, s):
+                    # no device-side loop here: this batch and the rest are
+                    # solved in turn
+                    use_async = False
+                    niters[k] = self._run(phi_d[s], rho_n, nb, eps_a)
+                self._charge_finish(phi_d[s], nb, q)
+            elif niters[k] is None:
                 niters[k] = self.solve_batch(phi_d[s], rho_d[s], eps=eps)
             done = torch.cuda.Event()
             done.record(compute)
             rho_free[s] = done
-            if use_async:
+            if use_async and niters[k] is None:
                 pending[k] = (done, s)
             with torch.cuda.stream(down):
                 down.wait_event(done)

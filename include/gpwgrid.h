@@ -103,8 +103,8 @@ int gpw_operator_get_diagonal_element(const gpw_operator *op, double *out);
 
 /* Fused residual r = A func - source and sum |r|^2 (new; replaces the
  * apply + `residual -= rho` + np.dot sequence of gpaw/poisson.py:357-361).
- * r may be NULL (norm only).  *sumsq_dev is a device double receiving the
- * deterministic sum over all `nin` grids.                                  */
+ * r may be NULL (norm only).  sumsq_dev points to `nin` device doubles;
+ * each receives its grid's sum |r|^2, reduced in a fixed order.            */
 int gpw_operator_residual(gpw_operator *op, int dtype, const void *func,
                           const void *source, void *r, int64_t nin,
                           double *sumsq_dev, gpw_stream stream);
@@ -113,7 +113,8 @@ int gpw_operator_residual(gpw_operator *op, int dtype, const void *func,
  * For callers that must not allocate device memory during a call -- code
  * running inside another framework's memory pool or allocator hook, or a
  * process that reserves all device memory up front: the partial sums of the
- * norm reduction live in a fixed ~272 KB array compiled into the library
+ * norm reduction live in a fixed 540,672-byte (~528 KB) array compiled into
+ * the library
  * (resident on every GPU that loads it until exit) instead of a workspace
  * grown with cudaMalloc.  Same arguments and results as
  * gpw_operator_residual.  Limits: nin <= 4096 grids and at most 65536
@@ -167,11 +168,40 @@ int gpw_sum(int dtype, int64_t nvec, int64_t n, const void *x, double *out_dev,
 /* out[m] = sum_i conj(x[m, i]) y[m, i] (real part only for complex).        */
 int gpw_dot(int dtype, int64_t nvec, int64_t n, const void *x, const void *y,
             double *out_dev, gpw_stream stream);
+/* gd.integrate(a_xg, b_yg), gpaw/grid_descriptor.py:294-319 (the gemm with
+ * transa 'c' it calls): out[ix * ny + iy] = sum_i conj(x[ix, i]) y[iy, i] for
+ * every pair of nx x-vectors and ny y-vectors of length n.  Real dtypes give
+ * one double per pair, complex dtypes a (re, im) pair.  nx * ny <= 65535.
+ * Deterministic order.                                                      */
+int gpw_dotc_pairs(int dtype, int64_t nx, int64_t ny, int64_t n, const void *x,
+                   const void *y, double *out_dev, gpw_stream stream);
 /* y = x + c (real dtypes, c added to every element)                         */
 int gpw_add_scalar(int dtype, int64_t n, double c, const void *x, void *y,
                    gpw_stream stream);
 
 /* ------------------------------------------------------------ Poisson */
+
+/* The charge branches of PoissonSolver.solve, gpaw/poisson.py:209-299, for
+ * nb float64 (rho, phi) pairs of n points each, on the device with no host
+ * round trip: charge = sum(rho) dv; neutral (|charge| <= maxcharge) or all
+ * axes periodic: rho_out = rho - charge / dv / npts_global (charged periodic
+ * with zero_initial_phi: phi = 0); charged with no periodic axis and the
+ * Gaussian arrays given: q = charge / sqrt(4 pi), rho_out = rho - q rho_gauss,
+ * phi -= q phi_gauss (or phi = 0).  q_dev[b] receives q (0 outside the
+ * Gaussian branch; NaN for a charged member with mixed boundaries, which
+ * the caller reports as the reference's NotImplementedError).  pbc_mask bit
+ * c set = axis c periodic.  After the neutral solve on rho_out,
+ * gpw_poisson_charge_finish adds q phi_gauss back (poisson.py:298-299).     */
+int gpw_poisson_charge_prepare(int64_t nb, int64_t n, const double *rho,
+                               double *rho_out, double *phi,
+                               const double *rho_gauss,
+                               const double *phi_gauss, double dv,
+                               double npts_global, double maxcharge,
+                               int pbc_mask, int zero_initial_phi,
+                               double *q_dev, gpw_stream stream);
+int gpw_poisson_charge_finish(int64_t nb, int64_t n, double *phi,
+                              const double *phi_gauss, const double *q_dev,
+                              gpw_stream stream);
 
 /* Multigrid engine behind FDPoissonSolver (gpaw/poisson.py:61-366).  The
  * level hierarchy is the one gpaw/poisson.py:91-132 builds: operators[0..L]

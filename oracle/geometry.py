@@ -78,12 +78,26 @@ class GridDescriptor:
         return np.empty(tuple(n) + tuple(self.n_c), dtype)
 
     def integrate(self, a_xg, b_yg=None):
-        """gpaw/grid_descriptor.py:263-319 (one-array form and the a*b dot)."""
+        """gpaw/grid_descriptor.py:263-319 (serial).
+
+        One array: ``sum(a) dv`` per leading index.  Two arrays: the matrix
+        ``dv * B_y . conj(A_x)`` that the gemm call at :306 forms, returned
+        transposed to ``xshape + yshape`` (:312-319), a scalar for two grids.
+        """
+        xshape = a_xg.shape[:-3]
         if b_yg is None:
-            xshape = a_xg.shape[:-3]
             r = a_xg.reshape(xshape + (-1,)).sum(axis=-1) * self.dv
             return r
-        return np.vdot(a_xg.ravel(), b_yg.ravel()) * self.dv
+        A_xg = np.ascontiguousarray(a_xg.reshape((-1,) + a_xg.shape[-3:]))
+        B_yg = np.ascontiguousarray(b_yg.reshape((-1,) + b_yg.shape[-3:]))
+        A = A_xg.reshape(len(A_xg), -1)
+        B = B_yg.reshape(len(B_yg), -1)
+        result_yx = self.dv * np.dot(B, A.conj().T)
+        yshape = b_yg.shape[:-3]
+        result = result_yx.T.reshape(xshape + yshape)
+        if result.ndim == 0:
+            return result.item()
+        return result
 
     def get_grid_point_coordinates(self):
         """gpaw/grid_descriptor.py:629-636."""

@@ -11,7 +11,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, '_ref')
-REF_TREE = '/root/reference'
+# the reference source tree (only where it is mounted; never on GPU boxes)
+REF_TREE = os.environ.get('GPAW_REFERENCE_TREE', '/root/reference')
 
 
 def available(omp=False):

@@ -24,7 +24,7 @@ def solvers(N, L, pbc, **kw):
     ps = PoissonSolver(**kw)
     ps.set_grid_descriptor(gd)
     ps.initialize()
-    ops = ol.PoissonSolver(**kw)
+    ops = ol.PoissonSolver(**{k: v for k, v in kw.items() if k != 'batch'})
     ops.set_grid_descriptor(ogd)
     ops.initialize()
     return gd, ogd, ps, ops
@@ -88,12 +88,13 @@ def test_charged_zero_boundary(cuda, center):
     ogd0 = OGD((N,) * 3, (a,) * 3, 0)
     rho = OGauss(ogd0, a=19, center=(a / 2, a / 2, 3 * a / 4)).get_gauss(0)
     gd, ogd, ps, ops = solvers(N, a, 0, nn=3, use_charge_center=center)
-    phi = gd.zeros()
-    n = ps.solve(phi, rho, charge=1.0)
-    ophi = ogd.zeros()
-    on = ops.solve(ophi, rho, charge=1.0)
-    assert n == on
-    assert np.abs(phi - ophi).max() < 1e-6 * np.abs(ophi).max()
+    for charge in (1.0, None):
+        phi = gd.zeros()
+        n = ps.solve(phi, rho, charge=charge)
+        ophi = ogd.zeros()
+        on = ops.solve(ophi, rho, charge=charge)
+        assert n == on
+        assert np.abs(phi - ophi).max() < 1e-6 * np.abs(ophi).max()
 
 
 def test_gauss_seidel_solver(cuda):
@@ -124,9 +125,41 @@ def test_batch_equals_single(cuda):
     nb = ps.solve_batch(phib, np.array(rhos), eps=2e-10)
     for s in range(3):
         phi = gd.zeros()
-        n = ps.solve_neutral(phi, rhos[s], eps=2e-10)
+        n = ps.solve(phi, rhos[s], eps=2e-10)
         assert n == nb[s]
         assert np.array_equal(phi, phib[s])
+
+
+@pytest.mark.parametrize('pbc', [0, 1])
+def test_batch_charge_branches(cuda, pbc):
+    """solve_batch runs solve()'s charge branches per member on the device
+    (gpaw/poisson.py:209-299): a neutral member (background shift), charged
+    members (Gaussian compensation on a zero-boundary grid, homogeneous
+    background on a periodic one).  Each member equals solve() of it alone,
+    and both follow the oracle."""
+    N = 32
+    rhos = []
+    for s in range(3):
+        rho, L = gaussian_density(N, 0.25, 4 + 2 * s, 70 + s, pbc=bool(pbc))
+        rhos.append(rho)
+    gd, ogd, ps, ops = solvers(N, L, pbc, nn=3, relax='J', eps=1e-14,
+                               batch=3)
+    rhos[1] = rhos[1] + 0.02 * (1 if pbc else np.exp(
+        -((np.indices(rhos[1].shape) - 15.0) ** 2).sum(0) / 20.0))
+    rhos[2] = rhos[2] - 0.01
+    assert abs(gd.integrate(rhos[0])) <= 1e-6
+    assert abs(gd.integrate(rhos[1])) > 1e-6
+    phib = np.zeros((3,) + tuple(gd.n_c))
+    nb = ps.solve_batch(phib, np.array(rhos))
+    for s in range(3):
+        phi = gd.zeros()
+        n = ps.solve(phi, rhos[s])
+        assert n == nb[s]
+        assert np.array_equal(phi, phib[s])
+        ophi = ogd.zeros()
+        on = ops.solve(ophi, rhos[s])
+        assert abs(n - on) <= 1
+        assert np.abs(phi - ophi).max() < 1e-7 * np.abs(ophi).max()
 
 
 def test_fp32_defect_correction(cuda):
@@ -191,7 +224,7 @@ def test_fp32_batch_equals_single(cuda):
     nb = ps.solve_batch(phib, np.array(rhos), eps=eps)
     for s in range(3):
         phi = gd.zeros()
-        n = ps.solve_neutral(phi, rhos[s], eps=eps[s])
+        n = ps.solve(phi, rhos[s], eps=eps[s])
         assert n == nb[s]
         assert np.array_equal(phi, phib[s])
 
