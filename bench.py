@@ -828,7 +828,8 @@ def run_learned(args):
 
 def run_bands(args):
     """256 complex Bloch bands on a 96^3 periodic grid (h = 0.18 A, random k,
-    phase-wrapped halos): Laplace nn=3 (scale -1/2), Gradient x/y/z n=3,
+    phase-wrapped halos): Laplace nn=3 (scale -1/2), the same kinetic
+    operator fused with a local potential, Gradient x/y/z n=3,
     restriction / interpolation nn=3 96^3 <-> 48^3, complex128 and complex64.
     GB/s of algorithmic bytes (input read once + output written once)."""
     import torch
@@ -869,7 +870,19 @@ def run_bands(args):
             gbs = 2 * a.numel() * es / t / 1e9
             res['%s_%s' % (name, nm)] = {'ms': t * 1e3, 'GB/s': gbs,
                                          'frac': gbs / peak}
-        del o
+        # kinetic + local potential in one pass (gpaw/wavefunctions/fd.py:
+        # 77-80): every band read once and written once, the potential
+        # (one grid) read once
+        vt = torch.randn((96, 96, 96), device='cuda', generator=g,
+                         dtype=torch.float64 if name == 'c128'
+                         else torch.float32)
+        kin = ops[0][1]
+        t = timeit(lambda: kin.apply_potential(a, o, vt, ph), args.steps)
+        gbs = (2 * a.numel() * es + vt.numel() * vt.element_size()) / t / 1e9
+        res['%s_kinetic_potential' % name] = {
+            'ms': t * 1e3, 'GB/s': gbs, 'frac': gbs / peak,
+            'vs_laplace_alone': t * 1e3 / res['%s_laplace' % name]['ms']}
+        del o, vt
         R = Transformer(gd, gc, 3, dt)
         Ip = Transformer(gc, gd, 3, dt)
         c = R.apply(a, None, ph)

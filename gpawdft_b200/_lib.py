@@ -23,7 +23,8 @@ GPW_F64, GPW_C128, GPW_F32, GPW_C64 = 0, 1, 2, 3
 # every symbol include/gpwgrid.h declares
 EXPORTS = [
     'gpw_last_error', 'gpw_version',
-    'gpw_operator_new', 'gpw_operator_apply', 'gpw_operator_relax',
+    'gpw_operator_new', 'gpw_operator_apply', 'gpw_operator_apply_potential',
+    'gpw_operator_relax',
     'gpw_operator_get_diagonal_element', 'gpw_operator_residual',
     'gpw_operator_residual_noalloc', 'gpw_operator_free',
     'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
@@ -60,6 +61,9 @@ _SIGS = {
                                         ctypes.c_int, ctypes.POINTER(_vp)]),
     'gpw_operator_apply': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp,
                                           ctypes.c_int64, _vp, _vp]),
+    'gpw_operator_apply_potential': (ctypes.c_int, [_vp, ctypes.c_int, _vp,
+                                                    _vp, ctypes.c_int64, _vp,
+                                                    _vp, _vp]),
     'gpw_operator_relax': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int,
                                           _vp, _vp, ctypes.c_int64,
                                           ctypes.c_int, ctypes.c_double,

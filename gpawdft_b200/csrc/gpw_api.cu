@@ -214,8 +214,8 @@ int gpw_operator_get_diagonal_element(const gpw_operator* op, double* out) {
   return GPW_OK;
 }
 
-int gpw_operator_apply(gpw_operator* op, int dtype, const void* in, void* out, int64_t nin, const double* phases,
-                       gpw_stream stream) {
+static int operator_apply(gpw_operator* op, int dtype, const void* in, void* out, int64_t nin, const double* phases,
+                          const void* pot, gpw_stream stream) {
   if (!op || !in || !out) return fail(GPW_EINVAL, "null argument");
   if (!valid_dtype(dtype)) return fail(GPW_EINVAL, "bad dtype");
   if (nin < 0) return fail(GPW_EINVAL, "nin < 0");
@@ -224,10 +224,10 @@ int gpw_operator_apply(gpw_operator* op, int dtype, const void* in, void* out, i
     // grid.z = nchunk * nbatch; split very large batches
     const int64_t half = nin / 2;
     const size_t es = elt_size(dtype) * (size_t)op->d.n[0] * op->d.n[1] * op->d.n[2];
-    int rc = gpw_operator_apply(op, dtype, in, out, half, phases, stream);
+    int rc = operator_apply(op, dtype, in, out, half, phases, pot, stream);
     if (rc) return rc;
-    return gpw_operator_apply(op, dtype, (const char*)in + half * es, (char*)out + half * es, nin - half, phases,
-                              stream);
+    return operator_apply(op, dtype, (const char*)in + half * es, (char*)out + half * es, nin - half, phases, pot,
+                          stream);
   }
   cudaStream_t st = (cudaStream_t)stream;
   const OpDesc& d = op->d;
@@ -243,9 +243,22 @@ int gpw_operator_apply(gpw_operator* op, int dtype, const void* in, void* out, i
   }
   Boundary bc = make_boundary(d.periodic, dtype, phases);
   GridSum gs{};
-  cudaError_t e = launch_stencil(d, dtype, MODE_APPLY, src, v, out, v, nullptr, v, (int)nin, bc, 1.0, nullptr, gs, st);
+  cudaError_t e =
+      launch_stencil(d, dtype, MODE_APPLY, src, v, out, v, nullptr, v, (int)nin, bc, 1.0, nullptr, gs, st, pot);
   if (e != cudaSuccess) return cuda_fail(e, "operator apply launch");
   return GPW_OK;
+}
+
+int gpw_operator_apply(gpw_operator* op, int dtype, const void* in, void* out, int64_t nin, const double* phases,
+                       gpw_stream stream) {
+  return operator_apply(op, dtype, in, out, nin, phases, nullptr, stream);
+}
+
+int gpw_operator_apply_potential(gpw_operator* op, int dtype, const void* in, void* out, int64_t nin,
+                                 const double* phases, const void* pot, gpw_stream stream) {
+  if (!pot) return fail(GPW_EINVAL, "apply_potential: null potential");
+  if (pot == out) return fail(GPW_EINVAL, "apply_potential: the potential must not alias the output");
+  return operator_apply(op, dtype, in, out, nin, phases, pot, stream);
 }
 
 int gpw_operator_residual(gpw_operator* op, int dtype, const void* func, const void* source, void* r, int64_t nin,

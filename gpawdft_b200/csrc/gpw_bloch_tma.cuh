@@ -63,6 +63,8 @@ struct BlochArgs {
   int rowbytes;           // n2 * sizeof(T)
   int stage_bytes;        // ROWS * rowbytes (a multiple of 128)
   int* status;
+  const void* pot;        // optional local potential (scalar type, the output's
+                          // layout without batch): out = A in + pot in
 };
 
 __device__ __forceinline__ void mbar_arrive(unsigned bar) {
@@ -241,6 +243,14 @@ __global__ void __launch_bounds__(32 * NW, (BlochCfg<T, R, VEC, NW, D, WPR>::MIN
         }
 #pragma unroll
         for (int e = 0; e < VEC; ++e) part[j][e] = add(fmac(k.cc, c[j][e], py[e]), pz[e]);
+        if (a.pot && p >= z0 && p < z1 && j < nrows_ok) {
+          // local potential of this (in-range) plane: its part is output p's
+          using S = typename EltTraits<T>::S;
+          const S* pr = static_cast<const S*>(a.pot) + (int64_t)p * a.vout.s0 + (int64_t)(ylo + j) * a.vout.s1 + xb;
+#pragma unroll
+          for (int e = 0; e < VEC; ++e)
+            if (e < nx) part[j][e] = fmac(pr[e], c[j][e], part[j][e]);
+        }
         if (cpx_phase && p_wrap) {
           const double2 pp = p < 0 ? bc.ph[0][1] : bc.ph[0][0];
 #pragma unroll

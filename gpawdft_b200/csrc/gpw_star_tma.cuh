@@ -346,6 +346,17 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
               p[e] = fma(k.cz[R - q], nb[XL + e - q], p[e]);
             }
           }
+          if constexpr (MODE == MODE_APPLY) {
+            // local potential of this (in-range) plane: its part is output
+            // plane pfirst + s's
+            const int pp = pfirst + s, y = y0 + yb + j;
+            if (a.pot && pp >= z0 && pp < z1 && y < a.vout.n[1]) {
+              const S* pr = static_cast<const S*>(a.pot) + (int64_t)pp * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
+#pragma unroll
+              for (int e = 0; e < VEC; ++e)
+                if (e < nx) p[e] = fma(pr[e], c.v[e], p[e]);
+            }
+          }
           // scatter along axis 0 (logical slot m receives offset R - m)
 #pragma unroll
           for (int m = 0; m < NR; ++m) {

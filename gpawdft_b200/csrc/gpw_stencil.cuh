@@ -74,6 +74,8 @@ struct StencilArgs {
   void* out2;       // RESID_DC: first inner iterate (float); JACOBI_ADD64: float64 phi
   double w2;        // RESID_DC: Jacobi weight of that first inner sweep
   GridView vco;     // RESID_RESTRICT: the next level's view (out, out2)
+  const void* pot;  // APPLY: optional local potential, one grid in the output's
+                    // layout and the element's scalar type: out = A in + pot in
 };
 
 struct GeneralCoefs {
@@ -185,6 +187,11 @@ __global__ void __launch_bounds__(GEN_TZ* GEN_TY)
         }
         const int64_t oi = (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
         if constexpr (MODE == MODE_APPLY) {
+          if (a.pot) {
+            const T* sl = ring + ((o - z0 + mp) % NP) * PS;
+            const S pv = static_cast<const S*>(a.pot)[(int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x];
+            acc = fmac(pv, sl[(ty + mp) * W + tx + mp], acc);
+          }
           static_cast<T*>(a.out)[oi] = acc;
         } else {
           const int64_t ri = (int64_t)b * a.vrho.sb + (int64_t)o * a.vrho.s0 + (int64_t)y * a.vrho.s1 + x;
@@ -397,6 +404,12 @@ __global__ void __launch_bounds__(StarCfg<R, T>::NT)
         for (int q = 1; q <= R; ++q) {
           part = fmac((S)k.cz[R + q], row[q], part);
           part = fmac((S)k.cz[R - q], row[-q], part);
+        }
+        if constexpr (MODE == MODE_APPLY) {
+          // local potential of this (in-range) plane: its part is output p's
+          const int y = y0 + yb + j;
+          if (a.pot && p >= z0 && p < z1 && xin && y < a.vout.n[1])
+            part = fmac(static_cast<const S*>(a.pot)[(int64_t)p * a.vout.s0 + (int64_t)y * a.vout.s1 + x], v, part);
         }
         // scatter along axis 0: output plane p-R+m receives offset R-m
 #pragma unroll

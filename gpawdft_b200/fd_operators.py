@@ -123,6 +123,45 @@ class FDOperator:
         if not arrays.is_device(out_xg):
             arrays.writeback(out_xg, dst)
 
+    def apply_potential(self, in_xg, out_xg, vt_g, phase_cd=None):
+        """out_xg = A in_xg + vt_g in_xg in one pass (new API).
+
+        The kinetic apply and the local potential of
+        gpaw/wavefunctions/fd.py:77-80 (``kin.apply`` then
+        ``ham.apply_local_potential``, gpaw/hamiltonian.py:397-424) fused:
+        every band is read once and written once.  ``vt_g`` is one real grid
+        of the operator's shape; float64 for float64 / complex128 bands,
+        float32 for float32 / complex64.
+        """
+        self._check_grid(in_xg)
+        self._check_grid(vt_g)
+        if tuple(in_xg.shape) != tuple(out_xg.shape):
+            raise ValueError('input and output shapes differ')
+        if arrays.np_dtype_of(in_xg) != arrays.np_dtype_of(out_xg):
+            raise ValueError('input and output dtypes differ')
+        code = arrays.code_of(in_xg)
+        want = np.float64 if code in (_lib.GPW_F64, _lib.GPW_C128) \
+            else np.float32
+        if tuple(vt_g.shape) != self.shape or \
+                arrays.np_dtype_of(vt_g) != np.dtype(want):
+            raise TypeError('vt_g must be one %s grid of shape %s'
+                            % (np.dtype(want).name, self.shape))
+        if code in (_lib.GPW_C128, _lib.GPW_C64) and phase_cd is not None:
+            if np.asarray(phase_cd).shape != (3, 2):
+                raise ValueError('phase_cd must have shape (3, 2)')
+        nin = int(np.prod(in_xg.shape[:-3])) if len(in_xg.shape) > 3 else 1
+        src = arrays.to_device(in_xg)
+        pot = arrays.to_device(vt_g)
+        dst = out_xg if arrays.is_device(out_xg) else None
+        if dst is None:
+            dst = arrays.empty_like_device(out_xg.shape, out_xg.dtype)
+        pbuf, pptr = arrays.phases_arg(phase_cd)
+        _lib.check(self._lib.gpw_operator_apply_potential(
+            self._h, code, arrays.ptr(src), arrays.ptr(dst), nin, pptr,
+            arrays.ptr(pot), arrays.stream()))
+        if not arrays.is_device(out_xg):
+            arrays.writeback(out_xg, dst)
+
     def relax(self, relax_method, f_g, s_g, n, w=None):
         """n relaxation sweeps of A f = s (c/operators.c:49-91), in place.
 
@@ -271,3 +310,12 @@ class LaplaceB(FDOperator):
                             [(0, 0, 0), (-1, 0, 0), (1, 0, 0),
                              (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)],
                             gd, dtype, 'O(h^4) Mehrstellen Laplacian (B)')
+
+
+def apply_pseudo_hamiltonian(kin, psit_xG, Htpsit_xG, vt_G, phase_cd=None):
+    """The grid part of gpaw/wavefunctions/fd.py:77-80 in one pass:
+    ``kin.apply(psit_xG, Htpsit_xG, phase_cd)`` then
+    ``Htpsit_xG += psit_xG * vt_G`` (gpaw/hamiltonian.py:397-424), fused in
+    the kinetic stencil kernel.  The atomic (projector) and orbital-dependent
+    XC terms that follow in the reference are not part of this path."""
+    kin.apply_potential(psit_xG, Htpsit_xG, vt_G, phase_cd)

@@ -86,6 +86,17 @@ int gpw_operator_new(const double *coefs, const int64_t *offsets, int ncoefs,
 int gpw_operator_apply(gpw_operator *op, int dtype, const void *in, void *out,
                        int64_t nin, const double *phases, gpw_stream stream);
 
+/* The kinetic operator and the local potential in one pass over the bands:
+ * out[x] = (A in)[x] + pot * in[x].  Replaces kin.apply(psit_xG, Htpsit_xG,
+ * phase_cd) followed by ham.apply_local_potential(psit_xG, Htpsit_xG, s),
+ * i.e. Htpsit_G += psit_G * vt_G (gpaw/wavefunctions/fd.py:77-80,
+ * gpaw/hamiltonian.py:397-424).  `pot` is one real grid of the operator's
+ * shape in the element's scalar type (float64 for float64 / complex128,
+ * float32 for float32 / complex64), shared by all `nin` grids.             */
+int gpw_operator_apply_potential(gpw_operator *op, int dtype, const void *in,
+                                 void *out, int64_t nin, const double *phases,
+                                 const void *pot, gpw_stream stream);
+
 /* Operator.relax(relax_method, func, source, nrelax, w), c/operators.c:49-91
  * and c/bmgs/relax.c:7-73.  relax_method 2 = weighted Jacobi (each sweep
  * func = (1-w) func + w (source - sum_{p!=0} c_p func[x+o_p]) / c_0);

@@ -1,0 +1,145 @@
+"""GPU parity of the fused kinetic + local-potential apply.
+
+``FDOperator.apply_potential(psit, Htpsit, vt, phase_cd)`` does in one pass
+what gpaw/wavefunctions/fd.py:77-80 does in two: ``kin.apply(psit, Htpsit,
+phase_cd)`` (c/operators.c:316-405) and ``Htpsit += psit * vt``
+(gpaw/hamiltonian.py:397-424).  The oracle runs those two steps: the
+restated operator over the compiled reference C (NumPy restatement where it
+is not built) and the NumPy product.  Every kernel that serves an apply
+carries the potential term -- the zero-boundary TMA star kernel, the
+periodic / Bloch row kernel (each tile layout pinned in turn), the cp.async
+star kernel and the general-offset kernel -- so each is pinned here.  Bars:
+1e-12 relative for float64 / complex128, 2e-6 for float32 / complex64.
+"""
+import numpy as np
+import pytest
+
+from helpers import TOL, oracle_dtype, rand, relerr
+from oracle import layer as ol
+from oracle import ref as oref
+from oracle.geometry import GridDescriptor as OGD, phase_cd_for_k
+
+pytestmark = pytest.mark.gpu
+
+BACKEND = 'ref' if oref.available() else 'numpy'
+
+
+def _setup(N, cell, pbc, dtype, nn=3, nb=3, seed=0, k=None):
+    from gpawdft_b200.fd_operators import Laplace
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    gd = GridDescriptor(N, cell, pbc)
+    ogd = OGD(N, cell, pbc)
+    kin = Laplace(gd, -0.5, nn, dtype)
+    okin = ol.Laplace(ogd, -0.5, nn, oracle_dtype(dtype), BACKEND)
+    psi = rand((nb,) + tuple(gd.n_c), dtype, seed)
+    sdt = np.float32 if np.dtype(dtype) in (np.float32, np.complex64) \
+        else np.float64
+    vt = rand(tuple(gd.n_c), sdt, seed + 1)
+    ph = None
+    if np.dtype(dtype).kind == 'c':
+        ph = phase_cd_for_k(ogd, k if k is not None else (0.2, -0.35, 0.4))
+    return gd, ogd, kin, okin, psi, vt, ph
+
+
+def _oracle(okin, psi, vt, ph):
+    p = psi.astype(oracle_dtype(psi.dtype))
+    out = np.empty_like(p)
+    okin.apply(p, out, ph)
+    out += p * vt.astype(np.float64)
+    return out
+
+
+@pytest.mark.parametrize('dtype', [complex, np.complex64])
+def test_bloch_bands(cuda, dtype):
+    """Complex Bloch bands, 48^3 periodic, nn=3, random k (config 2's case)."""
+    gd, ogd, kin, okin, psi, vt, ph = _setup((48, 48, 48), (48 * 0.34,) * 3,
+                                             1, dtype, nb=5, seed=1)
+    out = np.empty_like(psi)
+    kin.apply_potential(psi, out, vt, ph)
+    assert relerr(out, _oracle(okin, psi, vt, ph)) < TOL[np.dtype(dtype)]
+
+
+@pytest.mark.parametrize('layout', [1, 2, 3, 4])
+def test_bloch_row_kernel_layouts(cuda, layout):
+    """Each tile layout of the row kernel, the potential term included."""
+    from gpawdft_b200 import _lib
+    lib = _lib.load()
+    gd, ogd, kin, okin, psi, vt, ph = _setup((32, 32, 96), (6.0, 6.0, 18.0),
+                                             1, complex, nb=2, seed=2)
+    want = _oracle(okin, psi, vt, ph)
+    n0 = lib.gpw_bloch_launch_count()
+    try:
+        _lib.check(lib.gpw_set_bloch_layout(layout))
+        out = np.empty_like(psi)
+        kin.apply_potential(psi, out, vt, ph)
+    finally:
+        lib.gpw_set_bloch_layout(0)
+    assert lib.gpw_bloch_launch_count() > n0
+    assert relerr(out, want) < 1e-12
+
+
+@pytest.mark.parametrize('dtype', [float, np.float32])
+def test_zero_boundary_real(cuda, dtype):
+    """Real grids with zero boundaries: the TMA star kernel (Gamma point,
+    finite systems)."""
+    gd, ogd, kin, okin, psi, vt, ph = _setup((40, 36, 44), (8.0, 7.2, 8.8),
+                                             0, dtype, nb=4, seed=3)
+    out = np.empty_like(psi)
+    kin.apply_potential(psi, out, vt)
+    assert relerr(out, _oracle(okin, psi, vt, None)) < TOL[np.dtype(dtype)]
+
+
+def test_cpasync_star_kernel(cuda):
+    """Rows longer than the row kernel takes (130 complex points): the
+    cp.async star kernel."""
+    gd, ogd, kin, okin, psi, vt, ph = _setup((16, 20, 130), (3.2, 4.0, 26.0),
+                                             1, complex, nb=2, seed=4)
+    out = np.empty_like(psi)
+    kin.apply_potential(psi, out, vt, ph)
+    assert relerr(out, _oracle(okin, psi, vt, ph)) < 1e-12
+
+
+def test_general_offsets_kernel(cuda):
+    """A non-orthogonal cell: the GUC Laplacian's general-offset kernel."""
+    from gpawdft_b200.fd_operators import Laplace
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    cell = [(0, 2.55, 2.55), (2.55, 0, 2.55), (2.55, 2.55, 0)]
+    N = (14, 14, 14)
+    gd = GridDescriptor(N, cell, 1)
+    ogd = OGD(N, cell, 1)
+    kin = Laplace(gd, -0.5, 2, complex)
+    okin = ol.Laplace(ogd, -0.5, 2, complex, BACKEND)
+    psi = rand((2,) + tuple(gd.n_c), complex, 5)
+    vt = rand(tuple(gd.n_c), float, 6)
+    ph = phase_cd_for_k(ogd, (0.1, 0.25, -0.3))
+    out = np.empty_like(psi)
+    kin.apply_potential(psi, out, vt, ph)
+    assert relerr(out, _oracle(okin, psi, vt, ph)) < 1e-12
+
+
+def test_in_place_and_device_tensors(cuda):
+    """psit is Htpsit (in place, as apply allows) on device tensors; the
+    result equals the two-step form computed by the product itself."""
+    import torch
+    from gpawdft_b200.fd_operators import apply_pseudo_hamiltonian
+    gd, ogd, kin, okin, psi, vt, ph = _setup((32, 32, 32), (6.4,) * 3, 1,
+                                             complex, nb=3, seed=7)
+    want = _oracle(okin, psi, vt, ph)
+    x = torch.from_numpy(psi).cuda()
+    v = torch.from_numpy(vt).cuda()
+    apply_pseudo_hamiltonian(kin, x, x, v, ph)
+    assert relerr(x.cpu().numpy(), want) < 1e-12
+    two = np.empty_like(psi)
+    kin.apply(psi, two, ph)
+    two += psi * vt
+    assert relerr(x.cpu().numpy(), two) < 1e-12
+
+
+def test_rejects_bad_potential(cuda):
+    gd, ogd, kin, okin, psi, vt, ph = _setup((16, 16, 16), (3.2,) * 3, 1,
+                                             complex, nb=1, seed=8)
+    out = np.empty_like(psi)
+    with pytest.raises(TypeError):
+        kin.apply_potential(psi, out, vt.astype(np.float32), ph)
+    with pytest.raises(ValueError):
+        kin.apply_potential(psi, out, vt[:8], ph)
