@@ -27,6 +27,8 @@ EXPORTS = [
     'gpw_operator_relax',
     'gpw_operator_get_diagonal_element', 'gpw_operator_residual',
     'gpw_operator_residual_noalloc', 'gpw_operator_free',
+    'gpw_woperator_new', 'gpw_woperator_apply', 'gpw_woperator_relax',
+    'gpw_woperator_get_diagonal_element', 'gpw_woperator_free',
     'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
     'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_dotc_pairs',
     'gpw_add_scalar',
@@ -75,6 +77,17 @@ _SIGS = {
                                                      _vp, _vp, ctypes.c_int64,
                                                      _vp, _vp]),
     'gpw_operator_free': (None, [_vp]),
+    'gpw_woperator_new': (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp,
+                                         ctypes.c_int, _vp, ctypes.c_int,
+                                         ctypes.c_int, ctypes.POINTER(_vp)]),
+    'gpw_woperator_apply': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp,
+                                           ctypes.c_int64, _vp, _vp]),
+    'gpw_woperator_relax': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp,
+                                           ctypes.c_int, ctypes.c_double,
+                                           _vp]),
+    'gpw_woperator_get_diagonal_element': (ctypes.c_int, [_vp, _vp, _c_dp,
+                                                          _vp]),
+    'gpw_woperator_free': (None, [_vp]),
     'gpw_transformer_new': (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp,
                                            _vp, _vp, ctypes.c_int,
                                            ctypes.c_int, ctypes.POINTER(_vp)]),

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libgpwgrid.so')
 SOURCES = ['gpw_api.cu', 'gpw_launch.cu', 'gpw_poisson.cu', 'gpw_noalloc.cu',
            'gpw_tma_f64.cu', 'gpw_tma_f32.cu', 'gpw_nn.cu',
-           'gpw_bloch.cu']
+           'gpw_bloch.cu', 'gpw_woperator.cu']
 
 
 def nvcc_path():

@@ -302,13 +302,6 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
         P col[PY + 2 * R];
 #pragma unroll
         for (int i = 0; i < PY + 2 * R; ++i) col[i] = ldv<S, VEC>(sl + (yb + i) * W + xl);
-        if constexpr (MODE == MODE_JACOBI_SCALED_IN) {
-          // phi = (w2 / c0) rhs, rounded as RESID_DC rounds the stored iterate
-#pragma unroll
-          for (int i = 0; i < PY + 2 * R; ++i)
-#pragma unroll
-            for (int e = 0; e < VEC; ++e) col[i].v[e] = k.wc2 * col[i].v[e];
-        }
 #pragma unroll
         for (int j = 0; j < PY; ++j) {
           const S* row = sl + (yb + j + R) * W + xl;
@@ -320,13 +313,8 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
             const P hi = ldv<S, VEC>(row + VEC + q);
 #pragma unroll
             for (int e = 0; e < VEC; ++e) {
-              if constexpr (MODE == MODE_JACOBI_SCALED_IN) {
-                nb[q + e] = k.wc2 * lo.v[e];
-                nb[XL + VEC + q + e] = k.wc2 * hi.v[e];
-              } else {
-                nb[q + e] = lo.v[e];
-                nb[XL + VEC + q + e] = hi.v[e];
-              }
+              nb[q + e] = lo.v[e];
+              nb[XL + VEC + q + e] = hi.v[e];
             }
           }
           const P c = col[j + R];
@@ -406,16 +394,19 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
                 // the centre value, R planes behind in the ring
                 const S* osl = reinterpret_cast<const S*>(ring + ((s + NS - R) % NS) * C::STAGE_BYTES);
                 P cur = ldv<S, VEC>(osl + (yb + j + R) * W + xl);
+                P avs = av;
                 if constexpr (MODE == MODE_JACOBI_SCALED_IN) {
-                  // the ring holds rhs: rho = rhs, phi = (w2 / c0) rhs
+                  // the ring holds rhs: rho = rhs, phi = (w2 / c0) rhs, and
+                  // A phi = (w2 / c0) A rhs (one scaling per output point)
 #pragma unroll
                   for (int e = 0; e < VEC; ++e) {
                     rho.v[e] = cur.v[e];
                     cur.v[e] = k.wc2 * cur.v[e];
+                    avs.v[e] = k.wc2 * av.v[e];
                   }
                 }
 #pragma unroll
-                for (int e = 0; e < VEC; ++e) res.v[e] = k.w1 * cur.v[e] + k.wc * (rho.v[e] - av.v[e]);
+                for (int e = 0; e < VEC; ++e) res.v[e] = k.w1 * cur.v[e] + k.wc * (rho.v[e] - avs.v[e]);
               }
               if constexpr (MODE == MODE_RESID_DC) {
                 // float32 defect and first inner Jacobi iterate from zero

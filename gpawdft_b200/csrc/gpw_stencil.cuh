@@ -42,7 +42,9 @@ namespace gpw {
 // diagonal, to `out2`, both in the coarse view `vco`.  JACOBI_SCALED_IN is a
 // float32 Jacobi sweep whose iterate is never stored: it reads only the
 // defect rhs (`in`) and takes phi = (w2 / c0) rhs -- the first inner sweep
-// from zero, rounded exactly as RESID_DC rounds it -- with rho = rhs.
+// from zero -- with rho = rhs; A phi is formed as (w2 / c0) (A rhs), one
+// scaling per output point (it rounds differently from a stencil of the
+// stored iterate, within float32 rounding).
 enum StencilMode {
   MODE_APPLY = 0,
   MODE_RESIDUAL = 1,

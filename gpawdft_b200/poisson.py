@@ -12,8 +12,12 @@ Two options go beyond the reference:
   precision='fp32'  float32 V-cycles inside a float64 defect-correction loop
                     (float64 residual, update, charge integral and norms);
                     the inner cycles use Chebyshev-weighted Jacobi smoothing
-                    (``inner='chebyshev'``, see ``inner_schedule``) or the
-                    reference's schedule (``inner='reference'``);
+                    (``inner='chebyshev'``, see ``inner_schedule``), the
+                    reference's schedule (``inner='reference'``) or plain
+                    weighted Jacobi, 2 pre- and 2 post-sweeps with w = 2/3
+                    and 8 on the coarsest level (``inner='jacobi22'``);
+  max_levels=k      at most k multigrid levels (the reference coarsens while
+                    the grid allows, up to 9 levels);
   solve_batch()     many independent same-grid solves in one batched launch
                     sequence, each with its own convergence test.
 """
@@ -44,8 +48,11 @@ def create_poisson_solver(name='fd', **kwargs):
 
 
 def PoissonSolver(dipolelayer=None, **kwargs):
+    """gpaw/poisson.py:51-54: the finite-difference solver, wrapped in the
+    dipole-layer correction when ``dipolelayer`` names an axis or plane."""
     if dipolelayer is not None:
-        raise NotImplementedError('DipoleCorrection is not implemented by this package')
+        from .dipole_correction import DipoleCorrection
+        return DipoleCorrection(PoissonSolver(**kwargs), dipolelayer)
     return FDPoissonSolver(**kwargs)
 
 
@@ -123,10 +130,23 @@ def inner_schedule(operators, fine=(2, 6.0), coarse=(3, 4.0), coarsest=8):
     return npre, npost, weights
 
 
+def jacobi22_schedule(L, w=2.0 / 3.0, coarsest=8):
+    """Plain weighted-Jacobi inner schedule: 2 pre- and 2 post-sweeps of
+    weight w on every level but the coarsest, which gets ``coarsest``
+    post-sweeps of the same weight (layout of ``inner_schedule``)."""
+    npre = [2] * (L - 1) + [0]
+    npost = [2] * (L - 1) + [coarsest]
+    weights = []
+    for a, b in zip(npre, npost):
+        weights.extend([w] * (a + b))
+    return npre, npost, weights
+
+
 class FDPoissonSolver:
     def __init__(self, nn=3, relax='J', eps=2e-10, maxiter=1000,
                  remove_moment=None, use_charge_center=False,
-                 precision='fp64', batch=1, inner='chebyshev'):
+                 precision='fp64', batch=1, inner='chebyshev',
+                 max_levels=None):
         self.relax = relax
         self.nn = nn
         self.eps = eps
@@ -143,9 +163,13 @@ class FDPoissonSolver:
         if precision not in _PREC:
             raise ValueError("precision must be 'fp64' or 'fp32'")
         self.precision = precision
-        if inner not in ('chebyshev', 'reference'):
-            raise ValueError("inner must be 'chebyshev' or 'reference'")
+        if inner not in ('chebyshev', 'reference', 'jacobi22'):
+            raise ValueError("inner must be 'chebyshev', 'reference' or "
+                             "'jacobi22'")
         self.inner = inner
+        if max_levels is not None and int(max_levels) < 1:
+            raise ValueError('max_levels must be at least 1')
+        self.max_levels = None if max_levels is None else int(max_levels)
         self.batch = int(batch)
         self.description = None
         self._engine = None
@@ -177,7 +201,8 @@ class FDPoissonSolver:
         self.presmooths = [2]
         self.postsmooths = [1]
         self.weights = [2.0 / 3.0]
-        while level < 8:
+        while level < 8 and (self.max_levels is None or
+                             level + 1 < self.max_levels):
             try:
                 gd2 = gd.coarsen()
             except ValueError:
@@ -249,9 +274,12 @@ class FDPoissonSolver:
         self._lib = lib
         if not getattr(self, '_device_loop', True):
             _lib.check(lib.gpw_poisson_set_device_loop(h, 0))
-        if (self.precision == 'fp32' and self.inner == 'chebyshev' and
+        if (self.precision == 'fp32' and self.inner != 'reference' and
                 self.relax_method == 2 and L > 1):
-            npre, npost, ws = inner_schedule(self.operators)
+            if self.inner == 'chebyshev':
+                npre, npost, ws = inner_schedule(self.operators)
+            else:
+                npre, npost, ws = jacobi22_schedule(L)
             a_pre = (ctypes.c_int * L)(*npre)
             a_post = (ctypes.c_int * L)(*npost)
             a_w = (ctypes.c_double * len(ws))(*ws)

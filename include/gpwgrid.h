@@ -54,6 +54,7 @@ extern "C" {
 
 typedef struct gpw_operator gpw_operator;
 typedef struct gpw_transformer gpw_transformer;
+typedef struct gpw_woperator gpw_woperator;
 typedef struct gpw_poisson gpw_poisson;
 typedef void *gpw_stream; /* cudaStream_t */
 
@@ -137,6 +138,43 @@ int gpw_operator_residual_noalloc(gpw_operator *op, int dtype, const void *func,
                                   double *sumsq_dev, gpw_stream stream);
 
 void gpw_operator_free(gpw_operator *op);
+
+/* ------------------------------------------------------- weighted operator */
+
+/* Replaces _gpaw.WOperator(nweights, weights, coefs, offsets, size, range,
+ * neighbors, real, comm, cfd), c/woperators.c:497-588, built by
+ * gpaw/wfd_operators.py:8-76: A = sum_i w_i(r) S_i with nweights <= 4
+ * stencils S_i (coefs[i], linear offsets[i] into the range-padded array,
+ * ncoefs[i] <= 40 taps, offsets[i][0] == 0).  The weight grids are not held
+ * by the operator: every call passes the nweights device pointers (one
+ * float64 grid each), so a caller that updates them in place (as the
+ * dielectric solver restricts them to the coarse levels) is always seen.  */
+int gpw_woperator_new(int nweights, const double *const *coefs,
+                      const int64_t *const *offsets, const int *ncoefs,
+                      const int64_t size[3], int range,
+                      const int64_t neighbors[6], int real, int cfd,
+                      gpw_woperator **out);
+/* WOperator.apply(input, output, phases), c/woperators.c:362-465 with
+ * c/bmgs/wfd.c: float64 or complex128 grids, `in` may equal `out`.  The
+ * reference's nin > 1 reads each grid's weights past the end of the weight
+ * arrays; here every grid of the call uses the same weights.              */
+int gpw_woperator_apply(gpw_woperator *op, int dtype,
+                        const double *const *weights, const void *in,
+                        void *out, int64_t nin, const double *phases,
+                        gpw_stream stream);
+/* WOperator.relax(relax_method, func, source, nrelax, w),
+ * c/woperators.c:61-108 with c/bmgs/wrelax.c: weighted Gauss-Seidel (1) or
+ * Jacobi (2) on one float64 grid, in place.                               */
+int gpw_woperator_relax(gpw_woperator *op, int relax_method,
+                        const double *const *weights, double *func,
+                        const double *source, int nrelax, double w,
+                        gpw_stream stream);
+/* WOperator.get_diagonal_element(), c/woperators.c:466-496: the largest
+ * |sum_i w_i(r) c_i0| over the grid (blocks until it is known).           */
+int gpw_woperator_get_diagonal_element(gpw_woperator *op,
+                                       const double *const *weights,
+                                       double *out, gpw_stream stream);
+void gpw_woperator_free(gpw_woperator *op);
 
 /* ------------------------------------------------------------ transformer */
 

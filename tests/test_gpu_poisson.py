@@ -304,9 +304,13 @@ def test_pdl_off_equals_on(cuda, precision):
 
 @pytest.mark.parametrize('N', [64, 128, 192])
 def test_fused_residual_restriction(cuda, N):
-    """The float32 form's level-0 residual restricted in the same launch
-    (no residual stored) and in two launches: identical iteration counts and
-    bit-identical potentials (the same values in the same order)."""
+    """The float32 form's fused level-0 plan (the second pre-sweep reads the
+    defect alone and scales its stencil once; the residual is restricted in
+    the same launch and never stored) against the plan that stores the
+    first iterate and the residual: the inner corrections differ only by
+    float32 rounding, so both reach the tolerance in the same number of
+    outer iterations (one more at most) with potentials that agree to the
+    solver's accuracy."""
     from gpawdft_b200 import _lib
     from gpawdft_b200.grid_descriptor import GridDescriptor
     from gpawdft_b200.poisson import PoissonSolver
@@ -328,8 +332,8 @@ def test_fused_residual_restriction(cuda, N):
         n = ps.solve_batch(phi, rhos, eps=eps)
         assert (ps.last_errors <= eps).all()
         out.append((phi, n))
-    assert np.array_equal(out[0][1], out[1][1])
-    assert np.array_equal(out[0][0], out[1][0])
+    assert (np.abs(out[0][1] - out[1][1]) <= 1).all()
+    assert np.abs(out[0][0] - out[1][0]).max() < 1e-9 * np.abs(out[1][0]).max()
 
 
 @pytest.mark.parametrize('N', [64, 128, 192])
