@@ -473,6 +473,32 @@ int gpw_poisson_charge_finish(int64_t nb, int64_t n, double* phi, const double* 
   return e == cudaSuccess ? GPW_OK : cuda_fail(e, "charge_finish");
 }
 
+int gpw_copy_box(int dtype, const void* src, const int64_t src_n[3], const int64_t src_off[3], void* dst,
+                 const int64_t dst_n[3], const int64_t dst_off[3], const int64_t box[3], gpw_stream stream) {
+  if (!valid_dtype(dtype) || !src || !dst || !src_n || !src_off || !dst_n || !dst_off || !box)
+    return fail(GPW_EINVAL, "copy_box: bad arguments");
+  int sn[3], so[3], dn[3], dof[3], b[3];
+  for (int c = 0; c < 3; ++c) {
+    if (box[c] < 0 || src_off[c] < 0 || dst_off[c] < 0 || src_off[c] + box[c] > src_n[c] ||
+        dst_off[c] + box[c] > dst_n[c] || src_n[c] > (1 << 20) || dst_n[c] > (1 << 20))
+      return fail(GPW_EINVAL, "copy_box: the box leaves a grid");
+    sn[c] = (int)src_n[c];
+    so[c] = (int)src_off[c];
+    dn[c] = (int)dst_n[c];
+    dof[c] = (int)dst_off[c];
+    b[c] = (int)box[c];
+  }
+  cudaError_t e = launch_copy_box(dtype, src, sn, so, dst, dn, dof, b, (cudaStream_t)stream);
+  return e == cudaSuccess ? GPW_OK : cuda_fail(e, "copy_box");
+}
+
+int gpw_mul(int64_t n, const double* x, const double* y, double* out, gpw_stream stream) {
+  if (n < 0 || (n && (!x || !y || !out))) return fail(GPW_EINVAL, "mul: bad arguments");
+  if (!n) return GPW_OK;
+  cudaError_t e = launch_mul(n, x, y, out, (cudaStream_t)stream);
+  return e == cudaSuccess ? GPW_OK : cuda_fail(e, "mul");
+}
+
 int gpw_dotc_pairs(int dtype, int64_t nx, int64_t ny, int64_t n, const void* x, const void* y, double* out_dev,
                    gpw_stream stream) {
   if (!y) return fail(GPW_EINVAL, "null argument");

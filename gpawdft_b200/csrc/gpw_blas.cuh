@@ -154,6 +154,30 @@ __global__ void charge_finish_kernel(int64_t n, double* __restrict__ phi, const 
     ph[i] = fma(q, phi_g[i], ph[i]);
 }
 
+// dst[dst_off + i] = src[src_off + i] for every index i of the box (grid
+// extension / de-extension of the extended Poisson solver); element type T,
+// contiguous (n0, n1, n2) grids.
+template <typename T>
+__global__ void copy_box_kernel(const T* __restrict__ src, int sn1, int sn2, int so0, int so1, int so2,
+                                T* __restrict__ dst, int dn1, int dn2, int do0, int do1, int do2, int b0, int b1,
+                                int b2) {
+  const int64_t tot = (int64_t)b0 * b1 * b2;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int i2 = (int)(i % b2);
+    const int64_t r = i / b2;
+    const int i1 = (int)(r % b1), i0 = (int)(r / b1);
+    dst[((int64_t)(i0 + do0) * dn1 + (i1 + do1)) * dn2 + (i2 + do2)] =
+        src[((int64_t)(i0 + so0) * sn1 + (i1 + so1)) * sn2 + (i2 + so2)];
+  }
+}
+
+// out = x * y elementwise (float64; rounded once, as NumPy's product).
+__global__ void mul_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                           double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = __dmul_rn(x[i], y[i]);
+}
+
 // Fill `n` elements with zero (used for phi_{l+1} = 0 inside captured graphs
 // where a memset node would also do; a kernel keeps the batch mask).
 template <typename T>

@@ -175,6 +175,9 @@ cudaError_t launch_charge_prepare(int64_t nb, int64_t n, const double* rho, doub
                                   double* q_out, cudaStream_t st);
 cudaError_t launch_charge_finish(int64_t nb, int64_t n, double* phi, const double* phi_g, const double* q,
                                  cudaStream_t st);
+cudaError_t launch_copy_box(int dtype, const void* src, const int sn[3], const int so[3], void* dst,
+                            const int dn[3], const int dof[3], const int box[3], cudaStream_t st);
+cudaError_t launch_mul(int64_t n, const double* x, const double* y, double* out, cudaStream_t st);
 cudaError_t launch_add_scalar(int dtype, int64_t n, double c, const void* x, void* y, cudaStream_t st);
 cudaError_t launch_zero(int dtype, const GridView& v, void* x, int nbatch, const unsigned char* active,
                         cudaStream_t st);

@@ -1053,6 +1053,31 @@ cudaError_t launch_charge_finish(int64_t nb, int64_t n, double* phi, const doubl
   return cudaGetLastError();
 }
 
+cudaError_t launch_copy_box(int dtype, const void* src, const int sn[3], const int so[3], void* dst,
+                            const int dn[3], const int dof[3], const int box[3], cudaStream_t st) {
+  const int64_t tot = (int64_t)box[0] * box[1] * box[2];
+  if (tot <= 0) return cudaSuccess;
+  const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, 4LL * num_sms()));
+#define GPW_BOX_CASE(T)                                                                                   \
+  copy_box_kernel<T><<<g, 256, 0, st>>>((const T*)src, sn[1], sn[2], so[0], so[1], so[2], (T*)dst, dn[1], dn[2], \
+                                        dof[0], dof[1], dof[2], box[0], box[1], box[2]);
+  switch (dtype) {
+    case GPW_F64: GPW_BOX_CASE(double) break;
+    case GPW_F32: GPW_BOX_CASE(float) break;
+    case GPW_C128: GPW_BOX_CASE(double2) break;
+    case GPW_C64: GPW_BOX_CASE(float2) break;
+    default: return cudaErrorInvalidValue;
+  }
+#undef GPW_BOX_CASE
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mul(int64_t n, const double* x, const double* y, double* out, cudaStream_t st) {
+  const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 4LL * num_sms()));
+  mul_kernel<<<g, 256, 0, st>>>(n, x, y, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_zero(int dtype, const GridView& v, void* x, int nbatch, const unsigned char* active,
                         cudaStream_t st) {
   const int64_t tot = view_points(v);

@@ -224,6 +224,18 @@ int gpw_dot(int dtype, int64_t nvec, int64_t n, const void *x, const void *y,
  * Deterministic order.                                                      */
 int gpw_dotc_pairs(int dtype, int64_t nx, int64_t ny, int64_t n, const void *x,
                    const void *y, double *out_dev, gpw_stream stream);
+/* dst[dst_off + i] = src[src_off + i] over a box of contiguous (n0, n1, n2)
+ * grids: the array copies of extend_array / deextend_array
+ * (gpaw/utilities/extend_grid.py:46-56, grid2grid with an offset) for the
+ * extended Poisson solver.                                                */
+int gpw_copy_box(int dtype, const void *src, const int64_t src_n[3],
+                 const int64_t src_off[3], void *dst, const int64_t dst_n[3],
+                 const int64_t dst_off[3], const int64_t box[3],
+                 gpw_stream stream);
+/* out = x * y elementwise, float64 (the NumPy products rho * mask_g of
+ * gpaw/poisson_extended.py:214).                                          */
+int gpw_mul(int64_t n, const double *x, const double *y, double *out,
+            gpw_stream stream);
 /* y = x + c (real dtypes, c added to every element)                         */
 int gpw_add_scalar(int dtype, int64_t n, double c, const void *x, void *y,
                    gpw_stream stream);

@@ -344,3 +344,109 @@ class WeightedFDPoissonSolver(layer.PoissonSolver):
                    for j in (0, 1, 2)]
             self.operators.append(WeightedFDOperator(weights, operators,
                                                      self.backend))
+
+
+# ------------------------------------------------------------ extended grid
+def extended_grid_descriptor(gd, N_c):
+    """gpaw/utilities/extend_grid.py:7-43 (serial, N_c form)."""
+    from .geometry import GridDescriptor
+    N_c = np.array(N_c, dtype=int)
+    extend_N_cd = np.tile((N_c - gd.N_c) // 2, (2, 1)).T
+    egd = GridDescriptor(N_c, gd.h_cv * N_c, gd.pbc_c)
+    egd.extend_N_cd = extend_N_cd
+    return egd
+
+
+def extend_array(gd, egd, a_g, aext_g):
+    """gpaw/utilities/extend_grid.py:46-49 (grid2grid with an offset)."""
+    o = egd.extend_N_cd[:, 0]
+    n = gd.n_c
+    aext_g[o[0]:o[0] + n[0], o[1]:o[1] + n[1], o[2]:o[2] + n[2]] = a_g
+
+
+def deextend_array(gd, egd, a_g, aext_g):
+    """gpaw/utilities/extend_grid.py:52-56."""
+    o = egd.extend_N_cd[:, 0]
+    n = gd.n_c
+    a_g[:] = aext_g[o[0]:o[0] + n[0], o[1]:o[1] + n[1], o[2]:o[2] + n[2]]
+
+
+class ExtendedPoissonSolver(layer.PoissonSolver):
+    """gpaw/poisson_extended.py:13-241 (serial)."""
+
+    def __init__(self, nn=3, relax='J', eps=2e-10, maxiter=1000,
+                 moment_corrections=None, extended=None, backend='numpy'):
+        layer.PoissonSolver.__init__(self, nn=nn, relax=relax, eps=eps,
+                                     maxiter=maxiter, backend=backend)
+        if moment_corrections is None:
+            self.moment_corrections = None
+        elif isinstance(moment_corrections, int):
+            self.moment_corrections = [{'moms': range(moment_corrections),
+                                        'center': None}]
+        else:
+            self.moment_corrections = moment_corrections
+        self.is_extended = extended is not None
+        if self.is_extended:
+            self.extended = dict(extended)
+            self.extended['finegpts'] = np.array(self.extended['gpts']) * 2
+
+    def set_grid_descriptor(self, gd):
+        if self.is_extended:
+            self.gd_original = gd
+            gd = extended_grid_descriptor(gd, self.extended['finegpts'])
+        layer.PoissonSolver.set_grid_descriptor(self, gd)
+
+    def initialize(self):
+        layer.PoissonSolver.initialize(self)
+        if self.is_extended:
+            self.rho_g = self.gd.zeros()
+            self.phi_g = self.gd.zeros()
+        if self.moment_corrections is not None:
+            self.gauss_i, self.mom_ij, r_ir = [], [], []
+            for rmom in self.moment_corrections:
+                center = None if rmom['center'] is None else \
+                    np.array(rmom['center'])
+                g = Gaussian(self.gd, center=center)
+                self.gauss_i.append(g)
+                r_ir.append(g.r.ravel())
+                self.mom_ij.append(rmom['moms'])
+            r_ir = np.array(r_ir)
+            mask_ir = np.zeros(r_ir.shape, dtype=int)
+            for r in range(r_ir.shape[1]):
+                mask_ir[np.argmin(r_ir[:, r]), r] = 1
+            self.mask_ig = [m.reshape(self.gd.n_c) for m in mask_ir]
+
+    def solve(self, phi, rho, charge=None, eps=None, maxcharge=1e-6,
+              zero_initial_phi=False):
+        if self.is_extended:
+            self.rho_g[:] = 0
+            if not self.extended['useprev']:
+                self.phi_g[:] = 0
+            extend_array(self.gd_original, self.gd, rho, self.rho_g)
+            retval = self._solve(self.phi_g, self.rho_g, charge, eps,
+                                 maxcharge, zero_initial_phi)
+            deextend_array(self.gd_original, self.gd, phi, self.phi_g)
+            return retval
+        return self._solve(phi, rho, charge, eps, maxcharge, zero_initial_phi)
+
+    def _solve(self, phi, rho, charge=None, eps=None, maxcharge=1e-6,
+               zero_initial_phi=False):
+        if eps is None:
+            eps = self.eps
+        if self.moment_corrections:
+            rho_neutral = rho * 0.0
+            phi_cor_k = []
+            for gauss, mask_g, mom_j in zip(self.gauss_i, self.mask_ig,
+                                            self.mom_ij):
+                rho_masked = rho * mask_g
+                for mom in mom_j:
+                    phi_cor_k.append(gauss.remove_moment(rho_masked, mom))
+                rho_neutral += rho_masked
+            for phi_cor in phi_cor_k:
+                phi -= phi_cor
+            niter = self.solve_neutral(phi, rho_neutral, eps=eps)
+            for phi_cor in phi_cor_k:
+                phi += phi_cor
+            return niter
+        return layer.PoissonSolver.solve(self, phi, rho, charge, eps,
+                                         maxcharge, zero_initial_phi)

@@ -274,3 +274,44 @@ def test_dipole_correction_slab(cuda):
     assert np.abs(phi - ophi).max() < 1e-7 * np.abs(ophi).max()
     # the correction flattens the potential far from the slab on both sides
     assert abs(ps.correction) > 1e-3
+
+
+# ------------------------------------------------------------ extended grid
+def test_extended_solver_golden_values(cuda):
+    """gpaw/test/poisson/poisson_extended.py on the GPU: every option's
+    max |phi - phi_default| equals the reference's own value to 1e-10, and
+    each potential follows the oracle's; useprev restarts from the last
+    extended potential."""
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    from gpawdft_b200.poisson_extended import ExtendedPoissonSolver
+    from test_oracle_variants import EXT_GOLDEN, extended_case
+    ogd, rho = extended_case()
+    gd = GridDescriptor((16, 16, 48), (1, 1, 3), False)
+
+    def run(ps, g):
+        ps.set_grid_descriptor(g)
+        ps.initialize()
+        phi = g.zeros()
+        n = ps.solve(phi, rho)
+        return phi, n, ps
+
+    ref, _, _ = run(PoissonSolver(eps=1e-20), gd)
+    oref_phi, _, _ = run(ol.PoissonSolver(eps=1e-20, backend=BACKEND), ogd)
+    assert np.abs(ref - oref_phi).max() < 1e-9 * np.abs(oref_phi).max()
+    for kw, val in EXT_GOLDEN:
+        phi, n, ps = run(ExtendedPoissonSolver(eps=1e-20, **kw), gd)
+        assert abs(np.abs(phi - ref).max() - val) < 1e-10, kw
+        ophi, on, _ = run(ov.ExtendedPoissonSolver(eps=1e-20, backend=BACKEND,
+                                                   **kw), ogd)
+        assert n == on, kw
+        assert np.abs(phi - ophi).max() < 1e-9 * np.abs(ophi).max(), kw
+    # useprev: the second solve starts from the first's extended potential
+    kw = dict(extended={'gpts': (24, 24, 72), 'useprev': True},
+              moment_corrections=[{'moms': range(4), 'center': [.5, .5, 1]},
+                                  {'moms': range(4), 'center': [.5, .5, 2]}])
+    phi1, n1, ps = run(ExtendedPoissonSolver(eps=1e-20, **kw), gd)
+    phi2 = gd.zeros()
+    n2 = ps.solve(phi2, rho)
+    assert n2 < n1
+    assert np.abs(phi2 - phi1).max() < 1e-8 * np.abs(phi1).max()
