@@ -667,6 +667,68 @@ def run_mixed192(args):
     print(json.dumps(line), flush=True)
 
 
+def run_general(args):
+    """General-offset stencils (gpaw/fd_operators.py:158-251): the GUC
+    Laplacian of a face-centred-cubic cell (6 directions, nn=3: 37 points)
+    on complex128 Bloch bands of a 96^3 periodic grid, and the Mehrstellen
+    pair (LaplaceA, 19 points; LaplaceB, 7 points) on float64 127^3
+    zero-boundary grids (the Poisson solver's nn='M').  GB/s of algorithmic
+    bytes (input read once, output written once)."""
+    import torch
+    from gpawdft_b200.fd_operators import LaplaceA, LaplaceB, Laplace
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    peak, _ = measured_peak()
+    res = {}
+
+    def timeit(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    a0 = 96 * 0.18 / 0.52917721
+    cell = [(0, a0 / 2, a0 / 2), (a0 / 2, 0, a0 / 2), (a0 / 2, a0 / 2, 0)]
+    gd = GridDescriptor((96,) * 3, cell, 1)
+    ph = np.exp(2j * np.pi * gd.sdisp_cd *
+                np.array([0.1, -0.2, 0.3])[:, None])
+    NB = 64
+    g = torch.Generator(device='cuda').manual_seed(3)
+    a = torch.randn((NB, 96, 96, 96), dtype=torch.complex128, device='cuda',
+                    generator=g)
+    o = torch.empty_like(a)
+    op = Laplace(gd, -0.5, 3, complex)
+    t = timeit(lambda: op.apply(a, o, ph), args.steps)
+    gbs = 2 * a.numel() * 16 / t / 1e9
+    res['guc_fcc_nn3_c128'] = {'ms': t * 1e3, 'GB/s': gbs, 'frac': gbs / peak,
+                               'points': int(op.npoints), 'bands': NB}
+    del a, o
+    torch.cuda.empty_cache()
+    gdz = GridDescriptor((128,) * 3, (128 * 0.2 / 0.52917721,) * 3, 0)
+    b = torch.randn((16, 127, 127, 127), dtype=torch.float64, device='cuda',
+                    generator=g)
+    ob = torch.empty_like(b)
+    for nm, opz in (('mehrstellen_A_f64', LaplaceA(gdz, 0.25 / np.pi)),
+                    ('mehrstellen_B_f64', LaplaceB(gdz))):
+        t = timeit(lambda: opz.apply(b, ob), args.steps)
+        gbs = 2 * b.numel() * 8 / t / 1e9
+        res[nm] = {'ms': t * 1e3, 'GB/s': gbs, 'frac': gbs / peak,
+                   'points': int(opz.npoints), 'grids': 16}
+    line = {'metric': 'general_stencil_GBps', 'value':
+            res['guc_fcc_nn3_c128']['GB/s'], 'unit': 'GB/s',
+            'higher_is_better': True, 'n_gpus': 1, 'steps': args.steps,
+            'dtype': 'c128', 'data': 'synthetic', 'peak_GBps': peak,
+            'config': {'workload': 'GUC nn=3 fcc 64 x 96^3 complex128; '
+                                   'Mehrstellen 16 x 127^3 float64'},
+            'ops': res}
+    print(json.dumps(line), flush=True)
+
+
 def run_uneven(args):
     """512 independent solves, cubic N_c log-uniform in [32, 128] rounded to
     multiples of 8 (seed 5), each density 4-32 neutral Gaussians (h = 0.2 A),
@@ -938,7 +1000,7 @@ def main():
     ap.add_argument('--precision', default='fp32', choices=['fp64', 'fp32'])
     ap.add_argument('--workload', default='poisson128',
                     choices=['poisson128', 'mixed192', 'uneven512', 'bands96',
-                             'learned128'])
+                             'learned128', 'general'])
     ap.add_argument('--pairs', type=int, default=20000,
                     help='learned128: training pairs')
     ap.add_argument('--save-weights', default=None,
@@ -951,7 +1013,8 @@ def main():
     args = ap.parse_args()
     if args.workload != 'poisson128':
         {'mixed192': run_mixed192, 'uneven512': run_uneven,
-         'bands96': run_bands, 'learned128': run_learned}[args.workload](args)
+         'bands96': run_bands, 'learned128': run_learned,
+         'general': run_general}[args.workload](args)
         return
     args.warmup = max(args.warmup, 3) if args.impl == 'ours' else args.warmup
     if 'WORLD_SIZE' not in os.environ and args.gpus > 1:

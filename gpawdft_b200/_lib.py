@@ -31,7 +31,7 @@ EXPORTS = [
     'gpw_woperator_get_diagonal_element', 'gpw_woperator_free',
     'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
     'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_dotc_pairs',
-    'gpw_copy_box', 'gpw_mul',
+    'gpw_copy_box', 'gpw_mul', 'gpw_tune_export', 'gpw_tune_import',
     'gpw_add_scalar',
     'gpw_poisson_charge_prepare', 'gpw_poisson_charge_finish',
     'gpw_poisson_new', 'gpw_poisson_solve', 'gpw_poisson_last_stats',
@@ -105,6 +105,9 @@ _SIGS = {
                                _vp, _vp, _vp, _vp]),
     'gpw_copy_box': (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
                                     _vp, _vp, _vp]),
+    'gpw_tune_export': (ctypes.c_int, [_vp, ctypes.c_int64, _c_i64p]),
+    'gpw_tune_import': (ctypes.c_int, [ctypes.c_char_p,
+                                       ctypes.POINTER(ctypes.c_int)]),
     'gpw_mul': (ctypes.c_int, [ctypes.c_int64, _vp, _vp, _vp, _vp]),
     'gpw_dotc_pairs': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64,
                                       ctypes.c_int64, ctypes.c_int64, _vp,
@@ -197,6 +200,10 @@ def load():
         f.restype = res
         f.argtypes = args
     _lib = lib
+    cache = os.environ.get('GPW_TUNE_CACHE')
+    if cache:
+        from . import tuning
+        tuning._auto(cache)
     return lib
 
 

@@ -26,16 +26,33 @@ def nvcc_path():
     raise RuntimeError('nvcc not found')
 
 
-def needs_build():
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
+STAMP = os.path.join(HERE, '_build', 'sources.mtime')
+
+
+def sources_mtime():
+    """Newest modification time of the library's sources and header."""
+    t = 0.0
     for root, _, files in os.walk(CSRC):
         for f in files:
-            if os.path.getmtime(os.path.join(root, f)) > t:
-                return True
+            t = max(t, os.path.getmtime(os.path.join(root, f)))
     hdr = os.path.join(os.path.dirname(HERE), 'include', 'gpwgrid.h')
-    return os.path.exists(hdr) and os.path.getmtime(hdr) > t
+    if os.path.exists(hdr):
+        t = max(t, os.path.getmtime(hdr))
+    return t
+
+
+def needs_build():
+    """The library is missing, or a source changed after the sources the
+    last build compiled (their newest time is stamped when a build starts,
+    so an edit made while nvcc runs is not missed)."""
+    if not os.path.exists(LIB):
+        return True
+    try:
+        with open(STAMP) as f:
+            built = float(f.read())
+    except (OSError, ValueError):
+        return sources_mtime() > os.path.getmtime(LIB)
+    return sources_mtime() > built
 
 
 def build(force=False, verbose=False, extra=()):
@@ -44,6 +61,7 @@ def build(force=False, verbose=False, extra=()):
     objs = []
     builddir = os.path.join(HERE, '_build')
     os.makedirs(builddir, exist_ok=True)
+    started = sources_mtime()
     flags = ['-O3', '-std=c++17', '-gencode', 'arch=compute_100a,code=sm_100a',
              '-lineinfo', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr',
              '-I', os.path.dirname(HERE)] + list(extra)
@@ -72,6 +90,8 @@ def build(force=False, verbose=False, extra=()):
            '-Xlinker', '-Bsymbolic', '-o', tmp] + objs
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    with open(STAMP, 'w') as f:
+        f.write(repr(started))
     return LIB
 
 

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <sstream>
 #include <string>
 
 #include "gpw_internal.h"
@@ -497,6 +498,50 @@ int gpw_mul(int64_t n, const double* x, const double* y, double* out, gpw_stream
   if (!n) return GPW_OK;
   cudaError_t e = launch_mul(n, x, y, out, (cudaStream_t)stream);
   return e == cudaSuccess ? GPW_OK : cuda_fail(e, "mul");
+}
+
+static std::string tune_header() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp p{};
+  cudaGetDeviceProperties(&p, dev);
+  std::string name(p.name);
+  for (char& ch : name)
+    if (ch == ' ') ch = '_';
+  return "gpwgrid-tune 1 sms " + std::to_string(num_sms()) + " device " + name + "\n";
+}
+
+int gpw_tune_export(char* buf, int64_t cap, int64_t* needed) {
+  if (!needed) return fail(GPW_EINVAL, "tune_export: null argument");
+  std::string text = tune_header();
+  tune_export_tma(text);
+  tune_export_bloch(text);
+  *needed = (int64_t)text.size() + 1;
+  if (!buf || cap < *needed) return buf ? fail(GPW_EINVAL, "tune_export: buffer too small") : GPW_OK;
+  std::memcpy(buf, text.c_str(), text.size() + 1);
+  return GPW_OK;
+}
+
+int gpw_tune_import(const char* text, int* imported) {
+  if (!text) return fail(GPW_EINVAL, "tune_import: null argument");
+  std::istringstream in(text);
+  std::string line;
+  if (!std::getline(in, line) || line + "\n" != tune_header())
+    return fail(GPW_EINVAL, "tune_import: records of another device or SM count (header mismatch)");
+  int n = 0;
+  while (std::getline(in, line)) {
+    std::istringstream ls(line);
+    std::string kind;
+    ls >> kind;
+    int f[11];
+    const int want = kind == "tma" ? 9 : (kind == "bloch" ? 11 : 0);
+    int got = 0;
+    while (got < want && (ls >> f[got])) ++got;
+    if (!want || got != want) continue;
+    if (kind == "tma" ? tune_import_tma(f) : tune_import_bloch(f)) ++n;
+  }
+  if (imported) *imported = n;
+  return GPW_OK;
 }
 
 int gpw_dotc_pairs(int dtype, int64_t nx, int64_t ny, int64_t n, const void* x, const void* y, double* out_dev,

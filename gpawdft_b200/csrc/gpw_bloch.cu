@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <atomic>
 #include <cstring>
 #include <map>
@@ -209,6 +210,45 @@ cudaError_t bloch_launch(int dtype, int R, const BlochChoice& ch, const void* in
 }
 
 }  // namespace
+
+// The row kernel's tuned layouts as text records "bloch dtype R axes n0 n1 n2
+// nbatch vec wpr nw nchunk" (gpw_tune_export).
+void tune_export_bloch(std::string& out) {
+  std::lock_guard<std::mutex> lock(g_bloch_mu);
+  char line[160];
+  for (const auto& kv : g_bloch_tune) {
+    const BlochKey& k = kv.first;
+    const BlochChoice& c = kv.second;
+    snprintf(line, sizeof line, "bloch %d %d %d %d %d %d %d %d %d %d %d\n", k.dtype, k.R, k.axes, k.n0, k.n1, k.n2,
+             k.nbatch, c.vec, c.wpr, c.nw, c.nchunk);
+    out += line;
+  }
+}
+
+// One "bloch ..." record back into the tuner; a layout that is not among
+// the shape's candidates (nor the cp.async kernel, vec 0) is refused.
+bool tune_import_bloch(const int* f) {
+  const int dtype = f[0], R = f[1];
+  if (!valid_dtype(dtype) || R < 1 || R > 3 || f[3] <= 0 || f[4] <= 0 || f[5] <= 0 || f[6] <= 0) return false;
+  const BlochChoice c{f[7], f[8], f[9], f[10]};
+  if (c.nchunk < -8 || c.nchunk > 64) return false;
+  if (c.vec != 0) {
+    GridView v{};
+    v.n[0] = f[3];
+    v.n[1] = f[4];
+    v.n[2] = f[5];
+    v.s1 = v.n[2];
+    v.s0 = (int64_t)v.n[1] * v.n[2];
+    v.sb = v.s0 * v.n[0];
+    bool ok = false;
+    for (const BlochChoice& k : bloch_candidates(dtype, R, v))
+      ok = ok || (k.vec == c.vec && k.wpr == c.wpr && k.nw == c.nw);
+    if (!ok) return false;
+  }
+  std::lock_guard<std::mutex> lock(g_bloch_mu);
+  g_bloch_tune[BlochKey{dtype, R, f[2], f[3], f[4], f[5], f[6]}] = c;
+  return true;
+}
 
 bool bloch_path_ok(const OpDesc& d, int dtype, const void* in, const GridView& vin, const void* out,
                    const GridView& vout, int nbatch) {

@@ -256,4 +256,10 @@ cudaError_t launch_apply_cpasync(const OpDesc& d, int dtype, const StencilArgs& 
 // stream capture (handle constructors call it).
 int* device_status_word();
 
+// Autotuner records (gpw_tune_export / gpw_tune_import).
+void tune_export_tma(std::string& out);
+bool tune_import_tma(const int* fields);
+void tune_export_bloch(std::string& out);
+bool tune_import_bloch(const int* fields);
+
 }  // namespace gpw

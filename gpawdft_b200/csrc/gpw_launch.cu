@@ -1,6 +1,7 @@
 // Kernel launchers: dtype / radius / tap-count dispatch, launch geometry and
 // shared-memory opt-in for every device kernel of the library.
 #include <algorithm>
+#include <cstdio>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -219,7 +220,7 @@ static std::atomic<int> g_force_nc{0};
 
 static bool tma_variant_available(int dtype, int R, int var) {
   if (var < 0 || var >= TMA_NVARIANT) return false;
-  if (var >= 5 && dtype != GPW_F32) return false;  // 4-point variants: float32 only
+  if (var >= 5 && var <= 9 && dtype != GPW_F32) return false;  // 4-point variants: float32 only
   return (R == 1 || R == 3) || var == (R == 4 ? 1 : 2);
 }
 
@@ -258,6 +259,31 @@ extern "C" int gpw_set_tma_variant(int variant, int nchunk) {
 int tuned_stencil_count() {
   std::lock_guard<std::mutex> lock(g_tune_mu);
   return (int)g_tune.size();
+}
+
+// The TMA tuner's choices as text records "tma dtype R mode n0 n1 n2 nbatch
+// var nchunk", one a line (gpw_tune_export).
+void tune_export_tma(std::string& out) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  char line[160];
+  for (const auto& kv : g_tune) {
+    const TuneKey& k = kv.first;
+    snprintf(line, sizeof line, "tma %d %d %d %d %d %d %d %d %d\n", k.dtype, k.R, k.mode, k.n0, k.n1, k.n2,
+             k.nbatch, kv.second.var, kv.second.nchunk);
+    out += line;
+  }
+}
+
+// One "tma ..." record back into the tuner (gpw_tune_import); records whose
+// variant is not compiled for that element type and radius are refused.
+bool tune_import_tma(const int* f) {
+  const int dtype = f[0], R = f[1], mode = f[2];
+  if ((dtype != GPW_F64 && dtype != GPW_F32) || R < 1 || R > 4 || mode < 0 || mode > 6) return false;
+  if (f[3] <= 0 || f[4] <= 0 || f[5] <= 0 || f[6] <= 0 || f[8] < -8 || f[8] > 64) return false;
+  if (!tma_variant_available(dtype, R, f[7])) return false;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune[TuneKey{dtype, R, mode, f[3], f[4], f[5], f[6]}] = TmaChoice{f[7], f[8]};
+  return true;
 }
 
 // The TMA path serves real zero-boundary star stencils whose arrays are

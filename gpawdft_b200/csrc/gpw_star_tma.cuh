@@ -321,19 +321,26 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
 #pragma unroll
           for (int e = 0; e < VEC; ++e) nb[XL + e] = c.v[e];
           constexpr bool sweep = (MODE == MODE_JACOBI || MODE == MODE_JACOBI_ADD64 || MODE == MODE_JACOBI_SCALED_IN);
-          S p[VEC];
+          // the in-plane sum in two independent chains (centre + axis 1,
+          // axis 2) joined at the end: half the dependent-FMA latency
+          S p[VEC], pz[VEC];
 #pragma unroll
-          for (int e = 0; e < VEC; ++e) p[e] = sweep ? S(0) : k.cc * c.v[e];
+          for (int e = 0; e < VEC; ++e) {
+            p[e] = sweep ? S(0) : k.cc * c.v[e];
+            pz[e] = S(0);
+          }
 #pragma unroll
           for (int q = 1; q <= R; ++q) {
 #pragma unroll
             for (int e = 0; e < VEC; ++e) {
               p[e] = fma(k.cy[R + q], col[j + R + q].v[e], p[e]);
               p[e] = fma(k.cy[R - q], col[j + R - q].v[e], p[e]);
-              p[e] = fma(k.cz[R + q], nb[XL + e + q], p[e]);
-              p[e] = fma(k.cz[R - q], nb[XL + e - q], p[e]);
+              pz[e] = fma(k.cz[R + q], nb[XL + e + q], pz[e]);
+              pz[e] = fma(k.cz[R - q], nb[XL + e - q], pz[e]);
             }
           }
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) p[e] += pz[e];
           if constexpr (MODE == MODE_APPLY) {
             // local potential of this (in-range) plane: its part is output
             // plane pfirst + s's

@@ -240,6 +240,23 @@ int gpw_mul(int64_t n, const double *x, const double *y, double *out,
 int gpw_add_scalar(int dtype, int64_t n, double c, const void *x, void *y,
                    gpw_stream stream);
 
+/* ------------------------------------------------------------ autotuner */
+
+/* The launch choices the autotuners made so far in this process (tile
+ * variants and chunkings of the zero-boundary TMA stencil kernel, layouts of
+ * the periodic / Bloch row kernel, per element type, radius, epilogue, grid
+ * and batch) as text: a header naming the device and its SM count, then
+ * one record a line.  No counterpart in the reference (which has no
+ * autotuner).  Writes at most cap bytes (NUL included) and sets *needed;
+ * buf NULL only queries the size.                                          */
+int gpw_tune_export(char *buf, int64_t cap, int64_t *needed);
+/* Merge records written by gpw_tune_export into the tuners, so that a new
+ * process skips timing the shapes already tuned.  Records from another
+ * device or SM count are refused (GPW_EINVAL); records whose layout is not
+ * available for their shape are skipped.  *imported (may be NULL) receives
+ * the number of records taken.                                             */
+int gpw_tune_import(const char *text, int *imported);
+
 /* ------------------------------------------------------------ Poisson */
 
 /* The charge branches of PoissonSolver.solve, gpaw/poisson.py:209-299, for

@@ -154,15 +154,18 @@ def test_training_reduces_loss(cuda):
     assert np.isfinite(last) and last < 0.5 * first, hist
 
 
-def test_warm_start_gain(cuda):
-    """What the trained network gains over the zero start, measured on
-    held-out densities (32^3 grids, float32 defect correction to relative
-    residual 1e-10).  The multigrid finishes every solve to the tolerance
-    and judges the guess after its first iteration, so the warm start costs
-    at most that judged iteration over the zero start.  The network's
-    held-out prediction error shows that it learned the potential; its bf16
-    activations leave grid-scale noise that the first smoothing removes, so
-    the iteration count moves by at most one either way."""
+def test_warm_start_measured_and_safeguarded(cuda):
+    """The trained network on held-out densities (32^3 grids, float32 defect
+    correction to relative residual 1e-10): what it gives is measured here,
+    not claimed.  Asserted: the network has learned the potential (held-out
+    prediction error below 50%); the multigrid finishes every solve to the
+    tolerance; judging each guess after one iteration bounds the cost of a
+    bad guess to that iteration; and the fallback to the zero start engages
+    for a guess that makes the residual grow (the prediction scaled by -50:
+    one V-cycle, contracting errors by ~0.15, leaves more residual than the
+    zero start had).  The network does not reduce the iteration count
+    on average at this precision (its bf16 activations leave grid-scale
+    noise), so no gain is asserted; the counts are printed."""
     import torch
     from gpawdft_b200 import blas, learned
     net = learned.PoissonUNet(seed=2)
@@ -183,6 +186,18 @@ def test_warm_start_gain(cuda):
     assert (ps.last_errors <= eps).all()
     assert err.max() < 0.5, err
     assert (n_warm <= n_zero + 1).all(), (n_warm, n_zero)
+    # a guess worse than zero is caught by the judging iteration
+    good_predict = net.predict
+    net.predict = lambda r, N=None: -50.0 * good_predict(r, N)
+    try:
+        phi_bad, used_bad, kb = learned.warm_start(net, ps, rho)
+    finally:
+        net.predict = good_predict
+    assert not used_bad.any()
+    assert float(phi_bad.abs().max().item()) == 0.0
+    n_bad = ps.solve_batch(phi_bad, rho, eps=eps) + kb
+    assert (n_bad == n_zero + 1).all(), (n_bad, n_zero)
     print('held-out prediction error %s; outer iterations zero start %s, '
-          'warm start %s (guess kept: %s)' % (np.round(err, 3), n_zero,
-                                              n_warm, used))
+          'warm start %s (guess kept: %s, mean change %+.2f)'
+          % (np.round(err, 3), n_zero, n_warm, used,
+             float(np.mean(n_warm - n_zero))))
