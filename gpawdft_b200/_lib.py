@@ -24,12 +24,14 @@ GPW_F64, GPW_C128, GPW_F32, GPW_C64 = 0, 1, 2, 3
 EXPORTS = [
     'gpw_last_error', 'gpw_version',
     'gpw_operator_new', 'gpw_operator_apply', 'gpw_operator_apply_potential',
+    'gpw_operator_apply_fused',
     'gpw_operator_relax',
     'gpw_operator_get_diagonal_element', 'gpw_operator_residual',
     'gpw_operator_residual_noalloc', 'gpw_operator_free',
     'gpw_woperator_new', 'gpw_woperator_apply', 'gpw_woperator_relax',
     'gpw_woperator_get_diagonal_element', 'gpw_woperator_free',
     'gpw_transformer_new', 'gpw_transformer_apply', 'gpw_transformer_free',
+    'gpw_transformer_apply_subtract',
     'gpw_axpy', 'gpw_scal', 'gpw_sum', 'gpw_dot', 'gpw_dotc_pairs',
     'gpw_copy_box', 'gpw_mul', 'gpw_tune_export', 'gpw_tune_import',
     'gpw_add_scalar',
@@ -67,6 +69,9 @@ _SIGS = {
     'gpw_operator_apply_potential': (ctypes.c_int, [_vp, ctypes.c_int, _vp,
                                                     _vp, ctypes.c_int64, _vp,
                                                     _vp, _vp]),
+    'gpw_operator_apply_fused': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp,
+                                                ctypes.c_int64, _vp, _vp, _vp,
+                                                ctypes.c_double, _vp]),
     'gpw_operator_relax': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int,
                                           _vp, _vp, ctypes.c_int64,
                                           ctypes.c_int, ctypes.c_double,
@@ -95,6 +100,9 @@ _SIGS = {
     'gpw_transformer_apply': (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp,
                                              ctypes.c_int64, _vp, _vp]),
     'gpw_transformer_free': (None, [_vp]),
+    'gpw_transformer_apply_subtract': (ctypes.c_int, [_vp, ctypes.c_int, _vp,
+                                                      _vp, _vp, ctypes.c_int64,
+                                                      _vp, _vp]),
     'gpw_axpy': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_double,
                                 ctypes.c_double, _vp, _vp, _vp]),
     'gpw_scal': (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_double,

@@ -216,7 +216,7 @@ int gpw_operator_get_diagonal_element(const gpw_operator* op, double* out) {
 }
 
 static int operator_apply(gpw_operator* op, int dtype, const void* in, void* out, int64_t nin, const double* phases,
-                          const void* pot, gpw_stream stream) {
+                          const void* pot, gpw_stream stream, const void* aux = nullptr, double aux_scale = 0.0) {
   if (!op || !in || !out) return fail(GPW_EINVAL, "null argument");
   if (!valid_dtype(dtype)) return fail(GPW_EINVAL, "bad dtype");
   if (nin < 0) return fail(GPW_EINVAL, "nin < 0");
@@ -225,10 +225,10 @@ static int operator_apply(gpw_operator* op, int dtype, const void* in, void* out
     // grid.z = nchunk * nbatch; split very large batches
     const int64_t half = nin / 2;
     const size_t es = elt_size(dtype) * (size_t)op->d.n[0] * op->d.n[1] * op->d.n[2];
-    int rc = operator_apply(op, dtype, in, out, half, phases, pot, stream);
+    int rc = operator_apply(op, dtype, in, out, half, phases, pot, stream, aux, aux_scale);
     if (rc) return rc;
     return operator_apply(op, dtype, (const char*)in + half * es, (char*)out + half * es, nin - half, phases, pot,
-                          stream);
+                          stream, aux ? (const char*)aux + half * es : nullptr, aux_scale);
   }
   cudaStream_t st = (cudaStream_t)stream;
   const OpDesc& d = op->d;
@@ -245,7 +245,8 @@ static int operator_apply(gpw_operator* op, int dtype, const void* in, void* out
   Boundary bc = make_boundary(d.periodic, dtype, phases);
   GridSum gs{};
   cudaError_t e =
-      launch_stencil(d, dtype, MODE_APPLY, src, v, out, v, nullptr, v, (int)nin, bc, 1.0, nullptr, gs, st, pot);
+      launch_stencil(d, dtype, MODE_APPLY, src, v, out, v, nullptr, v, (int)nin, bc, 1.0, nullptr, gs, st, pot, aux,
+                     aux_scale);
   if (e != cudaSuccess) return cuda_fail(e, "operator apply launch");
   return GPW_OK;
 }
@@ -253,6 +254,13 @@ static int operator_apply(gpw_operator* op, int dtype, const void* in, void* out
 int gpw_operator_apply(gpw_operator* op, int dtype, const void* in, void* out, int64_t nin, const double* phases,
                        gpw_stream stream) {
   return operator_apply(op, dtype, in, out, nin, phases, nullptr, stream);
+}
+
+int gpw_operator_apply_fused(gpw_operator* op, int dtype, const void* in, void* out, int64_t nin,
+                             const double* phases, const void* pot, const void* aux, double aux_scale,
+                             gpw_stream stream) {
+  if (pot && pot == out) return fail(GPW_EINVAL, "apply_fused: the potential must not alias the output");
+  return operator_apply(op, dtype, in, out, nin, phases, pot, stream, aux, aux ? aux_scale : 0.0);
 }
 
 int gpw_operator_apply_potential(gpw_operator* op, int dtype, const void* in, void* out, int64_t nin,
@@ -393,6 +401,21 @@ int gpw_transformer_apply(gpw_transformer* t, int dtype, const void* in, void* o
   Boundary bc = make_boundary(t->d.periodic, dtype, phases);
   cudaError_t e =
       launch_transfer(t->d, dtype, in, vi, out, vo, (int)nin, bc, 0, nullptr, nullptr, nullptr, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "transformer launch");
+  return GPW_OK;
+}
+
+int gpw_transformer_apply_subtract(gpw_transformer* t, int dtype, const void* in, const void* base, void* out,
+                                   int64_t nin, const double* phases, gpw_stream stream) {
+  if (!t || !in || !out || !base) return fail(GPW_EINVAL, "null argument");
+  if (!valid_dtype(dtype)) return fail(GPW_EINVAL, "bad dtype");
+  if (!t->d.interpolate) return fail(GPW_EINVAL, "apply_subtract: interpolating transformers only");
+  if (nin <= 0 || nin > 8192) return fail(GPW_EINVAL, "apply_subtract: 1 <= nin <= 8192");
+  if (in == out || base == out) return fail(GPW_EINVAL, "apply_subtract: out must differ from in and base");
+  GridView vi = contiguous_view(t->d.nin), vo = contiguous_view(t->d.nout);
+  Boundary bc = make_boundary(t->d.periodic, dtype, phases);
+  cudaError_t e =
+      launch_transfer(t->d, dtype, in, vi, out, vo, (int)nin, bc, 1, base, &vo, nullptr, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(e, "transformer launch");
   return GPW_OK;
 }

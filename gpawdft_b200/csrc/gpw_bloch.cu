@@ -112,7 +112,8 @@ std::vector<BlochChoice> bloch_candidates(int dtype, int R, const GridView& v) {
 
 template <typename T, int R, int VEC, int NW, int WPR>
 cudaError_t bloch_run(const void* in, const GridView& vin, void* out, const GridView& vout, int nbatch,
-                      const Boundary& bc, const StarCoefs& sc, int nchunk, const void* pot, cudaStream_t st) {
+                      const Boundary& bc, const StarCoefs& sc, int nchunk, const void* pot, const void* aux,
+                      double aux_scale, cudaStream_t st) {
   using C = BlochCfg<T, R, VEC, NW, BLOCH_D, WPR>;
   using S = typename EltTraits<T>::S;
   constexpr bool cpx = EltTraits<T>::cpx;
@@ -143,6 +144,8 @@ cudaError_t bloch_run(const void* in, const GridView& vin, void* out, const Grid
   a.stage_bytes = stage;
   a.status = device_status_word();
   a.pot = pot;
+  a.aux = aux;
+  a.aux_scale = aux_scale;
   BlochCoefs<S> k{};
   bool has_y = false, has_z = false;
   for (int i = 0; i <= 2 * R; ++i) {
@@ -165,10 +168,10 @@ cudaError_t bloch_run(const void* in, const GridView& vin, void* out, const Grid
 template <typename T, int R>
 cudaError_t bloch_run_layout(const BlochChoice& c, const void* in, const GridView& vin, void* out,
                              const GridView& vout, int nbatch, const Boundary& bc, const StarCoefs& sc,
-                             const void* pot, cudaStream_t st) {
+                             const void* pot, const void* aux, double aux_scale, cudaStream_t st) {
 #define GPW_BLOCH_CASE(V, N, W)                                                                 \
   if (c.vec == V && c.nw == N && c.wpr == W)                                                    \
-    return bloch_run<T, R, V, N, W>(in, vin, out, vout, nbatch, bc, sc, c.nchunk, pot, st);
+    return bloch_run<T, R, V, N, W>(in, vin, out, vout, nbatch, bc, sc, c.nchunk, pot, aux, aux_scale, st);
   // a warp per row
   GPW_BLOCH_CASE(1, 4, 1) GPW_BLOCH_CASE(1, 8, 1)
   GPW_BLOCH_CASE(2, 4, 1) GPW_BLOCH_CASE(2, 8, 1)
@@ -188,23 +191,25 @@ cudaError_t bloch_run_layout(const BlochChoice& c, const void* in, const GridVie
 template <typename T>
 cudaError_t bloch_dispatch(int R, const BlochChoice& ch, const void* in, const GridView& vin, void* out,
                            const GridView& vout, int nbatch, const Boundary& bc, const StarCoefs& sc,
-                           const void* pot, cudaStream_t st) {
+                           const void* pot, const void* aux, double aux_scale, cudaStream_t st) {
   switch (R) {
-    case 1: return bloch_run_layout<T, 1>(ch, in, vin, out, vout, nbatch, bc, sc, pot, st);
-    case 2: return bloch_run_layout<T, 2>(ch, in, vin, out, vout, nbatch, bc, sc, pot, st);
-    case 3: return bloch_run_layout<T, 3>(ch, in, vin, out, vout, nbatch, bc, sc, pot, st);
+    case 1: return bloch_run_layout<T, 1>(ch, in, vin, out, vout, nbatch, bc, sc, pot, aux, aux_scale, st);
+    case 2: return bloch_run_layout<T, 2>(ch, in, vin, out, vout, nbatch, bc, sc, pot, aux, aux_scale, st);
+    case 3: return bloch_run_layout<T, 3>(ch, in, vin, out, vout, nbatch, bc, sc, pot, aux, aux_scale, st);
   }
   return cudaErrorInvalidValue;
 }
 
 cudaError_t bloch_launch(int dtype, int R, const BlochChoice& ch, const void* in, const GridView& vin, void* out,
                          const GridView& vout, int nbatch, const Boundary& bc, const StarCoefs& sc,
-                         const void* pot, cudaStream_t st) {
+                         const void* pot, const void* aux, double aux_scale, cudaStream_t st) {
   switch (dtype) {
-    case GPW_F64: return bloch_dispatch<double>(R, ch, in, vin, out, vout, nbatch, bc, sc, pot, st);
-    case GPW_F32: return bloch_dispatch<float>(R, ch, in, vin, out, vout, nbatch, bc, sc, pot, st);
-    case GPW_C128: return bloch_dispatch<double2>(R, ch, in, vin, out, vout, nbatch, bc, sc, pot, st);
-    case GPW_C64: return bloch_dispatch<float2>(R, ch, in, vin, out, vout, nbatch, bc, sc, pot, st);
+    case GPW_F64: return bloch_dispatch<double>(R, ch, in, vin, out, vout, nbatch, bc, sc, pot, aux, aux_scale, st);
+    case GPW_F32: return bloch_dispatch<float>(R, ch, in, vin, out, vout, nbatch, bc, sc, pot, aux, aux_scale, st);
+    case GPW_C128:
+      return bloch_dispatch<double2>(R, ch, in, vin, out, vout, nbatch, bc, sc, pot, aux, aux_scale, st);
+    case GPW_C64:
+      return bloch_dispatch<float2>(R, ch, in, vin, out, vout, nbatch, bc, sc, pot, aux, aux_scale, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -274,7 +279,8 @@ cudaError_t launch_bloch(const OpDesc& d, int dtype, const StencilArgs& sa, int 
   if (cands.empty()) return cudaErrorInvalidValue;
   auto run = [&](const BlochChoice& c) {
     return c.vec == 0 ? launch_apply_cpasync(d, dtype, sa, nbatch, st)
-                      : bloch_launch(dtype, d.R, c, in, vin, out, vout, nbatch, bc, d.sc, sa.pot, st);
+                      : bloch_launch(dtype, d.R, c, in, vin, out, vout, nbatch, bc, d.sc, sa.pot, sa.aux,
+                                     sa.aux_scale, st);
   };
   // pinned layout (test hook): the shape's forced-th candidate, if it has one
   const int forced = g_bloch_force.load();

@@ -65,6 +65,8 @@ struct BlochArgs {
   int* status;
   const void* pot;        // optional local potential (scalar type, the output's
                           // layout without batch): out = A in + pot in
+  const void* aux;        // optional grids in the output's layout and type:
+  double aux_scale;       //   out += aux_scale aux
 };
 
 __device__ __forceinline__ void mbar_arrive(unsigned bar) {
@@ -281,13 +283,16 @@ __global__ void __launch_bounds__(32 * NW, (BlochCfg<T, R, VEC, NW, D, WPR>::MIN
       // output plane o is complete: logical slot 0 = physical ph
       if (o >= z0 && nx > 0) {
         T* op0 = outb + (int64_t)o * a.vout.s0;
+        const T* ax0 = a.aux ? static_cast<const T*>(a.aux) + (op0 - static_cast<T*>(a.out)) : nullptr;
+        using S = typename EltTraits<T>::S;
 #pragma unroll
         for (int j = 0; j < PY; ++j) {
           if (j < nrows_ok) {
             T* op = op0 + j * a.vout.s1;
 #pragma unroll
             for (int e = 0; e < VEC; ++e)
-              if (e < nx) op[e] = acc[j][ph][e];
+              if (e < nx)
+                op[e] = ax0 ? fmac((S)a.aux_scale, ax0[j * a.vout.s1 + e], acc[j][ph][e]) : acc[j][ph][e];
           }
         }
       }

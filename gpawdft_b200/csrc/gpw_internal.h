@@ -86,7 +86,8 @@ int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& vout, i
 cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, void* out,
                            const GridView& vout, const void* rho, const GridView& vrho, int nbatch,
                            const Boundary& bc, double w, const unsigned char* active, const GridSum& gs,
-                           cudaStream_t st, const void* pot = nullptr);
+                           cudaStream_t st, const void* pot = nullptr, const void* aux = nullptr,
+                           double aux_scale = 0.0);
 
 // Fused defect-correction steps (TMA kernel; zero boundaries, 16-byte-pitched
 // engine buffers).  mode MODE_RESID_DC: in/rho float64, out (rhs) and out2

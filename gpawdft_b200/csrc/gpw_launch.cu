@@ -306,9 +306,11 @@ static bool tma_path_ok(const OpDesc& d, int dtype, int mode, const void* in, co
 cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in, const GridView& vin, void* out,
                            const GridView& vout, const void* rho, const GridView& vrho, int nbatch,
                            const Boundary& bc, double w, const unsigned char* active, const GridSum& gs,
-                           cudaStream_t st, const void* pot) {
+                           cudaStream_t st, const void* pot, const void* aux, double aux_scale) {
   StencilArgs a{};
   a.pot = mode == MODE_APPLY ? pot : nullptr;
+  a.aux = mode == MODE_APPLY ? aux : nullptr;
+  a.aux_scale = aux_scale;
   a.in = in;
   a.out = out;
   a.rho = rho;

@@ -381,6 +381,13 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
                   (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
               if constexpr (MODE == MODE_APPLY) {
                 res = av;
+                if (a.aux) {
+                  const S* xp = static_cast<const S*>(a.aux) + oidx;
+                  const S g = (S)a.aux_scale;
+#pragma unroll
+                  for (int e = 0; e < VEC; ++e)
+                    if (e < nx) res.v[e] = fma(g, xp[e], res.v[e]);
+                }
               } else if constexpr (C::RR) {
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) res.v[e] = av.v[e] - rho.v[e];

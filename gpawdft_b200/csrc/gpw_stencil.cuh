@@ -78,6 +78,8 @@ struct StencilArgs {
   GridView vco;     // RESID_RESTRICT: the next level's view (out, out2)
   const void* pot;  // APPLY: optional local potential, one grid in the output's
                     // layout and the element's scalar type: out = A in + pot in
+  const void* aux;  // APPLY: optional grids in the output's layout and type:
+  double aux_scale; //   out += aux_scale aux
 };
 
 struct GeneralCoefs {
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(GEN_TZ* GEN_TY)
             const S pv = static_cast<const S*>(a.pot)[(int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x];
             acc = fmac(pv, sl[(ty + mp) * W + tx + mp], acc);
           }
+          if (a.aux) acc = fmac((S)a.aux_scale, static_cast<const T*>(a.aux)[oi], acc);
           static_cast<T*>(a.out)[oi] = acc;
         } else {
           const int64_t ri = (int64_t)b * a.vrho.sb + (int64_t)o * a.vrho.s0 + (int64_t)y * a.vrho.s1 + x;
@@ -436,7 +439,8 @@ __global__ void __launch_bounds__(StarCfg<R, T>::NT)
             const int64_t oi = (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
             const T av = acc[j][0];
             if constexpr (MODE == MODE_APPLY) {
-              static_cast<T*>(a.out)[oi] = av;
+              static_cast<T*>(a.out)[oi] =
+                  a.aux ? fmac((S)a.aux_scale, static_cast<const T*>(a.aux)[oi], av) : av;
             } else if constexpr (MODE == MODE_RESIDUAL) {
               const T r = sub(av, rho[j]);
               if (a.out) static_cast<T*>(a.out)[oi] = r;

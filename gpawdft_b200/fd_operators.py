@@ -162,6 +162,43 @@ class FDOperator:
         if not arrays.is_device(out_xg):
             arrays.writeback(out_xg, dst)
 
+    def scaled(self, alpha, beta=0.0):
+        """The operator alpha A + beta I: coefficients scaled by alpha on the
+        host, beta added to the centre (new API; lets the glue around an
+        apply fold into it, see ``apply_fused``)."""
+        coef = np.array(self.coef_p, float) * alpha
+        centre = [i for i, o in enumerate(self.offset_pc) if not np.any(o)]
+        if centre:
+            coef[centre[0]] += beta
+            op = FDOperator(coef, self.offset_pc, self.gd, self.dtype)
+        else:
+            op = FDOperator(np.hstack(([beta], coef)),
+                            np.vstack(([[0, 0, 0]], self.offset_pc)),
+                            self.gd, self.dtype)
+        op.description = '%s scaled' % self.description
+        return op
+
+    def apply_fused(self, in_xg, out_xg, phase_cd=None, vt_g=None, aux=None,
+                    aux_scale=1.0):
+        """out = A in + vt in + aux_scale aux in one pass (new API;
+        gpw_operator_apply_fused).  Device tensors."""
+        self._check_grid(in_xg)
+        code = arrays.code_of(in_xg)
+        nin = int(np.prod(in_xg.shape[:-3])) if len(in_xg.shape) > 3 else 1
+        src = arrays.to_device(in_xg)
+        dst = arrays.to_device(out_xg)
+        pot = None if vt_g is None else arrays.to_device(vt_g)
+        ax = None if aux is None else arrays.to_device(aux)
+        if ax is not None and (tuple(ax.shape) != tuple(dst.shape) or
+                               arrays.code_of(ax) != code):
+            raise ValueError('aux must have the output\'s shape and dtype')
+        pbuf, pptr = arrays.phases_arg(phase_cd)
+        _lib.check(self._lib.gpw_operator_apply_fused(
+            self._h, code, arrays.ptr(src), arrays.ptr(dst), nin, pptr,
+            None if pot is None else arrays.ptr(pot),
+            None if ax is None else arrays.ptr(ax), float(aux_scale),
+            arrays.stream()))
+
     def relax(self, relax_method, f_g, s_g, n, w=None):
         """n relaxation sweeps of A f = s (c/operators.c:49-91), in place.
 

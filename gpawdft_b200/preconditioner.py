@@ -5,7 +5,7 @@ runs the fixed three-grid smoothing sequence of gpaw/preconditioner.py:34-60
 on a block of residuals: restrictions / interpolations (nn=1 Transformers
 with the k-point's Bloch phases), the caller's kinetic operator on the fine
 grid and nn=1 Laplacians (scale -1/2) on the two coarse grids, with the
-array arithmetic as device axpy / scal kernels.  Returns a device view of
+array arithmetic folded into those launches (see ``__call__``).  Returns a device view of
 internal scratch (as the reference returns a view of its scratch arrays) --
 or a NumPy array when the residuals were NumPy.
 """
@@ -42,7 +42,36 @@ class Preconditioner:
     def calculate_kinetic_energy(self, psit_xG, kpt):
         return None
 
+    def _fused_operators(self):
+        """The scaled operators that fold the sequence's array arithmetic
+        into the applies (built once, on the host)."""
+        if getattr(self, '_ops', None) is None:
+            step = self.step
+            self._ops = (self.kin1.scaled(-4 * step, 1.0),       # q1 from s1
+                         self.kin2.scaled(-256 * step * step, 32 * step),
+                         self.kin1.scaled(4 * step, -1.0),       # -d1''
+                         self.kin0.scaled(step, -1.0))           # the result
+        return self._ops
+
     def __call__(self, residuals, kpt, ekin=None):
+        """gpaw/preconditioner.py:34-60 in eight fused launches.
+
+        With s1 = R0(residuals) (so the reference's r1 = R0(-residuals) is
+        -s1) the reference's sequence is, exactly in real arithmetic,
+          q1  = (I - 4 step A1) s1                      (d1 = -4 step s1)
+          r2  = R1(q1)
+          d2  = (32 step I - 256 step^2 A2) r2          (its d2 after the update)
+          d1  = -4 step s1 - I2(d2)
+          -d1 = (4 step A1 - I) d1 + 4 step s1          (its d1 after the update)
+          d0  = I1(-d1)
+          out = (step A0 - I) d0 - step residuals       (its -(d0 - step q0))
+        Every line is one launch: a transfer, or an apply of an operator whose
+        coefficients were scaled on the host, its additive term folded into
+        the apply's output stage (gpw_operator_apply_fused) or the
+        interpolation's (gpw_transformer_apply_subtract).  Rounding differs
+        from the reference's step-by-step NumPy arithmetic only in the last
+        bits.
+        """
         phases = getattr(kpt, 'phase_cd', kpt)
         host = not arrays.is_device(residuals)
         res = arrays.to_device(residuals)
@@ -53,34 +82,21 @@ class Preconditioner:
         if nb > self.block:
             raise ValueError('more residuals than the preconditioner block')
         step = self.step
-        d0, q0 = self.scratch0[:, :nb]
-        r1, d1, q1 = self.scratch1[:, :nb]
-        r2, d2, q2 = self.scratch2[:, :nb]
-        # r1 = R0(-residuals): restriction is linear and exact under negation
-        self.restrictor0(res, r1, phases)
-        blas.scal(-1.0, r1)
-        d1.copy_(r1)
-        blas.scal(4 * step, d1)                      # d1 = 4 step r1
-        self.kin1.apply(d1, q1, phases)
-        blas.axpy(-1.0, r1, q1)                      # q1 -= r1
-        self.restrictor1(q1, r2, phases)
-        d2.copy_(r2)
-        blas.scal(16 * step, d2)                     # d2 = 16 step r2
-        self.kin2.apply(d2, q2, phases)
-        blas.axpy(-1.0, r2, q2)                      # q2 -= r2
-        blas.axpy(-16 * step, q2, d2)                # d2 -= 16 step q2
-        self.interpolator2(d2, q1, phases)
-        blas.axpy(-1.0, q1, d1)                      # d1 -= q1
-        self.kin1.apply(d1, q1, phases)
-        blas.axpy(-1.0, r1, q1)                      # q1 -= r1
-        blas.axpy(-4 * step, q1, d1)                 # d1 -= 4 step q1
-        self.interpolator1(d1, d0, phases)
-        blas.scal(-1.0, d0)                          # d0 = I1(-d1)
-        self.kin0.apply(d0, q0, phases)
-        blas.axpy(-1.0, res, q0)                     # q0 -= residuals
-        blas.axpy(-step, q0, d0)                     # d0 -= step q0
-        blas.scal(-1.0, d0)                          # d0 *= -1
-        out = d0[0] if single else d0
+        op1a, op2, op1b, op0 = self._fused_operators()
+        out, d0 = self.scratch0[:, :nb]
+        s1, t1, u1 = self.scratch1[:, :nb]
+        r2, d2, _ = self.scratch2[:, :nb]
+        self.restrictor0(res, s1, phases)                   # s1 = R0(res)
+        op1a.apply(s1, u1, phases)                           # q1
+        self.restrictor1(u1, r2, phases)                     # r2
+        op2.apply(r2, d2, phases)                            # d2
+        t1.copy_(s1)
+        blas.scal(-4 * step, t1)                             # d1 = -4 step s1
+        self.interpolator_object2.apply_subtract(d2, t1, u1, phases)
+        op1b.apply_fused(u1, t1, phases, aux=s1, aux_scale=4 * step)
+        self.interpolator1(t1, d0, phases)                   # d0 = I1(-d1)
+        op0.apply_fused(d0, out, phases, aux=res, aux_scale=-step)
+        result = out[0] if single else out
         if host:
-            return out.cpu().numpy()
-        return out
+            return result.cpu().numpy()
+        return result

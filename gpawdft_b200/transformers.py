@@ -106,6 +106,17 @@ class _Transformer:
         del dev_out
         return output
 
+    def apply_subtract(self, input, base, output, phases=None):
+        """output = base - I(input) in one pass (interpolation only; device
+        tensors; gpw_transformer_apply_subtract)."""
+        code = arrays.code_of(input)
+        nin = int(np.prod(input.shape[:-3])) if len(input.shape) > 3 else 1
+        pbuf, pptr = arrays.phases_arg(phases)
+        _lib.check(self._lib.gpw_transformer_apply_subtract(
+            self._h, code, arrays.ptr(input), arrays.ptr(base),
+            arrays.ptr(output), nin, pptr, arrays.stream()))
+        return output
+
     def get_async_sizes(self):
         return (0, 1)
 

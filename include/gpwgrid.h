@@ -98,6 +98,17 @@ int gpw_operator_apply_potential(gpw_operator *op, int dtype, const void *in,
                                  void *out, int64_t nin, const double *phases,
                                  const void *pot, gpw_stream stream);
 
+/* The apply with the NumPy glue that follows it folded into its output
+ * stage: out = A in + pot in + aux_scale aux (pot and aux may be NULL; aux
+ * is `nin` grids of the element type, as `out`).  Together with an operator
+ * whose coefficients were scaled on the host it replaces sequences such as
+ * the preconditioner's `kin0.apply(d0, q0); q0 -= residuals; axpy(-step,
+ * q0, d0); d0 *= -1` (gpaw/preconditioner.py:56-60) by one pass.          */
+int gpw_operator_apply_fused(gpw_operator *op, int dtype, const void *in,
+                             void *out, int64_t nin, const double *phases,
+                             const void *pot, const void *aux,
+                             double aux_scale, gpw_stream stream);
+
 /* Operator.relax(relax_method, func, source, nrelax, w), c/operators.c:49-91
  * and c/bmgs/relax.c:7-73.  relax_method 2 = weighted Jacobi (each sweep
  * func = (1-w) func + w (source - sum_{p!=0} c_p func[x+o_p]) / c_0);
@@ -195,6 +206,15 @@ int gpw_transformer_new(const int64_t size_in[3], const int64_t size_out[3],
 int gpw_transformer_apply(gpw_transformer *tr, int dtype, const void *in,
                           void *out, int64_t nin, const double *phases,
                           gpw_stream stream);
+
+/* out = base - I(in) for an interpolating transformer: the interpolation
+ * and the subtraction that follows it (gpaw/poisson.py:351-352 `phis -=
+ * residual`, gpaw/preconditioner.py:49-50 `d1 -= q1`) in one pass; `base`
+ * has the output's shape and must not alias `out`.                         */
+int gpw_transformer_apply_subtract(gpw_transformer *tr, int dtype,
+                                   const void *in, const void *base,
+                                   void *out, int64_t nin,
+                                   const double *phases, gpw_stream stream);
 
 void gpw_transformer_free(gpw_transformer *tr);
 

@@ -143,3 +143,50 @@ def test_rejects_bad_potential(cuda):
         kin.apply_potential(psi, out, vt.astype(np.float32), ph)
     with pytest.raises(ValueError):
         kin.apply_potential(psi, out, vt[:8], ph)
+
+
+@pytest.mark.parametrize('case', ['bloch-c128', 'bloch-c64', 'tma-f64',
+                                  'cpasync-c128', 'general-c128'])
+def test_apply_fused_aux(cuda, case):
+    """out = A in + vt in + g aux (gpw_operator_apply_fused) on every apply
+    kernel, and an operator scaled on the host (alpha A + beta I)."""
+    import torch
+    from gpawdft_b200.fd_operators import Laplace
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    if case == 'general-c128':
+        cell = [(0, 2.55, 2.55), (2.55, 0, 2.55), (2.55, 2.55, 0)]
+        N, pbc, dtype, nn = (14, 14, 14), 1, complex, 2
+    else:
+        dtype = {'bloch-c128': complex, 'bloch-c64': np.complex64,
+                 'tma-f64': float, 'cpasync-c128': complex}[case]
+        N = (16, 20, 130) if case == 'cpasync-c128' else (32, 32, 32)
+        cell = tuple(0.2 * n for n in N)
+        pbc, nn = (0 if case == 'tma-f64' else 1), 3
+    if case == 'tma-f64':
+        N = (41, 37, 45)
+        cell = tuple(0.2 * n for n in N)
+    gd = GridDescriptor(N, cell, pbc)
+    ogd = OGD(N, cell, pbc)
+    kin = Laplace(gd, -0.5, nn, dtype)
+    okin = ol.Laplace(ogd, -0.5, nn, oracle_dtype(dtype), BACKEND)
+    psi = rand((2,) + tuple(gd.n_c), dtype, 21)
+    aux = rand((2,) + tuple(gd.n_c), dtype, 22)
+    sdt = np.float32 if np.dtype(dtype) in (np.float32, np.complex64) \
+        else np.float64
+    vt = rand(tuple(gd.n_c), sdt, 23)
+    ph = None if np.dtype(dtype).kind == 'f' else \
+        phase_cd_for_k(ogd, (0.15, -0.3, 0.35))
+    want = _oracle(okin, psi, vt, ph) - 0.7 * aux.astype(
+        oracle_dtype(dtype))
+    x = torch.from_numpy(psi).cuda()
+    out = torch.empty_like(x)
+    kin.apply_fused(x, out, ph, vt_g=torch.from_numpy(vt).cuda(),
+                    aux=torch.from_numpy(aux).cuda(), aux_scale=-0.7)
+    assert relerr(out.cpu().numpy(), want) < TOL[np.dtype(dtype)]
+    # alpha A + beta I built on the host
+    op = kin.scaled(0.3, -1.25)
+    op.apply_fused(x, out, ph)
+    o2 = np.empty_like(psi.astype(oracle_dtype(dtype)))
+    okin.apply(psi.astype(oracle_dtype(dtype)), o2, ph)
+    want2 = 0.3 * o2 - 1.25 * psi.astype(oracle_dtype(dtype))
+    assert relerr(out.cpu().numpy(), want2) < TOL[np.dtype(dtype)]
