@@ -478,7 +478,7 @@ static cudaError_t tune_stencil_args(const OpDesc& d, int ldtype, int mode, cons
   TmaChoice best{d.R == 4 ? 1 : 2, 0};
   float best_ms = 1e30f;
   for (int var = 0; var < TMA_NVARIANT; ++var) {
-    for (int nc : {0, -2}) {
+    for (int nc : {0, -2, TMA_SPLIT}) {
       const TmaChoice ch{var, nc};
       cudaError_t e = tma_launch(ldtype, mode, d.R, ch, a, nbatch, d.sc, st);
       if (e != cudaSuccess) {

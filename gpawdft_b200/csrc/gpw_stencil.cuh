@@ -57,6 +57,10 @@ enum StencilMode {
 
 // Number of tile-shape variants of the TMA star kernel (gpw_star_tma.cuh).
 constexpr int TMA_NVARIANT = 11;  // 5 - 9: float32 only
+// Axis-0 chunk count meaning "balanced split over the resident CTA slots"
+// (the other counts: > 0 explicit, 0 the wave model, < 0 the model's count
+// times its magnitude).
+constexpr int TMA_SPLIT = -1;
 
 constexpr int PMAX = 80;  // GUC n<=6 with 6 directions needs 73
 
@@ -80,6 +84,12 @@ struct StencilArgs {
                     // layout and the element's scalar type: out = A in + pot in
   const void* aux;  // APPLY: optional grids in the output's layout and type:
   double aux_scale; //   out += aux_scale aux
+  // TMA star kernel, balanced split (split_npl > 0): a 1D grid whose CTA i
+  // takes units [i T / G, (i + 1) T / G) of T = split_gx split_gy split_nb
+  // split_npl units, a unit being one plane (RESID_RESTRICT: one coarse
+  // plane) of one tile column (split_gx x split_gy tiles per batch member,
+  // split_nb members); a CTA's range may span several columns
+  int split_gx, split_gy, split_nb, split_npl;
 };
 
 struct GeneralCoefs {

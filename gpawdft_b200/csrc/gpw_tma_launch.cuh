@@ -83,7 +83,9 @@ struct TmaKernel {
     });
     return n;
   }
-  // nchunk == 0: from the wave model; nchunk < 0: the model's count times -nchunk
+  // nchunk == 0: from the wave model; nchunk == TMA_SPLIT: the balanced
+  // split over one CTA per resident slot (the model where a norm is
+  // summed); other nchunk < 0: the model's count times -nchunk
   static cudaError_t run(const StencilArgs& a0, int nbatch, const StarCoefs& sc, int nchunk, cudaStream_t st) {
     const int spm = slots_per_sm();
     if (spm <= 0) return cudaErrorInvalidConfiguration;
@@ -103,6 +105,28 @@ struct TmaKernel {
       grid = dim3((a.vco.n[2] + C::CX - 1) / C::CX, (a.vco.n[1] + C::CY - 1) / C::CY, 1);
     }
     const int64_t tiles = (int64_t)grid.x * grid.y * nbatch;
+    // per-CTA norm partials need whole chunks: the split falls back to the model
+    if (nchunk == TMA_SPLIT && a.gsum.partial) nchunk = 0;
+    if (nchunk == TMA_SPLIT) {
+      // units: planes of a tile column (RESID_RESTRICT: coarse planes); CTAs:
+      // the resident slots, but no fewer than 2R + 2 planes of work each
+      const int npl = C::RR ? a.vco.n[0] : v.n[0];
+      const int64_t units = tiles * npl;
+      const int64_t minu = C::RR ? 2 : 2 * R + 2;
+      const int64_t nblk = std::max<int64_t>(1, std::min<int64_t>((int64_t)spm * num_sms(), units / minu));
+      a.split_gx = (int)grid.x;
+      a.split_gy = (int)grid.y;
+      a.split_nb = nbatch;
+      a.split_npl = npl;
+      a.nchunk = 1;
+      a.zchunk = v.n[0];
+      a.nblk_seg = 0;
+      TmaArgs ta{a, device_status_word()};
+      const TmaCoefs<S> kc = tma_coefs<S>(sc, R, a.w, a.c0, a.w2);
+      return launch_pdl(star_tma_kernel<S, R, MODE, VAR>, dim3((unsigned)nblk, 1, 1), dim3(C::NTX, C::NTY), C::smem,
+                        st, map_in, map_rho, map_aux, ta, kc);
+    }
+    a.split_npl = 0;
     int nc = nchunk > 0 ? nchunk
                         : tma_model_chunks(v.n[0], tiles, R, (int64_t)spm * num_sms()) * std::max(1, -nchunk);
     nc = std::max(1, std::min(nc, tma_max_chunks(v.n[0], R)));

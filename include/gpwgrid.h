@@ -422,8 +422,10 @@ int gpw_set_pdl(int on);
 /* Pins the tile variant of the TMA star-stencil kernels (no counterpart in
  * the reference): with variant >= 0 every later TMA stencil launch whose
  * element type and radius have that variant uses it, with `nchunk` axis-0
- * chunks (0 = the wave model, < 0 = the model's count times -nchunk);
- * variant -1 returns to the autotuned choice.  Variants 0-4 and 10 (48-wide
+ * chunks (0 = the wave model, -1 = a balanced split of the tile columns'
+ * planes over one CTA per resident slot -- the wave model for launches
+ * that sum a norm --, < -1 = the model's count times -nchunk); variant -1
+ * returns to the autotuned choice.  Variants 0-4 and 10 (48-wide
  * tiles) exist for both element types, 5-9 (4 points per thread) for float32
  * only.  Process-wide; meant for tests and tuning studies.  GPW_EINVAL
  * outside [-1, 10].                                                        */

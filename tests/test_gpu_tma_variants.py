@@ -19,7 +19,9 @@ from gpawdft_b200.workloads import gaussian_density
 pytestmark = pytest.mark.gpu
 
 NVARIANT = 11           # 0-4 and 10 both element types, 5-9 float32 only
-CHUNKS = [0, 1, -2]     # wave model, one chunk, twice the model's count
+# wave model, one chunk, twice the model's count, balanced split over the
+# resident slots (CTAs whose work spans several tile columns)
+CHUNKS = [0, 1, -2, -1]
 
 
 @pytest.fixture
@@ -79,8 +81,9 @@ def test_variant_apply_relax_residual(cuda, pin, var, dtype, nn):
 def test_variant_poisson_equals_tuned(cuda, pin, N, precision):
     """Batched Poisson solves on the engine's pitched grids (31^3 / 47^3
     rows: the last thread of a row holds 1-3 of its 4 points) with each
-    variant pinned: the same iteration counts and bit-identical potentials
-    as the autotuned solve."""
+    variant pinned, chunked by the wave model and split over the resident
+    slots: the same iteration counts and bit-identical potentials as the
+    autotuned solve."""
     from gpawdft_b200.grid_descriptor import GridDescriptor
     from gpawdft_b200.poisson import PoissonSolver
     rhos = []
@@ -101,7 +104,8 @@ def test_variant_poisson_equals_tuned(cuda, pin, N, precision):
 
     want, want_n = solve()
     for var in range(NVARIANT):
-        pin(var, 0)
-        phi, n = solve()
-        assert np.array_equal(n, want_n), var
-        assert np.array_equal(phi, want), var
+        for nc in (0, -1):
+            pin(var, nc)
+            phi, n = solve()
+            assert np.array_equal(n, want_n), (var, nc)
+            assert np.array_equal(phi, want), (var, nc)
