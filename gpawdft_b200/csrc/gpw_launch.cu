@@ -2,6 +2,7 @@
 // shared-memory opt-in for every device kernel of the library.
 #include <algorithm>
 #include <cstdio>
+#include <initializer_list>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -69,30 +70,71 @@ static cudaError_t run_star(const StencilArgs& a0, const OpDesc& d, int nbatch, 
   return cudaGetLastError();
 }
 
+// Tile of a general-offset launch for element size es and radius mp: the
+// register-blocked kernel's where its ring of planes fits in shared memory
+// (next to its static tables), else the plain kernel's.
+static void general_tile(int mp, size_t es, int& tz, int& ty, bool& blocked) {
+  const int btz = es >= 16 ? 32 : 64, bty = 16;  // GenBlk's TZ x TY
+  blocked = mp >= 1 && mp <= GEN_BLK_MAXMP && general_block_smem(mp, es, btz, bty, PMAX) <= 220 * 1024;
+  tz = blocked ? btz : GEN_TZ;
+  ty = blocked ? bty : GEN_TY;
+}
+
+// Opt kernel `kern` in to `smem` bytes of dynamic shared memory (the
+// largest so far; the static part counts against the same per-CTA limit).
+template <typename K>
+static cudaError_t general_optin(K kern, size_t smem, std::mutex& mu, size_t& opted) {
+  std::lock_guard<std::mutex> lock(mu);
+  if (smem > opted) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    opted = smem;
+  }
+  return cudaSuccess;
+}
+
 template <typename T, int MODE>
 static cudaError_t run_general(const StencilArgs& a0, const OpDesc& d, int nbatch, cudaStream_t st) {
   StencilArgs a = a0;
   const GridView& v = a.vout;
   const int mp = d.mp;
-  dim3 grid((v.n[2] + GEN_TZ - 1) / GEN_TZ, (v.n[1] + GEN_TY - 1) / GEN_TY, 1);
+  int tz, ty;
+  bool blocked;
+  general_tile(mp, sizeof(T), tz, ty, blocked);
+  if (blocked && (tz != GenBlk<T, 1>::TZ || ty != GenBlk<T, 1>::TY)) return cudaErrorInvalidConfiguration;
+  dim3 grid((v.n[2] + tz - 1) / tz, (v.n[1] + ty - 1) / ty, 1);
   choose_chunks(v.n[0], (int64_t)grid.x * grid.y * nbatch, 2 * mp + 2, a.zchunk, a.nchunk);
   grid.z = a.nchunk * nbatch;
   a.nblk_seg = grid.x * grid.y * a.nchunk;
-  const size_t smem = (size_t)(2 * mp + 2) * (GEN_TY + 2 * mp) * (GEN_TZ + 2 * mp) * sizeof(T);
+  // planes loaded ahead: as many (up to 4) as keep two CTAs per SM
+  int depth = 1;
+  while (blocked && depth < 4 && general_block_smem(mp, sizeof(T), tz, ty, d.gc.ncoef, depth + 1) <= 110 * 1024)
+    ++depth;
+  a.gdepth = depth;
+  const size_t smem = blocked ? general_block_smem(mp, sizeof(T), tz, ty, d.gc.ncoef, depth)
+                              : (size_t)(2 * mp + 2) * (ty + 2 * mp) * (tz + 2 * mp) * sizeof(T);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  if (blocked) {
+    auto go = [&](auto kern, std::mutex& mu, size_t& opted) -> cudaError_t {
+      cudaError_t e = general_optin(kern, smem, mu, opted);
+      if (e != cudaSuccess) return e;
+      kern<<<grid, dim3(32, GenBlk<T, 1>::NTY), smem, st>>>(a, d.gc);
+      return cudaGetLastError();
+    };
+    static std::mutex mu[GEN_BLK_MAXMP];
+    static size_t opted[GEN_BLK_MAXMP] = {48 * 1024, 48 * 1024, 48 * 1024};
+    switch (mp) {
+      case 1: return go(general_block_kernel<T, MODE, 1>, mu[0], opted[0]);
+      case 2: return go(general_block_kernel<T, MODE, 2>, mu[1], opted[1]);
+      case 3: return go(general_block_kernel<T, MODE, 3>, mu[2], opted[2]);
+    }
+    return cudaErrorInvalidValue;
+  }
   auto kern = general_stencil_kernel<T, MODE>;
-  // opt in to exactly the dynamic shared memory needed (the largest so far):
-  // the static part of the kernel counts against the same per-CTA limit
   static std::mutex mu;
   static size_t opted = 48 * 1024;
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (smem > opted) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      opted = smem;
-    }
-  }
+  cudaError_t e = general_optin(kern, smem, mu, opted);
+  if (e != cudaSuccess) return e;
   kern<<<grid, dim3(GEN_TZ, GEN_TY), smem, st>>>(a, d.gc);
   return cudaGetLastError();
 }
@@ -136,20 +178,25 @@ cudaError_t launch_apply_cpasync(const OpDesc& d, int dtype, const StencilArgs& 
 
 int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& v, int nbatch) {
   const bool use_star = ((mode == MODE_JACOBI) ? d.star_jacobi : d.star) && star_radius_ok(d.R);
-  int tz, ty, minz;
+  auto blocks = [&](int tz, int ty, int minz) {
+    const int gx = (v.n[2] + tz - 1) / tz, gy = (v.n[1] + ty - 1) / ty;
+    int zc, nc;
+    choose_chunks(v.n[0], (int64_t)gx * gy * nbatch, minz, zc, nc);
+    return gx * gy * nc;
+  };
+  int nblk;
   if (use_star) {
-    tz = 32;
-    ty = GPW_STAR_TY;
-    minz = 2 * d.R + 2;
+    nblk = blocks(32, GPW_STAR_TY, 2 * d.R + 2);
   } else {
-    tz = GEN_TZ;
-    ty = GEN_TY;
-    minz = 2 * d.mp + 2;
+    // the tile depends on the element size: the most CTAs over the op's types
+    nblk = 0;
+    for (size_t es : d.real ? std::initializer_list<size_t>{4, 8} : std::initializer_list<size_t>{8, 16}) {
+      int tz, ty;
+      bool blocked;
+      general_tile(d.mp, es, tz, ty, blocked);
+      nblk = std::max(nblk, blocks(tz, ty, 2 * d.mp + 2));
+    }
   }
-  const int gx = (v.n[2] + tz - 1) / tz, gy = (v.n[1] + ty - 1) / ty;
-  int zc, nc;
-  choose_chunks(v.n[0], (int64_t)gx * gy * nbatch, minz, zc, nc);
-  int nblk = gx * gy * nc;
   if (use_star) {  // a TMA tile variant may be chosen instead: bound its CTA count
     // (tiles at least 48 points wide and 8 rows high, at most n0 / (2R + 2)
     // axis-0 chunks)
@@ -403,7 +450,7 @@ static cudaError_t tune_stencil_args(const OpDesc& d, int ldtype, int mode, cons
 
 bool resid_restrict_ok(const OpDesc& d, const void* in, const void* rho, const GridView& v, const void* out,
                        const void* out2, const GridView& vco, int nbatch) {
-  if (!dc_fusable(d) || d.R != 3 || !tensor_map_encoder()) return false;
+  if (!dc_fusable(d) || (d.R != 1 && d.R != 3) || !tensor_map_encoder()) return false;
   if (!aligned16(in) || !aligned16(rho) || !aligned16(out) || !aligned16(out2)) return false;
   if (!view_tma_ok(v, 4, nbatch)) return false;
   for (int c = 0; c < 3; ++c)

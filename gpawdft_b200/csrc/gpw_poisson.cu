@@ -162,6 +162,7 @@ struct gpw_poisson {
   size_t ctsmem = 0;
   bool use_cluster = true;
   bool use_rr = true;  // float32 form: level-0 residual restricted in the same launch
+  bool use_rr_coarse = true;  // ... and the coarser levels' residuals
   Workspace d_err, d_eps, d_niter, d_active, d_any, d_r64, d_gs_old, d_maxiter, d_tdone, d_t0;
   SumScratch sums;
   int* h_any = nullptr;  // pinned
@@ -237,6 +238,23 @@ struct Rec {
   }
 };
 
+// The float32 residual of level l >= 1 restricted in the same launch
+// (MODE_RESID_RESTRICT) into rho_{l+1} and its first weighted-Jacobi sweep:
+// K = 2 zero-boundary restriction, Jacobi relaxation, and a level l+1 that
+// the cluster kernel or the recursive V-cycle takes from there (the one-CTA
+// coarse kernel starts from rho alone).
+bool level_rr_ok(const gpw_poisson* ps, int l, const void* in, int nb) {
+  const int nl = (int)ps->lv.size();
+  if (!ps->use_rr_coarse || ps->relax_method != 2 || l < 1 || l + 1 >= nl || l + 1 == ps->lc[1]) return false;
+  const Level& L = ps->lv[l];
+  const Level& C = ps->lv[l + 1];
+  const std::vector<double>& first = (l + 2 == nl) ? C.wpost[1] : C.wpre[1];
+  if (first.empty() || C.op->coefs.empty() || L.restr->k != 2) return false;
+  for (int c = 0; c < 3; ++c)
+    if (L.restr->pad[c][0] != 0) return false;
+  return resid_restrict_ok(*L.op, in, L.rho32.ptr, L.v, C.rho32.ptr, C.phi32[0].ptr, C.v, nb);
+}
+
 // Relax `n` sweeps on level l (dtype f64 or f32); returns the index of the
 // phi buffer holding the result.
 int rec_relax(Rec& r, int l, int cur, const double* ws, int nsweeps, bool f32) {
@@ -267,8 +285,10 @@ int rec_relax(Rec& r, int l, int cur, const double* ws, int nsweeps, bool f32) {
 // else the recursive V-cycle from phi_{l+1} = 0, whose first weighted-Jacobi
 // sweep ((w / c0) rho_{l+1}, exactly) the restriction writes alongside.
 // Returns the buffer holding phi_{l+1}.
+// restricted: rho_{l+1} and its first sweep were written by the fused
+// residual-restriction launch (float32, not into the one-CTA kernel).
 int rec_vcycle(Rec& r, int l, int cur, bool f32, bool first_done = false);
-int rec_lower(Rec& r, int l, const void* res, bool f32) {
+int rec_lower(Rec& r, int l, const void* res, bool f32, bool restricted = false) {
   gpw_poisson* ps = r.ps;
   const int nl = (int)ps->lv.size();
   const int p = f32 ? 1 : 0;
@@ -296,9 +316,9 @@ int rec_lower(Rec& r, int l, const void* res, bool f32) {
   }
   const bool coarsest = (l + 2 == nl);
   const std::vector<double>& first = coarsest ? C.wpost[p] : C.wpre[p];
-  const bool fuse = ps->relax_method == 2 && !first.empty() && restrict_sweep_ok(*L.restr, dt) &&
-                    !C.op->coefs.empty();
-  if (!r.tune) {
+  const bool fuse = restricted || (ps->relax_method == 2 && !first.empty() && restrict_sweep_ok(*L.restr, dt) &&
+                                   !C.op->coefs.empty());
+  if (!r.tune && !restricted) {
     if (fuse) {
       const RestrictSweep sw{cphi[0].ptr, first[0], C.op->coefs[0]};
       r.ok(launch_transfer(*L.restr, dt, res, L.v, crho.ptr, C.v, r.nb, bc, 0, nullptr, nullptr, r.active, r.st,
@@ -357,9 +377,19 @@ int rec_vcycle(Rec& r, int l, int cur, bool f32, bool first_done) {
     const int skip = first_done ? 1 : 0;
     cur = rec_relax(r, l, cur, L.wpre[p].data() + skip, (int)L.wpre[p].size() - skip, f32);
     // the residual's norm is not needed below level 0's convergence test
-    r.stencil(*L.op, dt, MODE_RESIDUAL, phi[cur].ptr, res.ptr, rho.ptr, L.v, 1.0, GridSum{});
-    r.tick("L" + std::to_string(l) + (f32 ? " f32" : " f64") + " residual");
-    const int ccur = rec_lower(r, l, res.ptr, f32);
+    int ccur;
+    if (f32 && level_rr_ok(ps, l, phi[cur].ptr, r.nb)) {
+      // float32: the residual restricted straight into rho_{l+1} and its first sweep
+      const std::vector<double>& first = (l + 2 == nl) ? C.wpost[1] : C.wpre[1];
+      r.ok(launch_resid_restrict(*L.op, phi[cur].ptr, rho.ptr, L.v, C.rho32.ptr, C.phi32[0].ptr, C.v, r.nb,
+                                 first[0], C.op->coefs[0], r.active, r.tune, r.st));
+      r.tick("L" + std::to_string(l) + " f32 residual + restriction");
+      ccur = rec_lower(r, l, nullptr, f32, true);
+    } else {
+      r.stencil(*L.op, dt, MODE_RESIDUAL, phi[cur].ptr, res.ptr, rho.ptr, L.v, 1.0, GridSum{});
+      r.tick("L" + std::to_string(l) + (f32 ? " f32" : " f64") + " residual");
+      ccur = rec_lower(r, l, res.ptr, f32);
+    }
     Boundary cbc = make_boundary(C.op->periodic, dt, nullptr);
     if (!r.tune) {
       r.ok(launch_transfer(*L.interp, dt, cphi[ccur].ptr, C.v, phi[1 - cur].ptr, L.v, r.nb, cbc, 1, phi[cur].ptr,
@@ -1302,7 +1332,9 @@ extern "C" int gpw_poisson_set_inner_schedule(gpw_poisson* ps, const int* npre, 
 // compute the same values.  Captured float32 graphs are discarded.
 extern "C" int gpw_poisson_set_fusion(gpw_poisson* ps, int on) {
   if (!ps) return fail(GPW_EINVAL, "null argument");
+  if (on < 0 || on > 2) return fail(GPW_EINVAL, "set_fusion: on must be 0, 1 or 2");
   ps->use_rr = on != 0;
+  ps->use_rr_coarse = on == 1;
   discard_f32_graphs(ps);
   return GPW_OK;
 }

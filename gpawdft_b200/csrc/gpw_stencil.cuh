@@ -90,6 +90,7 @@ struct StencilArgs {
   // plane) of one tile column (split_gx x split_gy tiles per batch member,
   // split_nb members); a CTA's range may span several columns
   int split_gx, split_gy, split_nb, split_npl;
+  int gdepth;       // general_block_kernel: planes loaded ahead of the one completed (1 - 4)
 };
 
 struct GeneralCoefs {
@@ -224,6 +225,260 @@ __global__ void __launch_bounds__(GEN_TZ* GEN_TY)
             } else {
               const S w = (S)a.w, c0 = (S)a.c0;
               static_cast<T*>(a.out)[oi] = (S(1) - w) * cur + (w * (rho - acc)) / c0;
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if constexpr (MODE == MODE_RESIDUAL) {
+    if (!a.gsum.partial) return;  // residual without its norm
+    double tot = block_sum(sumsq, red);
+    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
+    grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);
+  }
+}
+
+// ------------------------------------------------------------------ general, register-blocked
+// The same stencil, outputs and arithmetic as general_stencil_kernel, laid
+// out for throughput: a CTA owns a TY x TZ tile (16 x 64 points with 128
+// threads; 16 x 32 with 256 threads for 16-byte elements) and each thread
+// PY x VX outputs (4 x 2; 2 x 1) in rows NTY apart and columns 32 apart, so
+// a warp's shared-memory reads for one coefficient are consecutive.  Per coefficient the ring slot and in-plane
+// offset come from shared-memory tables, so each output costs one
+// shared-memory load and the reference's unfused multiply-add, in the
+// reference's coefficient order (float64 results bit-identical to
+// c/bmgs/fd.c).  Planes are staged row by row with cp.async, up to four
+// planes ahead of the one completed: the wrapped axis-2 source index of a
+// lane's columns is computed once per CTA, the axis-1 one once per row.
+// What bounds it is that one shared-memory load per output and coefficient:
+// at 19 - 37 coefficients the L1 / shared-memory pipe runs at ~70% (ncu).
+// Taken where a ring of 2mp + 2 planes fits in shared memory, for radii
+// mp <= 3 (compiled per radius, so the staged plane's shape and every
+// in-plane offset of a thread's outputs are constants).
+// (4 rows a thread for 4- and 8-byte elements, 128 threads: measured ~8%
+// faster than 2 rows and 256 threads at 16 x 127^3 float64)
+template <typename T, int MP, int PY_ = (sizeof(T) >= 16 ? 2 : 4), int NTY_ = (sizeof(T) >= 16 ? 8 : 4)>
+struct GenBlk {
+  static constexpr int VX = sizeof(T) >= 16 ? 1 : 2;  // outputs per thread along axis 2
+  static constexpr int PY = PY_, NTY = NTY_;          // along axis 1, and thread rows
+  static constexpr int TZ = 32 * VX, TY = NTY * PY, NT = 32 * NTY;
+  static constexpr int H = TY + 2 * MP, W = TZ + 2 * MP, PS = H * W;  // staged plane
+  static constexpr int NCOL = (W + 31) / 32;          // staged columns per lane
+  static constexpr int NROW = (H + NTY - 1) / NTY;    // staged rows per thread row
+};
+constexpr int GEN_BLK_MAXMP = 3;  // radii with a register-blocked instance
+
+// One coefficient as the inner loop reads it (one shared-memory load): its
+// value and the byte offset of its neighbour from the output cell, for one
+// ring position of the output plane.
+template <typename S>
+struct alignas(2 * sizeof(S)) GenTab {
+  S coef;
+  int off;
+};
+
+// Dynamic shared memory of general_block_kernel with `depth` planes loaded
+// ahead: the ring of 2mp + 1 + depth planes, then a table of ncoef entries
+// per ring position of the output plane.
+inline size_t general_block_smem(int mp, size_t es, int tz, int ty, int ncoef, int depth = 1) {
+  const int np = 2 * mp + 1 + depth;
+  const size_t ring = (size_t)np * (ty + 2 * mp) * (tz + 2 * mp) * es;
+  const size_t tab = (size_t)np * ncoef * (es >= 8 ? 16 : 8);
+  return (ring + 15) / 16 * 16 + tab;
+}
+
+template <typename T, int MODE, int MP, int PY_ = GenBlk<T, MP>::PY, int NTY_ = GenBlk<T, MP>::NTY>
+__global__ void __launch_bounds__(GenBlk<T, MP, PY_, NTY_>::NT, 2)
+    general_block_kernel(const StencilArgs a, const GeneralCoefs k) {
+  using G = GenBlk<T, MP, PY_, NTY_>;
+  using S = typename EltTraits<T>::S;
+  constexpr int VX = G::VX, PY = G::PY, NTY = G::NTY, W = G::W, H = G::H, PS = G::PS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = reinterpret_cast<T*>(smem_raw);
+  __shared__ double red[32];
+
+  const int ncoef = k.ncoef, D = a.gdepth, NP = 2 * MP + 1 + D;
+  GenTab<S>* tab = reinterpret_cast<GenTab<S>*>(smem_raw + ((size_t)NP * PS * sizeof(T) + 15) / 16 * 16);
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int x0 = blockIdx.x * G::TZ, y0 = blockIdx.y * G::TY;
+  const int n0 = a.vout.n[0];
+  const int z0 = chunk * a.zchunk;
+  const int z1 = min(n0, z0 + a.zchunk);
+  const T* in = static_cast<const T*>(a.in) + (int64_t)b * a.vin.sb;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
+  const Boundary& bc = a.bc;
+  // tab[cs * ncoef + c]: coefficient c with plane o in ring slot cs
+  for (int e = tid; e < NP * ncoef; e += G::NT) {
+    const int cs = e / ncoef, c = e - cs * ncoef;
+    int sl = cs + k.off[c][0];
+    sl = sl < 0 ? sl + NP : (sl >= NP ? sl - NP : sl);
+    tab[e].coef = (S)k.coef[c];
+    tab[e].off = ((sl - cs) * PS + k.off[c][1] * W + k.off[c][2]) * (int)sizeof(T);
+  }
+  // this thread's staged cells (rows ty + NTY q, columns tx + 32 m): source
+  // offsets within a plane and periodic-image sides, computed once
+  int64_t roff[G::NROW];
+  int jx[G::NCOL];
+  unsigned rowok = 0, colok = 0, fixmask = 0;  // fixmask bit q * NCOL + m: an in-plane periodic image
+  signed char sy[G::NROW], sx[G::NCOL];
+#pragma unroll
+  for (int m = 0; m < G::NCOL; ++m) {
+    const int c = tx + 32 * m;
+    int s = -1;
+    if (c < W && wrap_axis(x0 - MP + c, a.vin.n[2], bc.periodic[2], jx[m], s)) colok |= 1u << m;
+    sx[m] = (signed char)s;
+  }
+#pragma unroll
+  for (int q = 0; q < G::NROW; ++q) {
+    const int r = ty + NTY * q;
+    int j1 = 0, s = -1;
+    if (r < H && wrap_axis(y0 - MP + r, a.vin.n[1], bc.periodic[1], j1, s)) rowok |= 1u << q;
+    roff[q] = (int64_t)j1 * a.vin.s1;
+    sy[q] = (signed char)s;
+#pragma unroll
+    for (int m = 0; m < G::NCOL; ++m)
+      if (((rowok >> q) & (colok >> m) & 1u) && (s >= 0 || sx[m] >= 0)) fixmask |= 1u << (q * G::NCOL + m);
+  }
+  double sumsq = 0.0;
+  __syncthreads();
+
+  if (z0 < z1) {
+    // plane p into its ring slot
+    auto load = [&](int p) {
+      int j0, s0;
+      const bool ok0 = wrap_axis(p, a.vin.n[0], bc.periodic[0], j0, s0);
+      T* slot = ring + ((p - z0 + MP) % NP) * PS;
+      const T* base = in + (int64_t)j0 * a.vin.s0;
+#pragma unroll
+      for (int q = 0; q < G::NROW; ++q) {
+        const int r = ty + NTY * q;
+#pragma unroll
+        for (int m = 0; m < G::NCOL; ++m) {
+          const int c = tx + 32 * m;
+          if (r < H && c < W) {
+            const bool ok = ok0 && ((rowok >> q) & (colok >> m) & 1u);
+            cp_async<sizeof(T)>(slot + r * W + c, ok ? base + roff[q] + jx[m] : in, ok);
+          }
+        }
+      }
+    };
+    // Bloch phases of this thread's periodic-image cells of plane p, axis by
+    // axis as the reference's chained halo copies apply them
+    auto fix = [&](int p) {
+      if constexpr (EltTraits<T>::cpx) {
+        int j0, s0;
+        if (!wrap_axis(p, a.vin.n[0], bc.periodic[0], j0, s0)) return;
+        if (s0 < 0 && !fixmask) return;
+        T* slot = ring + ((p - z0 + MP) % NP) * PS;
+#pragma unroll
+        for (int q = 0; q < G::NROW; ++q) {
+#pragma unroll
+          for (int m = 0; m < G::NCOL; ++m) {
+            const int r = ty + NTY * q, c = tx + 32 * m;
+            if (!((rowok >> q) & (colok >> m) & 1u)) continue;
+            if (s0 < 0 && !((fixmask >> (q * G::NCOL + m)) & 1u)) continue;
+            T val = slot[r * W + c];
+            if (s0 >= 0) val = phase_mul(bc.ph[0][s0], val);
+            if (sy[q] >= 0) val = phase_mul(bc.ph[1][sy[q]], val);
+            if (sx[m] >= 0) val = phase_mul(bc.ph[2][sx[m]], val);
+            slot[r * W + c] = val;
+          }
+        }
+      }
+    };
+    // one commit group for the first 2mp + 1 planes, then one per plane: at
+    // output plane o the groups of planes o + mp + 1 .. o + mp + D may still
+    // be in flight
+    for (int p = z0 - MP; p <= z0 + MP; ++p) load(p);
+    cp_async_commit();
+    for (int d = 1; d < D; ++d) {
+      if (z0 + d < z1) load(z0 + MP + d);
+      cp_async_commit();
+    }
+    // this thread's first output cell within slot 0
+    const unsigned char* cen = reinterpret_cast<const unsigned char*>(ring + (ty + MP) * W + tx + MP);
+    // its outputs (rows NTY apart, columns 32 apart): inside the grid, and
+    // their element offsets less the plane's (the potential's drops the batch's)
+    const int64_t ob = (int64_t)b * a.vout.sb;
+    int64_t obase[PY][VX], rbase[PY][VX];
+    unsigned omask = 0;
+#pragma unroll
+    for (int i = 0; i < PY; ++i)
+#pragma unroll
+      for (int j = 0; j < VX; ++j) {
+        const int y = y0 + ty + NTY * i, x = x0 + tx + 32 * j;
+        if (y < a.vout.n[1] && x < a.vout.n[2]) omask |= 1u << (i * VX + j);
+        obase[i][j] = ob + (int64_t)y * a.vout.s1 + x;
+        rbase[i][j] = (int64_t)b * a.vrho.sb + (int64_t)y * a.vrho.s1 + x;
+      }
+    for (int o = z0; o < z1; ++o) {
+      if (o + D < z1) load(o + MP + D);
+      cp_async_commit();
+      switch (D) {
+        case 1: cp_async_wait<1>(); break;
+        case 2: cp_async_wait<2>(); break;
+        case 3: cp_async_wait<3>(); break;
+        default: cp_async_wait<4>(); break;
+      }
+      if (bc.use_phase) {
+        if (o == z0) {
+          for (int p = z0 - MP; p <= z0 + MP; ++p) fix(p);
+        } else {
+          fix(o + MP);
+        }
+      }
+      __syncthreads();
+      const int cs = (o - z0 + MP) % NP;  // slot of plane o
+      const GenTab<S>* tc = tab + cs * ncoef;
+      const unsigned char* co = cen + cs * PS * (int)sizeof(T);
+      T acc[PY][VX];
+#pragma unroll
+      for (int i = 0; i < PY; ++i)
+#pragma unroll
+        for (int j = 0; j < VX; ++j) acc[i][j] = zero<T>();
+#pragma unroll 4
+      for (int c = (MODE == MODE_JACOBI) ? 1 : 0; c < ncoef; ++c) {
+        const GenTab<S> e = tc[c];
+        const T* src = reinterpret_cast<const T*>(co + e.off);
+#pragma unroll
+        for (int i = 0; i < PY; ++i)
+#pragma unroll
+          for (int j = 0; j < VX; ++j) acc[i][j] = mac_rn(e.coef, src[i * NTY * W + 32 * j], acc[i][j]);
+      }
+      const T* cp = reinterpret_cast<const T*>(co);  // plane o's centre cells
+      const int64_t oz = (int64_t)o * a.vout.s0, rz = (int64_t)o * a.vrho.s0;
+#pragma unroll
+      for (int i = 0; i < PY; ++i) {
+#pragma unroll
+        for (int j = 0; j < VX; ++j) {
+          if (!((omask >> (i * VX + j)) & 1u)) continue;
+          T r = acc[i][j];
+          const T cur = cp[i * NTY * W + 32 * j];
+          const int64_t oi = obase[i][j] + oz;
+          if constexpr (MODE == MODE_APPLY) {
+            if (a.pot) {
+              const S pv = static_cast<const S*>(a.pot)[oi - ob];
+              r = fmac(pv, cur, r);
+            }
+            if (a.aux) r = fmac((S)a.aux_scale, static_cast<const T*>(a.aux)[oi], r);
+            static_cast<T*>(a.out)[oi] = r;
+          } else {
+            const T rho = static_cast<const T*>(a.rho)[rbase[i][j] + rz];
+            if constexpr (MODE == MODE_RESIDUAL) {
+              const T d = sub(r, rho);
+              if (a.out) static_cast<T*>(a.out)[oi] = d;
+              sumsq += norm2(d);
+            } else {
+              // (1 - w) * b + w * (src - x) / c0   (c/bmgs/relax.c:62)
+              if constexpr (EltTraits<T>::cpx) {
+                static_cast<T*>(a.out)[oi] = cur;  // relax is real-only (asserted on host)
+              } else {
+                const S w = (S)a.w, c0 = (S)a.c0;
+                static_cast<T*>(a.out)[oi] = (S(1) - w) * cur + (w * (rho - r)) / c0;
+              }
             }
           }
         }

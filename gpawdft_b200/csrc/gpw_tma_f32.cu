@@ -14,8 +14,9 @@ cudaError_t tma_stencil_f32(int mode, int R, int var, const StencilArgs& a, int 
     case MODE_JACOBI_ADD64: return tma_run_radius<float, MODE_JACOBI_ADD64>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_JACOBI_SCALED_IN:
       return tma_run_radius<float, MODE_JACOBI_SCALED_IN>(R, var, a, nbatch, sc, nchunk, st);
-    case MODE_RESID_RESTRICT:  // the float32 form's level 0 (nn = 3) only
+    case MODE_RESID_RESTRICT:  // the float32 form's level 0 (nn = 3) and coarse levels (nn = 1)
       if (R == 3) return tma_run_variant<float, 3, MODE_RESID_RESTRICT>(var, a, nbatch, sc, nchunk, st);
+      if (R == 1) return tma_run_variant<float, 1, MODE_RESID_RESTRICT>(var, a, nbatch, sc, nchunk, st);
       return cudaErrorInvalidValue;
   }
   return cudaErrorInvalidValue;

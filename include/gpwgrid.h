@@ -401,14 +401,20 @@ int gpw_poisson_set_device_loop(gpw_poisson *ps, int on);
  * different order (results within float32 rounding of each other).       */
 int gpw_poisson_set_cluster(gpw_poisson *ps, int on);
 
-/* Level-0 launch plan of the float32 form (no counterpart in the
- * reference): on = 1 (default) computes the level-0 residual and restricts
- * it into level 1 (its rho and first Jacobi sweep) in one launch, without
- * storing the residual, and (with two or more level-0 pre-sweeps) lets the
- * second pre-sweep read the float32 defect alone and form the first
- * sweep's iterate itself, so the float64 defect stores no iterate; on = 0
- * launches the residual and the restriction separately and stores the
- * first iterate.  The two plans compute identical values.                 */
+/* Launch plan of the float32 form (no counterpart in the reference):
+ * on = 1 (default) computes the level-0 residual and restricts it into
+ * level 1 (its rho and first Jacobi sweep) in one launch, without storing
+ * the residual, lets (with two or more level-0 pre-sweeps) the second
+ * pre-sweep read the float32 defect alone and form the first sweep's
+ * iterate itself, so the float64 defect stores no iterate, and fuses the
+ * residual and restriction of the coarser levels the same way where the
+ * next level is a cluster or stencil level (not the one-CTA kernel's);
+ * on = 2 keeps the level-0 plan and launches the coarser levels' residuals
+ * and restrictions separately (identical values); on = 0 launches every
+ * residual and restriction separately and stores the first iterate (the
+ * level-0 inner corrections then differ from on = 1 by float32 rounding:
+ * the fused second pre-sweep scales the stencil of the defect instead of
+ * taking the stencil of the stored iterate).                              */
 int gpw_poisson_set_fusion(gpw_poisson *ps, int on);
 
 /* Programmatic dependent launch of the V-cycle's kernels (no counterpart in

@@ -336,6 +336,43 @@ def test_fused_residual_restriction(cuda, N):
     assert np.abs(out[0][0] - out[1][0]).max() < 1e-9 * np.abs(out[1][0]).max()
 
 
+@pytest.mark.parametrize('cluster', [1, 0])
+@pytest.mark.parametrize('N', [128, 192])
+def test_coarse_residual_restriction(cuda, N, cluster):
+    """The float32 residual of the coarser levels (63^3 at N_c = 128; 95^3
+    and 47^3 at 192, and with the cluster launch off every level above the
+    one-CTA kernel's) restricted into the next level's rho and first sweep in
+    one launch, against the residual, restriction and sweep launched apart:
+    the same operations in the same order, so bit-identical potentials and
+    iteration counts."""
+    from gpawdft_b200 import _lib
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    from gpawdft_b200.poisson import PoissonSolver
+    lib = _lib.load()
+    rhos = np.array([gaussian_density(N, 0.2, 8, 150 + s)[0] for s in range(2)])
+    L = gaussian_density(N, 0.2, 8, 150)[1]
+    gd = GridDescriptor((N,) * 3, (L,) * 3, 0)
+    eps = [1e-20 * float(np.dot(r.ravel(), r.ravel())) * gd.dv for r in rhos]
+    out = []
+    for on in (1, 2):
+        ps = PoissonSolver(nn=3, batch=2, precision='fp32', maxiter=100)
+        ps.set_grid_descriptor(gd)
+        ps.initialize()
+        _lib.check(lib.gpw_poisson_set_fusion(ps._engine[0], on))
+        _lib.check(lib.gpw_poisson_set_cluster(ps._engine[0], cluster))
+        phi = np.zeros_like(rhos)
+        n = ps.solve_batch(phi, rhos, eps=eps)
+        assert (ps.last_errors <= eps).all()
+        labels = [lab for lab, _ in ps.profile_iteration(2, reps=1)]
+        out.append((phi, n, labels))
+    # the fused plan launches no coarse residual of its own
+    assert any(lab.startswith('L1 f32 residual + restriction')
+               for lab in out[0][2]), out[0][2]
+    assert 'L1 f32 residual' in out[1][2]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][0], out[1][0])
+
+
 @pytest.mark.parametrize('N', [64, 128, 192])
 def test_cluster_level_plan(cuda, N):
     """The float32 form with the two levels above the one-CTA coarse levels
