@@ -516,6 +516,25 @@ def run_ours(args, rank, world, dist):
            'single_solve': single,
            'iteration_breakdown': breakdown,
            'stencil_config_a': stencil}
+    if rank == 0 and world == 1 and not args.no_secondary:
+        # the other configurations' key numbers, measured after the timed
+        # region on the same GPU (each also runs alone: --workload bands96 /
+        # general / mixed192; the 512-solve uneven batch is left out, its
+        # densities take most of a minute to generate on the host)
+        import copy
+        sa = copy.copy(args)
+        sa.steps = min(args.steps, 10)
+        del ps, rho_d, phi_d
+        torch.cuda.empty_cache()
+        sec = {}
+        for key, fn in (('bands96', bands_line), ('general', general_line),
+                        ('mixed192', mixed192_line)):
+            w0 = time.time()
+            line = fn(sa)
+            line['wall_s'] = time.time() - w0
+            sec[key] = line
+            torch.cuda.empty_cache()
+        out['secondary'] = sec
     if rank == 0 and world == 1 and not args.no_cpu:
         r = cpu_arm(1, 0)
         out['cpu_baseline'] = {'value': float(np.mean(r['rates'])),
@@ -606,6 +625,10 @@ def _events():
 
 
 def run_mixed192(args):
+    print(json.dumps(mixed192_line(args)), flush=True)
+
+
+def mixed192_line(args):
     """Mixed precision: one 191^3 solve (N_c=192, h=0.15 A, 64 Gaussians with
     log-uniform widths 0.3-2.0 A and N(0,1) charges re-centred to neutral,
     seed 4) to relative residual 1e-10: float32 V-cycles inside float64
@@ -664,10 +687,14 @@ def run_mixed192(args):
                 res['fp32_4levels_jacobi22']['E_H'] - res['fp64']['E_H']),
                 speedup_vs_fp64=res['fp64']['time_s'] /
                 res['fp32_4levels_jacobi22']['time_s'])}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_general(args):
+    print(json.dumps(general_line(args)), flush=True)
+
+
+def general_line(args):
     """General-offset stencils (gpaw/fd_operators.py:158-251): the GUC
     Laplacian of a face-centred-cubic cell (6 directions, nn=3: 37 points)
     on complex128 Bloch bands of a 96^3 periodic grid, and the Mehrstellen
@@ -726,7 +753,7 @@ def run_general(args):
             'config': {'workload': 'GUC nn=3 fcc 64 x 96^3 complex128; '
                                    'Mehrstellen 16 x 127^3 float64'},
             'ops': res}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_uneven(args):
@@ -901,6 +928,10 @@ def run_learned(args):
 
 
 def run_bands(args):
+    print(json.dumps(bands_line(args)), flush=True)
+
+
+def bands_line(args):
     """256 complex Bloch bands on a 96^3 periodic grid (h = 0.18 A, random k,
     phase-wrapped halos): Laplace nn=3 (scale -1/2), the same kinetic
     operator fused with a local potential, Gradient x/y/z n=3,
@@ -987,7 +1018,7 @@ def run_bands(args):
             'dtype': 'c128', 'data': 'synthetic', 'peak_GBps': peak,
             'config': {'workload': '%d complex Bloch bands, 96^3 periodic' % NB},
             'ops': res}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -1010,6 +1041,10 @@ def main():
                          'the device-side loop (for per-kernel profiling)')
     ap.add_argument('--no-cpu', action='store_true',
                     help='skip the cpu_baseline sample')
+    ap.add_argument('--no-secondary', action='store_true',
+                    help='poisson128: skip the secondary configurations '
+                         '(band stencils, general stencils, 191^3 mixed '
+                         'precision) measured after the headline')
     args = ap.parse_args()
     if args.workload != 'poisson128':
         {'mixed192': run_mixed192, 'uneven512': run_uneven,
