@@ -532,17 +532,23 @@ static cudaError_t tune_stencil_args(const OpDesc& d, int ldtype, int mode, cons
         cudaGetLastError();  // a variant this shape cannot launch: skip it
         continue;
       }
-      const int reps = 3;
-      cudaEventRecord(e0, st);
-      for (int i = 0; i < reps && e == cudaSuccess; ++i) e = tma_launch(ldtype, mode, d.R, ch, a, nbatch, d.sc, st);
-      cudaEventRecord(e1, st);
-      if (cudaEventSynchronize(e1) != cudaSuccess || e != cudaSuccess) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        return e != cudaSuccess ? e : cudaGetLastError();
+      // the faster of two rounds of eight launches (one round of three let
+      // run-to-run noise pick tiles up to 1.4x slower than the steady state)
+      const int reps = 8;
+      float ms = 1e30f;
+      for (int round = 0; round < 2; ++round) {
+        cudaEventRecord(e0, st);
+        for (int i = 0; i < reps && e == cudaSuccess; ++i) e = tma_launch(ldtype, mode, d.R, ch, a, nbatch, d.sc, st);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess || e != cudaSuccess) {
+          cudaEventDestroy(e0);
+          cudaEventDestroy(e1);
+          return e != cudaSuccess ? e : cudaGetLastError();
+        }
+        float r = 0.f;
+        cudaEventElapsedTime(&r, e0, e1);
+        ms = std::min(ms, r);
       }
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
       if (ms < best_ms) {
         best_ms = ms;
         best = ch;
