@@ -473,7 +473,13 @@ cudaError_t launch_resid_restrict(const OpDesc& d, const void* in, const void* r
   a.w2 = w2;
   a.c0 = c02;  // the next level's diagonal: the first coarse sweep's w2 / c0
   a.active = active;
-  if (tune) return tune_stencil_args(d, GPW_F32, MODE_RESID_RESTRICT, a, nbatch, st);
+  // the tuning pass runs on the engine's buffers before any solve, when the
+  // mask may mark every member inactive (the timed launches would then do no
+  // work): it times every member, like the other stencils' tuning
+  if (tune) {
+    a.active = nullptr;
+    return tune_stencil_args(d, GPW_F32, MODE_RESID_RESTRICT, a, nbatch, st);
+  }
   const TmaChoice ch = tma_choice(GPW_F32, d.R, MODE_RESID_RESTRICT, v, nbatch);
   return tma_launch(GPW_F32, MODE_RESID_RESTRICT, d.R, ch, a, nbatch, d.sc, st);
 }
