@@ -66,7 +66,7 @@ static cudaError_t run_star(const StencilArgs& a0, const OpDesc& d, int nbatch, 
   cudaError_t e = cudaSuccess;
   std::call_once(once, [&] { e = smem_optin(kern, smem); });
   if (e != cudaSuccess) return e;
-  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, d.sc);  // NT threads
+  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, star_coefs_typed<typename EltTraits<T>::S>(d.sc));  // NT threads
   return cudaGetLastError();
 }
 

@@ -92,7 +92,7 @@ cudaError_t star_residual(StencilArgs a, const OpDesc& d, int nbatch, bool launc
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, d.sc);
+  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, star_coefs_typed<typename EltTraits<T>::S>(d.sc));
   return cudaGetLastError();
 }
 

@@ -522,6 +522,26 @@ struct StarCoefs {
   double cc;                      // total centre (diagonal) coefficient
 };
 
+// The same coefficients in the kernel's scalar type, rounded once on the host
+// (the rounding a per-use conversion makes): a float32 / complex64 kernel
+// then holds no float64 constants to convert inside its plane loop.
+template <typename S>
+struct StarCoefsT {
+  S cx[13], cy[13], cz[13];
+  S cc;
+};
+template <typename S>
+inline StarCoefsT<S> star_coefs_typed(const StarCoefs& sc) {
+  StarCoefsT<S> t{};
+  for (int i = 0; i < 13; ++i) {
+    t.cx[i] = (S)sc.cx[i];
+    t.cy[i] = (S)sc.cy[i];
+    t.cz[i] = (S)sc.cz[i];
+  }
+  t.cc = (S)sc.cc;
+  return t;
+}
+
 // Per-thread plane-load descriptors: the tile position in (axis 1, axis 2) is
 // fixed for the CTA, so each cell's in-plane source offset, validity and
 // wrap sides are computed once; a plane load is then one cp.async per cell.
@@ -587,7 +607,7 @@ struct StarLoader {
 
 template <typename T, int R, int MODE>
 __global__ void __launch_bounds__(StarCfg<R, T>::NT)
-    star_stencil_kernel(const StencilArgs a, const StarCoefs k) {
+    star_stencil_kernel(const StencilArgs a, const StarCoefsT<typename EltTraits<T>::S> k) {
   using C = StarCfg<R, T>;
   using S = typename EltTraits<T>::S;
   constexpr int PY = C::PY, W = C::W, PS = C::PS, NS = C::NSTAGE;
