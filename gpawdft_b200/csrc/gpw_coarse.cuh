@@ -188,6 +188,30 @@ struct PadGeom {
   __device__ __forceinline__ int at(int i0, int i1, int i2) const { return (i0 + 1) * sz + (i1 + 1) * sy + i2 + 1; }
 };
 
+// Walk the points of a padded level: each thread takes whole axis-0 columns
+// (neighbours at fixed strides, no index divisions) when the level has at
+// least as many columns as the CTA has threads; on smaller levels, where that
+// would leave most threads idle and the rest walking long columns, the
+// threads take single points.  body(i0, i1, i2, k), k the padded index.
+template <typename F>
+__device__ __forceinline__ void pg_points(const PadGeom& g, F body) {
+  const int ncol = g.n1 * g.n2;
+  if (ncol >= (int)blockDim.x) {
+    for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+      const int i1 = c / g.n2, i2 = c - i1 * g.n2;
+      int k = g.at(0, i1, i2);
+#pragma unroll 4
+      for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) body(i0, i1, i2, k);
+    }
+  } else {
+    for (int i = threadIdx.x; i < ncol * g.n0; i += blockDim.x) {
+      const int i0 = i / ncol, c = i - i0 * ncol;
+      const int i1 = c / g.n2, i2 = c - i1 * g.n2;
+      body(i0, i1, i2, g.at(i0, i1, i2));
+    }
+  }
+}
+
 template <typename S>
 __device__ __forceinline__ void pg_jacobi(const CoarseLevel& L, const S* __restrict__ src, S* __restrict__ dst,
                                           const S* __restrict__ rho, double wd) {
@@ -195,20 +219,15 @@ __device__ __forceinline__ void pg_jacobi(const CoarseLevel& L, const S* __restr
   const S w = (S)wd, wc = w / (S)L.cc;
   const S c0m = (S)L.cm[0], c0p = (S)L.cp[0], c1m = (S)L.cm[1], c1p = (S)L.cp[1], c2m = (S)L.cm[2],
           c2p = (S)L.cp[2];
-  for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
-    const int i1 = c / g.n2, i2 = c - i1 * g.n2;
-    int k = g.at(0, i1, i2);
-#pragma unroll 4
-    for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) {
-      S av = c2m * src[k - 1];
-      av = fmac(c2p, src[k + 1], av);
-      av = fmac(c1m, src[k - g.sy], av);
-      av = fmac(c1p, src[k + g.sy], av);
-      av = fmac(c0m, src[k - g.sz], av);
-      av = fmac(c0p, src[k + g.sz], av);
-      dst[k] = (S(1) - w) * src[k] + wc * (rho[k] - av);
-    }
-  }
+  pg_points(g, [&](int, int, int, int k) {
+    S av = c2m * src[k - 1];
+    av = fmac(c2p, src[k + 1], av);
+    av = fmac(c1m, src[k - g.sy], av);
+    av = fmac(c1p, src[k + g.sy], av);
+    av = fmac(c0m, src[k - g.sz], av);
+    av = fmac(c0p, src[k + g.sz], av);
+    dst[k] = (S(1) - w) * src[k] + wc * (rho[k] - av);
+  });
   __syncthreads();
 }
 
@@ -218,20 +237,15 @@ __device__ __forceinline__ void pg_residual(const CoarseLevel& L, const S* __res
   const PadGeom g(L);
   const S c0m = (S)L.cm[0], c0p = (S)L.cp[0], c1m = (S)L.cm[1], c1p = (S)L.cp[1], c2m = (S)L.cm[2],
           c2p = (S)L.cp[2], cc = (S)L.cc;
-  for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
-    const int i1 = c / g.n2, i2 = c - i1 * g.n2;
-    int k = g.at(0, i1, i2);
-#pragma unroll 4
-    for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) {
-      S av = c2m * phi[k - 1];
-      av = fmac(c2p, phi[k + 1], av);
-      av = fmac(c1m, phi[k - g.sy], av);
-      av = fmac(c1p, phi[k + g.sy], av);
-      av = fmac(c0m, phi[k - g.sz], av);
-      av = fmac(c0p, phi[k + g.sz], av);
-      r[k] = fmac(cc, phi[k], av) - rho[k];
-    }
-  }
+  pg_points(g, [&](int, int, int, int k) {
+    S av = c2m * phi[k - 1];
+    av = fmac(c2p, phi[k + 1], av);
+    av = fmac(c1m, phi[k - g.sy], av);
+    av = fmac(c1p, phi[k + g.sy], av);
+    av = fmac(c0m, phi[k - g.sz], av);
+    av = fmac(c0p, phi[k + g.sz], av);
+    r[k] = fmac(cc, phi[k], av) - rho[k];
+  });
   __syncthreads();
 }
 
@@ -240,27 +254,22 @@ template <typename S>
 __device__ __forceinline__ void pg_restrict(const CoarseLevel& F, const S* __restrict__ r, const CoarseLevel& C,
                                             S* __restrict__ rho_c, S* __restrict__ phi_c) {
   const PadGeom f(F), g(C);
-  for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
-    const int I1 = c / g.n2, I2 = c - I1 * g.n2;
-    int k = g.at(0, I1, I2);
-    int kf = f.at(1, 2 * I1 + 1, 2 * I2 + 1);  // fine centre of I0 = 0
-#pragma unroll 2
-    for (int I0 = 0; I0 < g.n0; ++I0, k += g.sz, kf += 2 * f.sz) {
-      S y[3];
+  pg_points(g, [&](int I0, int I1, int I2, int k) {
+    const int kf = f.at(2 * I0 + 1, 2 * I1 + 1, 2 * I2 + 1);  // fine centre
+    S y[3];
 #pragma unroll
-      for (int d0 = 0; d0 < 3; ++d0) {
-        S z[3];
+    for (int d0 = 0; d0 < 3; ++d0) {
+      S z[3];
 #pragma unroll
-        for (int d1 = 0; d1 < 3; ++d1) {
-          const int q = kf + (d0 - 1) * f.sz + (d1 - 1) * f.sy;
-          z[d1] = r2(r[q - 1], r[q], r[q + 1]);
-        }
-        y[d0] = r2(z[0], z[1], z[2]);
+      for (int d1 = 0; d1 < 3; ++d1) {
+        const int q = kf + (d0 - 1) * f.sz + (d1 - 1) * f.sy;
+        z[d1] = r2(r[q - 1], r[q], r[q + 1]);
       }
-      rho_c[k] = r2(y[0], y[1], y[2]);
-      phi_c[k] = S(0);
+      y[d0] = r2(z[0], z[1], z[2]);
     }
-  }
+    rho_c[k] = r2(y[0], y[1], y[2]);
+    phi_c[k] = S(0);
+  });
   __syncthreads();
 }
 
@@ -279,22 +288,15 @@ template <typename S>
 __device__ __forceinline__ void pg_interp_sub(const CoarseLevel& F, const S* __restrict__ base, S* __restrict__ dst,
                                               const CoarseLevel& C, const S* __restrict__ e) {
   const PadGeom f(F), g(C);
-  for (int c = threadIdx.x; c < f.n1 * f.n2; c += blockDim.x) {
-    const int o1 = c / f.n2, o2 = c - o1 * f.n2;
+  pg_points(f, [&](int o0, int o1, int o2, int k) {
     // t = o + 1; coarse u = t / 2 - 1 (padded index u + 1 = t / 2), e = t & 1
-    const int t1 = o1 + 1, t2 = o2 + 1;
+    const int t0 = o0 + 1, t1 = o1 + 1, t2 = o2 + 1;
     const int e1 = t1 & 1, e2 = t2 & 1;
-    const int qc = (t1 >> 1) * g.sy + (t2 >> 1);  // padded in-plane coarse index
-    int k = f.at(0, o1, o2);
-#pragma unroll 4
-    for (int o0 = 0; o0 < f.n0; ++o0, k += f.sz) {
-      const int t0 = o0 + 1;
-      const int q = (t0 >> 1) * g.sz + qc;
-      S v = pg_interp_plane(e, g, q, e1, e2);
-      if (t0 & 1) v = i2h(v, pg_interp_plane(e, g, q + g.sz, e1, e2));
-      dst[k] = base[k] - v;
-    }
-  }
+    const int q = (t0 >> 1) * g.sz + (t1 >> 1) * g.sy + (t2 >> 1);  // padded coarse index
+    S v = pg_interp_plane(e, g, q, e1, e2);
+    if (t0 & 1) v = i2h(v, pg_interp_plane(e, g, q + g.sz, e1, e2));
+    dst[k] = base[k] - v;
+  });
   __syncthreads();
 }
 
@@ -315,6 +317,7 @@ __device__ void coarse_vcycle_padded(const CoarseArgs& a, S* sm, int b) {
     for (int c = threadIdx.x; c < g.n1 * g.n2; c += blockDim.x) {
       const int i1 = c / g.n2, i2 = c - i1 * g.n2;
       int k = g.at(0, i1, i2);
+#pragma unroll 4
       for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz) rho[k] = gr[(int64_t)i0 * a.vrho.s0 + (int64_t)i1 * a.vrho.s1 + i2];
     }
     __syncthreads();
@@ -602,6 +605,8 @@ __global__ void __launch_bounds__(CG_CLUSTER_THREADS, 2) cluster_vcycle_kernel(c
     for (int c = threadIdx.x; c < gs.n1 * gs.n2; c += blockDim.x) {
       const int i1 = c / gs.n2, i2 = c - i1 * gs.n2;
       int k = gs.at(0, i1, i2);
+      // (unrolled: the loads of several planes are in flight together)
+#pragma unroll 4
       for (int i0 = 0; i0 < np; ++i0, k += gs.sz) {
         const int64_t gi = (int64_t)(z0 + i0) * t.v.s0 + (int64_t)i1 * t.v.s1 + i2;
         rho[k] = gr[gi];
@@ -643,6 +648,7 @@ __global__ void __launch_bounds__(CG_CLUSTER_THREADS, 2) cluster_vcycle_kernel(c
     for (int q = threadIdx.x; q < g.n1 * g.n2; q += blockDim.x) {
       const int i1 = q / g.n2, i2 = q - i1 * g.n2;
       int k = g.at(0, i1, i2);
+#pragma unroll 4
       for (int i0 = 0; i0 < g.n0; ++i0, k += g.sz)
         e[k] = __ldcg(gp + (int64_t)i0 * a.ca.vphi.s0 + (int64_t)i1 * a.ca.vphi.s1 + i2);
     }
