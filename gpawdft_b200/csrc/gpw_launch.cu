@@ -765,14 +765,20 @@ static cudaError_t dispatch_transfer(const TransferArgs& a, int k, bool interp, 
 // ------------------------------------------------------------------ coarse levels
 // The cluster V-cycle (float32): CG_NCL CTAs per solve in one cluster.
 cudaError_t launch_cluster_vcycle(const ClusterArgs& a, size_t smem, int nbatch, cudaStream_t st) {
-  if (nbatch < 1 || smem > 227 * 1024) return cudaErrorInvalidValue;
+  // dynamic shared memory up to the per-CTA limit less the kernel's static part
   static std::once_flag once;
   static cudaError_t oe = cudaSuccess;
+  static size_t max_dyn = 0;
   std::call_once(once, [] {
+    cudaFuncAttributes fa{};
+    oe = cudaFuncGetAttributes(&fa, cluster_vcycle_kernel<float>);
+    if (oe != cudaSuccess) return;
+    max_dyn = 227 * 1024 - fa.sharedSizeBytes;
     oe = cudaFuncSetAttribute(cluster_vcycle_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              227 * 1024);
+                              (int)max_dyn);
   });
   if (oe != cudaSuccess) return oe;
+  if (nbatch < 1 || smem > max_dyn) return cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nbatch * CG_NCL);
   cfg.blockDim = dim3(CG_CLUSTER_THREADS);
