@@ -234,6 +234,11 @@ inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
   return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// The Mehrstellen Laplacian A on a real zero-boundary grid staged by TMA
+// (gpw_mehr_tma.cuh), for arguments chunked for 64 x 16 tiles.
+cudaError_t mehr_tma_f64(int mode, const StencilArgs& a, int nbatch, const GeneralCoefs& gc, cudaStream_t st);
+cudaError_t mehr_tma_f32(int mode, const StencilArgs& a, int nbatch, const GeneralCoefs& gc, cudaStream_t st);
+
 // The float32 level-0 residual restricted (K = 2, zero boundaries) into the
 // next level's rho and first Jacobi iterate in one TMA launch
 // (MODE_RESID_RESTRICT); `tune` times its tile variants instead.

@@ -93,8 +93,50 @@ static cudaError_t general_optin(K kern, size_t smem, std::mutex& mu, size_t& op
   return cudaSuccess;
 }
 
+// The operator is the Mehrstellen Laplacian A: 19 coefficients at exactly
+// the offsets of MEHR_OFF, in that order.
+static bool is_mehrstellen_a(const GeneralCoefs& gc) {
+  if (gc.ncoef != MEHR_NC || gc.mp != 1) return false;
+  for (int c = 0; c < MEHR_NC; ++c)
+    for (int e = 0; e < 3; ++e)
+      if (gc.off[c][e] != MEHR_OFF[c][e]) return false;
+  return true;
+}
+
+static bool aligned16(const void* p);
+static bool view_tma_ok(const GridView& v, size_t es, int nbatch);
+
+template <typename T, int MODE>
+static cudaError_t run_mehrstellen(const StencilArgs& a0, const OpDesc& d, int nbatch, cudaStream_t st) {
+  using C = MehrCfg;
+  StencilArgs a = a0;
+  const GridView& v = a.vout;
+  dim3 grid((v.n[2] + C::TZ - 1) / C::TZ, (v.n[1] + C::TY - 1) / C::TY, 1);
+  choose_chunks(v.n[0], (int64_t)grid.x * grid.y * nbatch, 4, a.zchunk, a.nchunk);
+  grid.z = a.nchunk * nbatch;
+  a.nblk_seg = grid.x * grid.y * a.nchunk;
+  // zero boundaries on 16-byte-pitched grids: planes staged by TMA
+  if (!d.periodic[0] && !d.periodic[1] && !d.periodic[2] && a.in != a.out && aligned16(a.in) &&
+      view_tma_ok(a.vin, sizeof(T), nbatch) && tensor_map_encoder()) {
+    if constexpr (sizeof(T) == 8) return mehr_tma_f64(MODE, a, nbatch, d.gc, st);
+    else return mehr_tma_f32(MODE, a, nbatch, d.gc, st);
+  }
+  a.gdepth = 4;  // planes loaded ahead (7 planes of 9.5 KB for float64)
+  const size_t smem = (size_t)(3 + a.gdepth) * C::PS * sizeof(T);
+  auto kern = mehrstellen_kernel<T, MODE>;
+  static std::once_flag once;
+  cudaError_t e = cudaSuccess;
+  std::call_once(once, [&] { e = smem_optin(kern, smem); });
+  if (e != cudaSuccess) return e;
+  kern<<<grid, dim3(C::NTX, C::NTY), smem, st>>>(a, d.gc);
+  return cudaGetLastError();
+}
+
 template <typename T, int MODE>
 static cudaError_t run_general(const StencilArgs& a0, const OpDesc& d, int nbatch, cudaStream_t st) {
+  if constexpr (!EltTraits<T>::cpx && (MODE == MODE_APPLY || MODE == MODE_RESIDUAL || MODE == MODE_JACOBI)) {
+    if (is_mehrstellen_a(d.gc)) return run_mehrstellen<T, MODE>(a0, d, nbatch, st);
+  }
   StencilArgs a = a0;
   const GridView& v = a.vout;
   const int mp = d.mp;

@@ -150,6 +150,16 @@ __device__ __forceinline__ void fix_plane(T* slot, const GridView& v, const Boun
 // ------------------------------------------------------------------ general
 constexpr int GEN_TZ = 32, GEN_TY = 8;
 
+// The weighted-Jacobi update of c/bmgs/relax.c:62, (1 - w) b + w (src - x) / c0,
+// with every operation rounded on its own (no contraction into a fused
+// multiply-add), as the reference's C evaluates it.
+__device__ __forceinline__ double jacobi_rn(double w, double cur, double rho, double x, double c0) {
+  return __dadd_rn(__dmul_rn(1.0 - w, cur), __ddiv_rn(__dmul_rn(w, __dsub_rn(rho, x)), c0));
+}
+__device__ __forceinline__ float jacobi_rn(float w, float cur, float rho, float x, float c0) {
+  return __fadd_rn(__fmul_rn(1.0f - w, cur), __fdiv_rn(__fmul_rn(w, __fsub_rn(rho, x)), c0));
+}
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(GEN_TZ* GEN_TY)
     general_stencil_kernel(const StencilArgs a, const GeneralCoefs k) {
@@ -224,7 +234,7 @@ __global__ void __launch_bounds__(GEN_TZ* GEN_TY)
               static_cast<T*>(a.out)[oi] = cur;  // relax is real-only (asserted on host)
             } else {
               const S w = (S)a.w, c0 = (S)a.c0;
-              static_cast<T*>(a.out)[oi] = (S(1) - w) * cur + (w * (rho - acc)) / c0;
+              static_cast<T*>(a.out)[oi] = jacobi_rn(w, cur, rho, acc, c0);
             }
           }
         }
@@ -477,8 +487,196 @@ __global__ void __launch_bounds__(GenBlk<T, MP, PY_, NTY_>::NT, 2)
                 static_cast<T*>(a.out)[oi] = cur;  // relax is real-only (asserted on host)
               } else {
                 const S w = (S)a.w, c0 = (S)a.c0;
-                static_cast<T*>(a.out)[oi] = (S(1) - w) * cur + (w * (rho - r)) / c0;
+                static_cast<T*>(a.out)[oi] = jacobi_rn(w, cur, rho, r, c0);
               }
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if constexpr (MODE == MODE_RESIDUAL) {
+    if (!a.gsum.partial) return;  // residual without its norm
+    double tot = block_sum(sumsq, red);
+    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
+    grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);
+  }
+}
+
+// ------------------------------------------------------------------ Mehrstellen A
+// The O(h^4) Mehrstellen Laplacian A (gpaw/fd_operators.py LaplaceA: 19
+// points, the centre, the 6 faces and the 12 edges of [-1, 1]^3, in that
+// table order) on real grids, with the general kernel's arithmetic (each
+// output sums its coefficients in table order with unfused multiply and add:
+// bit-identical to c/bmgs/fd.c) but with the offsets known at compile time:
+// each thread computes 2 x 2 adjacent outputs and holds the row segments they
+// share in registers, 10 shared-memory values per output instead of 19.
+// MEHR_OFF is the table order the launcher checks the operator against.
+constexpr int MEHR_NC = 19;
+constexpr signed char MEHR_OFF[MEHR_NC][3] = {
+    {0, 0, 0},   {-1, 0, 0},  {1, 0, 0},   {0, -1, 0},  {0, 1, 0},  {0, 0, -1}, {0, 0, 1},
+    {0, -1, -1}, {0, -1, 1},  {0, 1, -1},  {0, 1, 1},   {-1, 0, -1}, {-1, 0, 1}, {1, 0, -1},
+    {1, 0, 1},   {-1, -1, 0}, {-1, 1, 0},  {1, -1, 0},  {1, 1, 0}};
+struct MehrCfg {
+  static constexpr int NTX = 32, NTY = 8;  // threads; each 2 (axis 2) x 2 (axis 1) outputs
+  static constexpr int TZ = 2 * NTX, TY = 2 * NTY, NT = NTX * NTY;
+  static constexpr int H = TY + 2, W = TZ + 2, PS = H * W;
+  static constexpr int NCOL = (W + NT - 1) / NT;
+};
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(MehrCfg::NT, 2) mehrstellen_kernel(const StencilArgs a, const GeneralCoefs k) {
+  static_assert(!EltTraits<T>::cpx, "real grids");
+  using C = MehrCfg;
+  constexpr int W = C::W, H = C::H, PS = C::PS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = reinterpret_cast<T*>(smem_raw);
+  __shared__ double red[32];
+  const int D = a.gdepth, NP = 3 + D;
+  const int b = blockIdx.z / a.nchunk, chunk = blockIdx.z - b * a.nchunk;
+  if (a.active && !a.active[b]) return;
+  const int x0 = blockIdx.x * C::TZ, y0 = blockIdx.y * C::TY;
+  const int n0 = a.vout.n[0];
+  const int z0 = chunk * a.zchunk;
+  const int z1 = min(n0, z0 + a.zchunk);
+  const T* in = static_cast<const T*>(a.in) + (int64_t)b * a.vin.sb;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + C::NTX * ty;
+  const Boundary& bc = a.bc;
+  double sumsq = 0.0;
+  // this thread's staged cells: rows ty + NTY q, columns tx + 32 m (W = 66:
+  // three column slots, the third for two lanes)
+  constexpr int NROW = (H + C::NTY - 1) / C::NTY, NCOLS = (W + 31) / 32;
+  int64_t roff[NROW];
+  int jx[NCOLS];
+  unsigned rowok = 0, colok = 0;
+#pragma unroll
+  for (int m = 0; m < NCOLS; ++m) {
+    const int c = tx + 32 * m;
+    int s;
+    if (c < W && wrap_axis(x0 - 1 + c, a.vin.n[2], bc.periodic[2], jx[m], s)) colok |= 1u << m;
+  }
+#pragma unroll
+  for (int q = 0; q < NROW; ++q) {
+    const int r = ty + C::NTY * q;
+    int j1 = 0, s;
+    if (r < H && wrap_axis(y0 - 1 + r, a.vin.n[1], bc.periodic[1], j1, s)) rowok |= 1u << q;
+    roff[q] = (int64_t)j1 * a.vin.s1;
+  }
+  // outputs (rows y0 + 2 ty + i, columns x0 + 2 tx + j): inside the grid, offsets
+  int64_t obase[2][2], rbase[2][2];
+  unsigned omask = 0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int y = y0 + 2 * ty + i, x = x0 + 2 * tx + j;
+      if (y < a.vout.n[1] && x < a.vout.n[2]) omask |= 1u << (2 * i + j);
+      obase[i][j] = (int64_t)b * a.vout.sb + (int64_t)y * a.vout.s1 + x;
+      rbase[i][j] = (int64_t)b * a.vrho.sb + (int64_t)y * a.vrho.s1 + x;
+    }
+  // the coefficients, in table order
+  T cf[MEHR_NC];
+#pragma unroll
+  for (int c = 0; c < MEHR_NC; ++c) cf[c] = (T)k.coef[c];
+
+  if (z0 < z1) {
+    auto load = [&](int p) {
+      int j0, s0;
+      const bool ok0 = wrap_axis(p, a.vin.n[0], bc.periodic[0], j0, s0);
+      T* slot = ring + ((p - z0 + 1) % NP) * PS;
+      const T* base = in + (int64_t)j0 * a.vin.s0;
+#pragma unroll
+      for (int q = 0; q < NROW; ++q) {
+        const int r = ty + C::NTY * q;
+#pragma unroll
+        for (int m = 0; m < NCOLS; ++m) {
+          const int c = tx + 32 * m;
+          if (r < H && c < W) {
+            const bool ok = ok0 && ((rowok >> q) & (colok >> m) & 1u);
+            cp_async<sizeof(T)>(slot + r * W + c, ok ? base + roff[q] + jx[m] : in, ok);
+          }
+        }
+      }
+    };
+    for (int p = z0 - 1; p <= z0 + 1; ++p) load(p);
+    cp_async_commit();
+    for (int d = 1; d < D; ++d) {
+      if (z0 + d < z1) load(z0 + 1 + d);
+      cp_async_commit();
+    }
+    // this thread's first output cell (row 2 ty + 1, column 2 tx + 1 of a slot)
+    const int cell = (2 * ty + 1) * W + 2 * tx + 1;
+    for (int o = z0; o < z1; ++o) {
+      if (o + D < z1) load(o + 1 + D);
+      cp_async_commit();
+      switch (D) {
+        case 1: cp_async_wait<1>(); break;
+        case 2: cp_async_wait<2>(); break;
+        case 3: cp_async_wait<3>(); break;
+        default: cp_async_wait<4>(); break;
+      }
+      __syncthreads();
+      const int cs = (o - z0 + 1) % NP;
+      const T* pm = ring + ((cs + NP - 1) % NP) * PS + cell;  // plane o - 1
+      const T* pc = ring + cs * PS + cell;                    // plane o
+      const T* pp = ring + ((cs + 1) % NP) * PS + cell;       // plane o + 1
+      // row segments: columns -1 .. 2 around the first output column;
+      // plane o: rows -1 .. 2; planes o -+ 1: rows 0, 1 (and rows -1, 2 at
+      // the output columns only)
+      T c0[4][4], cm[2][4], cp[2][4], cmr[2][2], cpr[2][2];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) c0[r][e] = pc[(r - 1) * W + e - 1];
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          cm[r][e] = pm[r * W + e - 1];
+          cp[r][e] = pp[r * W + e - 1];
+        }
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        cmr[0][e] = pm[-W + e];
+        cmr[1][e] = pm[2 * W + e];
+        cpr[0][e] = pp[-W + e];
+        cpr[1][e] = pp[2 * W + e];
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          // the value of coefficient c at output (i, j), table order
+          const T v[MEHR_NC] = {c0[i + 1][j + 1],
+                                cm[i][j + 1],     cp[i][j + 1],
+                                c0[i][j + 1],     c0[i + 2][j + 1],
+                                c0[i + 1][j],     c0[i + 1][j + 2],
+                                c0[i][j],         c0[i][j + 2],     c0[i + 2][j],     c0[i + 2][j + 2],
+                                cm[i][j],         cm[i][j + 2],     cp[i][j],         cp[i][j + 2],
+                                i == 0 ? cmr[0][j] : cm[0][j + 1], i == 0 ? cm[1][j + 1] : cmr[1][j],
+                                i == 0 ? cpr[0][j] : cp[0][j + 1], i == 0 ? cp[1][j + 1] : cpr[1][j]};
+          T acc = T(0);
+#pragma unroll
+          for (int c = (MODE == MODE_JACOBI) ? 1 : 0; c < MEHR_NC; ++c) acc = mac_rn(cf[c], v[c], acc);
+          if (!((omask >> (2 * i + j)) & 1u)) continue;
+          const T cur = v[0];
+          const int64_t oi = obase[i][j] + (int64_t)o * a.vout.s0;
+          if constexpr (MODE == MODE_APPLY) {
+            using S = typename EltTraits<T>::S;
+            if (a.pot) acc = fmac(static_cast<const S*>(a.pot)[oi - (int64_t)b * a.vout.sb], cur, acc);
+            if (a.aux) acc = fmac((S)a.aux_scale, static_cast<const T*>(a.aux)[oi], acc);
+            static_cast<T*>(a.out)[oi] = acc;
+          } else {
+            const T rho = static_cast<const T*>(a.rho)[rbase[i][j] + (int64_t)o * a.vrho.s0];
+            if constexpr (MODE == MODE_RESIDUAL) {
+              const T d = acc - rho;
+              if (a.out) static_cast<T*>(a.out)[oi] = d;
+              sumsq += norm2(d);
+            } else {
+              // (1 - w) * b + w * (src - x) / c0   (c/bmgs/relax.c:62)
+              const T w = (T)a.w, cc = (T)a.c0;
+              static_cast<T*>(a.out)[oi] = jacobi_rn(w, cur, rho, acc, cc);
             }
           }
         }

@@ -1,6 +1,7 @@
 // TMA star-stencil launches for float32 grids (apply, residual, Jacobi, the
 // Jacobi sweep that adds its result into float64 phi, and the residual
 // restricted into the next level).
+#include "gpw_mehr_tma.cuh"
 #include "gpw_tma_launch.cuh"
 
 namespace gpw {
@@ -20,6 +21,10 @@ cudaError_t tma_stencil_f32(int mode, int R, int var, const StencilArgs& a, int 
       return cudaErrorInvalidValue;
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t mehr_tma_f32(int mode, const StencilArgs& a, int nbatch, const GeneralCoefs& gc, cudaStream_t st) {
+  return mehr_tma_mode<float>(mode, a, nbatch, gc, st);
 }
 
 }  // namespace gpw

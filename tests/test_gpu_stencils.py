@@ -106,6 +106,45 @@ def test_mehrstellen(cuda):
             assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize('N', [(3, 3, 3), (20, 16, 18), (21, 35, 70), (21, 35, 65)])
+@pytest.mark.parametrize('pbc', [0, 1])
+def test_mehrstellen_a_modes(cuda, N, pbc):
+    """LaplaceA through its own kernels (compile-time offsets, register-held
+    row segments; planes staged by TMA where the grid has zero boundaries
+    and 16-byte rows, as the 64-point rows of (21, 35, 65) with zero
+    boundaries, else by cp.async) on zero and periodic grids with partial
+    tiles in both in-plane axes, batched: apply, residual and weighted
+    Jacobi bit-identical to the reference's order (c/bmgs/fd.c, relax.c);
+    float32 within 2e-6."""
+    import torch
+    from gpawdft_b200.fd_operators import LaplaceA
+    from oracle import stencils
+    gd, ogd = gds(N, tuple(0.21 * n for n in N), pbc)
+    op = LaplaceA(gd, 0.7)
+    c, o = stencils.laplace_A(ogd, 0.7)
+    oop = ol.FDOperator(c, o, ogd)
+    a = rand((3,) + tuple(gd.n_c), np.float64, 40)
+    s = rand((3,) + tuple(gd.n_c), np.float64, 41)
+    ref = np.zeros_like(a)
+    oop.apply(a, ref)
+    out = np.zeros_like(a)
+    op.apply(a, out)
+    assert np.array_equal(out, ref)
+    r = torch.empty(a.shape, dtype=torch.float64, device='cuda')
+    ss = op.residual(torch.from_numpy(a).cuda(), torch.from_numpy(s).cuda(), r)
+    assert np.array_equal(r.cpu().numpy(), ref - s)
+    assert np.allclose(ss.cpu().numpy(), ((ref - s).reshape(3, -1) ** 2).sum(1), rtol=1e-12)
+    g = a[0].copy()
+    og = a[0].copy()
+    op.relax(2, g, s[0], 2, 2.0 / 3.0)
+    oop.relax(2, og, s[0], 2, 2.0 / 3.0)
+    assert np.array_equal(g, og)
+    op32 = LaplaceA(gd, 0.7, np.float32)
+    out32 = np.zeros(a.shape, np.float32)
+    op32.apply(a.astype(np.float32), out32)
+    assert relerr(out32, ref) < 2e-6
+
+
 @pytest.mark.parametrize('N', [(2, 2, 2), (3, 5, 7), (8, 2, 9), (40, 33, 65)])
 @pytest.mark.parametrize('pbc', [0, 1])
 def test_odd_and_tiny_sizes(cuda, N, pbc):
