@@ -73,7 +73,9 @@ __device__ __forceinline__ void mbar_arrive(unsigned bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
 }
 
-template <typename T, int R, int VEC, int NW, int D, int WPR>
+// EPI: a potential or aux term is present (a.pot / a.aux); the plain apply
+// is compiled without their loads and branches.
+template <typename T, int R, int VEC, int NW, int D, int WPR, bool EPI>
 __global__ void __launch_bounds__(32 * NW, (BlochCfg<T, R, VEC, NW, D, WPR>::MINB))
     bloch_star_kernel(const __grid_constant__ CUtensorMap tmain, const __grid_constant__ CUtensorMap thalo,
                       const BlochArgs a, const BlochCoefs<typename EltTraits<T>::S> k) {
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(32 * NW, (BlochCfg<T, R, VEC, NW, D, WPR>::MIN
         }
 #pragma unroll
         for (int e = 0; e < VEC; ++e) part[j][e] = add(fmac(k.cc, c[j][e], py[e]), pz[e]);
-        if (a.pot && p >= z0 && p < z1 && j < nrows_ok) {
+        if (EPI && a.pot && p >= z0 && p < z1 && j < nrows_ok) {
           // local potential of this (in-range) plane: its part is output p's
           using S = typename EltTraits<T>::S;
           const S* pr = static_cast<const S*>(a.pot) + (int64_t)p * a.vout.s0 + (int64_t)(ylo + j) * a.vout.s1 + xb;
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(32 * NW, (BlochCfg<T, R, VEC, NW, D, WPR>::MIN
       // output plane o is complete: logical slot 0 = physical ph
       if (o >= z0 && nx > 0) {
         T* op0 = outb + (int64_t)o * a.vout.s0;
-        const T* ax0 = a.aux ? static_cast<const T*>(a.aux) + (op0 - static_cast<T*>(a.out)) : nullptr;
+        const T* ax0 = (EPI && a.aux) ? static_cast<const T*>(a.aux) + (op0 - static_cast<T*>(a.out)) : nullptr;
         using S = typename EltTraits<T>::S;
 #pragma unroll
         for (int j = 0; j < PY; ++j) {
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(32 * NW, (BlochCfg<T, R, VEC, NW, D, WPR>::MIN
 #pragma unroll
             for (int e = 0; e < VEC; ++e)
               if (e < nx)
-                op[e] = ax0 ? fmac((S)a.aux_scale, ax0[j * a.vout.s1 + e], acc[j][ph][e]) : acc[j][ph][e];
+                op[e] = (EPI && ax0) ? fmac((S)a.aux_scale, ax0[j * a.vout.s1 + e], acc[j][ph][e]) : acc[j][ph][e];
           }
         }
       }

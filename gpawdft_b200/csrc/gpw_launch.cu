@@ -51,8 +51,8 @@ static void choose_chunks(int n0, int64_t tiles, int minz, int& zchunk, int& nch
 }
 
 // ------------------------------------------------------------------ stencils
-template <typename T, int R, int MODE>
-static cudaError_t run_star(const StencilArgs& a0, const OpDesc& d, int nbatch, cudaStream_t st) {
+template <typename T, int R, int MODE, bool EPI>
+static cudaError_t run_star_epi(const StencilArgs& a0, const OpDesc& d, int nbatch, cudaStream_t st) {
   using C = StarCfg<R, T>;
   StencilArgs a = a0;
   const GridView& v = a.vout;
@@ -61,13 +61,21 @@ static cudaError_t run_star(const StencilArgs& a0, const OpDesc& d, int nbatch, 
   grid.z = a.nchunk * nbatch;
   a.nblk_seg = grid.x * grid.y * a.nchunk;
   const size_t smem = (size_t)C::NSTAGE * C::PS * sizeof(T);
-  auto kern = star_stencil_kernel<T, R, MODE>;
+  auto kern = star_stencil_kernel<T, R, MODE, EPI>;
   static std::once_flag once;
   cudaError_t e = cudaSuccess;
   std::call_once(once, [&] { e = smem_optin(kern, smem); });
   if (e != cudaSuccess) return e;
   kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, star_coefs_typed<typename EltTraits<T>::S>(d.sc));  // NT threads
   return cudaGetLastError();
+}
+
+template <typename T, int R, int MODE>
+static cudaError_t run_star(const StencilArgs& a, const OpDesc& d, int nbatch, cudaStream_t st) {
+  if constexpr (MODE == MODE_APPLY) {
+    if (a.pot || a.aux) return run_star_epi<T, R, MODE, true>(a, d, nbatch, st);
+  }
+  return run_star_epi<T, R, MODE, false>(a, d, nbatch, st);
 }
 
 // Tile of a general-offset launch for element size es and radius mp: the

@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(MehrCfg::NT, 2) mehrstellen_kernel(const Stenc
   const int z0 = chunk * a.zchunk;
   const int z1 = min(n0, z0 + a.zchunk);
   const T* in = static_cast<const T*>(a.in) + (int64_t)b * a.vin.sb;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + C::NTX * ty;
+  const int tx = threadIdx.x, ty = threadIdx.y;
   const Boundary& bc = a.bc;
   double sumsq = 0.0;
   // this thread's staged cells: rows ty + NTY q, columns tx + 32 m (W = 66:
@@ -748,6 +748,7 @@ struct StarLoader {
   using C = StarCfg<R, T>;
   int off[C::NLD];      // j1 * s1 + j2 (element offset inside a plane)
   unsigned valid = 0;   // bit k: cell k is inside the grid or a periodic image
+  unsigned wrapped = 0; // bit k: cell k is a periodic image along axis 1 or 2
   unsigned char side[C::NLD];  // wrap sides: bits 0-1 axis 1 (+1), bits 2-3 axis 2 (+1)
 
   __device__ __forceinline__ void init(const GridView& v, const Boundary& bc, int y0, int x0) {
@@ -761,6 +762,7 @@ struct StarLoader {
                       wrap_axis(x0 - R + c, v.n[2], bc.periodic[2], j2, s2);
       off[k] = ok ? (int)((int64_t)j1 * v.s1 + j2) : 0;
       if (ok) valid |= 1u << k;
+      if (ok && (s1 >= 0 || s2 >= 0)) wrapped |= 1u << k;
       side[k] = (unsigned char)((s1 + 1) | ((s2 + 1) << 2));
     }
   }
@@ -787,12 +789,14 @@ struct StarLoader {
       const int tid = threadIdx.x + blockDim.x * threadIdx.y;
       int j0, s0;
       if (!wrap_axis(p, v.n[0], bc.periodic[0], j0, s0)) return;
+      // on a plane inside the grid only the in-plane periodic images change
+      const unsigned todo = s0 < 0 ? wrapped : valid;
+      if (!todo) return;
 #pragma unroll
       for (int k = 0; k < C::NLD; ++k) {
         const int idx = tid + k * C::NT;
-        if (idx >= C::PS || !((valid >> k) & 1u)) continue;
+        if (idx >= C::PS || !((todo >> k) & 1u)) continue;
         const int s1 = (side[k] & 3) - 1, s2 = ((side[k] >> 2) & 3) - 1;
-        if (s0 < 0 && s1 < 0 && s2 < 0) continue;
         T val = slot[idx];
         if (s0 >= 0) val = phase_mul(bc.ph[0][s0], val);
         if (s1 >= 0) val = phase_mul(bc.ph[1][s1], val);
@@ -803,7 +807,9 @@ struct StarLoader {
   }
 };
 
-template <typename T, int R, int MODE>
+// EPI: an apply with a potential or aux term (a.pot / a.aux); the plain
+// apply is compiled without their loads and branches.
+template <typename T, int R, int MODE, bool EPI = false>
 __global__ void __launch_bounds__(StarCfg<R, T>::NT)
     star_stencil_kernel(const StencilArgs a, const StarCoefsT<typename EltTraits<T>::S> k) {
   using C = StarCfg<R, T>;
@@ -893,7 +899,7 @@ __global__ void __launch_bounds__(StarCfg<R, T>::NT)
           part = fmac((S)k.cz[R + q], row[q], part);
           part = fmac((S)k.cz[R - q], row[-q], part);
         }
-        if constexpr (MODE == MODE_APPLY) {
+        if constexpr (MODE == MODE_APPLY && EPI) {
           // local potential of this (in-range) plane: its part is output p's
           const int y = y0 + yb + j;
           if (a.pot && p >= z0 && p < z1 && xin && y < a.vout.n[1])
@@ -923,7 +929,7 @@ __global__ void __launch_bounds__(StarCfg<R, T>::NT)
             const T av = acc[j][0];
             if constexpr (MODE == MODE_APPLY) {
               static_cast<T*>(a.out)[oi] =
-                  a.aux ? fmac((S)a.aux_scale, static_cast<const T*>(a.aux)[oi], av) : av;
+                  (EPI && a.aux) ? fmac((S)a.aux_scale, static_cast<const T*>(a.aux)[oi], av) : av;
             } else if constexpr (MODE == MODE_RESIDUAL) {
               const T r = sub(av, rho[j]);
               if (a.out) static_cast<T*>(a.out)[oi] = r;
