@@ -431,7 +431,10 @@ cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in,
       }
     }
     const TmaChoice ch = tma_choice(dtype, d.R, mode, vout, nbatch);
-    return tma_launch(dtype, mode, d.R, ch, a, nbatch, d.sc, st);
+    // an apply with a potential or aux term runs its own kernel instance, on
+    // the plain apply's tuned tiles
+    const int lmode = (mode == MODE_APPLY && (a.pot || a.aux)) ? MODE_APPLY_EPI : mode;
+    return tma_launch(dtype, lmode, d.R, ch, a, nbatch, d.sc, st);
   }
   if (mode == MODE_APPLY && !active && bloch_path_ok(d, dtype, in, vin, out, vout, nbatch))
     return launch_bloch(d, dtype, a, nbatch, st);

@@ -122,7 +122,8 @@ struct TmaCfg {
   static constexpr int NS = KEEP_CENTRE ? R + D + 1 : D + 1;
   // per stage: the input plane (with halo), the rho plane of the output
   // completed at that step, and (JACOBI_ADD64) the float64 phi plane
-  static constexpr bool HAS_RHO = MODE != MODE_APPLY && MODE != MODE_JACOBI_SCALED_IN;  // (scaled: rho is the input)
+  static constexpr bool HAS_RHO =
+      MODE != MODE_APPLY && MODE != MODE_APPLY_EPI && MODE != MODE_JACOBI_SCALED_IN;  // (scaled: rho is the input)
   static constexpr bool HAS_AUX = MODE == MODE_JACOBI_ADD64;
   static constexpr int IN_BYTES = H * W * (int)sizeof(S);
   static constexpr int RHO_BYTES = HAS_RHO ? TY * TZ * (int)sizeof(S) : 0;
@@ -381,7 +382,7 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
             }
 #pragma unroll
             for (int e = 0; e < VEC; ++e) p[e] += pz[e];
-            if constexpr (MODE == MODE_APPLY) {
+            if constexpr (MODE == MODE_APPLY_EPI) {
               // local potential of this (in-range) plane: its part is output
               // plane pfirst + s's
               const int pp = pfirst + s, y = y0 + yb + j;
@@ -419,9 +420,9 @@ __global__ void __launch_bounds__(TmaCfg<S, R, MODE, VAR>::NT, TmaCfg<S, R, MODE
                 if constexpr (C::HAS_RHO) rho = ldv<S, VEC>(rsl + (yb + j) * C::TZ + VEC * tx);
                 const int64_t oidx =
                     (int64_t)b * a.vout.sb + (int64_t)o * a.vout.s0 + (int64_t)y * a.vout.s1 + x;
-                if constexpr (MODE == MODE_APPLY) {
+                if constexpr (MODE == MODE_APPLY || MODE == MODE_APPLY_EPI) {
                   res = av;
-                  if (a.aux) {
+                  if (MODE == MODE_APPLY_EPI && a.aux) {
                     const S* xp = static_cast<const S*>(a.aux) + oidx;
                     const S g = (S)a.aux_scale;
 #pragma unroll

@@ -52,7 +52,10 @@ enum StencilMode {
   MODE_RESID_DC = 3,
   MODE_JACOBI_ADD64 = 4,
   MODE_RESID_RESTRICT = 5,
-  MODE_JACOBI_SCALED_IN = 6
+  MODE_JACOBI_SCALED_IN = 6,
+  // the TMA star kernel's apply with a potential or aux term (a plain
+  // MODE_APPLY instance is compiled without their loads and branches)
+  MODE_APPLY_EPI = 7
 };
 
 // Number of tile-shape variants of the TMA star kernel (gpw_star_tma.cuh).

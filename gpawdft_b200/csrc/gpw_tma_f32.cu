@@ -10,6 +10,7 @@ cudaError_t tma_stencil_f32(int mode, int R, int var, const StencilArgs& a, int 
                             int nchunk, cudaStream_t st) {
   switch (mode) {
     case MODE_APPLY: return tma_run_radius<float, MODE_APPLY>(R, var, a, nbatch, sc, nchunk, st);
+    case MODE_APPLY_EPI: return tma_run_radius<float, MODE_APPLY_EPI>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_RESIDUAL: return tma_run_radius<float, MODE_RESIDUAL>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_JACOBI: return tma_run_radius<float, MODE_JACOBI>(R, var, a, nbatch, sc, nchunk, st);
     case MODE_JACOBI_ADD64: return tma_run_radius<float, MODE_JACOBI_ADD64>(R, var, a, nbatch, sc, nchunk, st);
