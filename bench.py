@@ -519,8 +519,7 @@ def run_ours(args, rank, world, dist):
     if rank == 0 and world == 1 and not args.no_secondary:
         # the other configurations' key numbers, measured after the timed
         # region on the same GPU (each also runs alone: --workload bands96 /
-        # general / mixed192; the 512-solve uneven batch is left out, its
-        # densities take most of a minute to generate on the host)
+        # general / mixed192 / uneven512)
         import copy
         sa = copy.copy(args)
         sa.steps = min(args.steps, 10)
@@ -528,7 +527,7 @@ def run_ours(args, rank, world, dist):
         torch.cuda.empty_cache()
         sec = {}
         for key, fn in (('bands96', bands_line), ('general', general_line),
-                        ('mixed192', mixed192_line)):
+                        ('mixed192', mixed192_line), ('uneven512', uneven_line)):
             w0 = time.time()
             line = fn(sa)
             line['wall_s'] = time.time() - w0
@@ -771,6 +770,10 @@ def general_line(args):
 
 
 def run_uneven(args):
+    print(json.dumps(uneven_line(args)), flush=True)
+
+
+def uneven_line(args):
     """512 independent solves, cubic N_c log-uniform in [32, 128] rounded to
     multiples of 8 (seed 5), each density 4-32 neutral Gaussians (h = 0.2 A),
     relative residual 1e-10, float32 inner / float64 outer.  Solves of one
@@ -845,7 +848,8 @@ def run_uneven(args):
             'ms_per_step': 1e3 * T,
             'step_ms_min': 1e3 * min(ts),
             'vcycles_mean': float(np.mean(np.concatenate(nits)))}
-    print(json.dumps(line), flush=True)
+    del solvers, phis, rhos
+    return line
 
 
 def run_learned(args):
