@@ -307,8 +307,11 @@ cudaError_t launch_bloch(const OpDesc& d, int dtype, const StencilArgs& sa, int 
     tuned = it != g_bloch_tune.end();
     if (tuned) ch = it->second;
   }
+  // the timed repetitions must leave the result of one launch: an aux term
+  // read from the output itself would accumulate, so that call runs untuned
+  const bool repeatable = !(sa.aux && sa.aux == out);
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  if (!tuned && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+  if (!tuned && repeatable && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
       float best = 1e30f;

@@ -422,8 +422,11 @@ cudaError_t launch_stencil(const OpDesc& d, int dtype, int mode, const void* in,
   if (tma_path_ok(d, dtype, mode, in, vin, out, vout, rho, vrho, nbatch)) {
     // first launch of an untuned shape outside stream capture: tune it now
     // (apply / residual / Jacobi recompute their output from inputs they do
-    // not overwrite, so the timed repetitions leave the same result)
-    if (!active && out != rho && g_force_var.load() < 0 && !tma_tuned(dtype, d.R, mode, vout, nbatch)) {
+    // not overwrite, so the timed repetitions leave the same result; an aux
+    // term read from the output itself is such an input, so that call runs
+    // on the default tiles untuned)
+    if (!active && out != rho && (!aux || aux != out) && g_force_var.load() < 0 &&
+        !tma_tuned(dtype, d.R, mode, vout, nbatch)) {
       cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
       if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
         cudaError_t te = tune_stencil(d, dtype, mode, in, vin, out, vout, rho, vrho, nullptr, nbatch, w, gs, st);

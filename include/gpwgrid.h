@@ -100,7 +100,8 @@ int gpw_operator_apply_potential(gpw_operator *op, int dtype, const void *in,
 
 /* The apply with the NumPy glue that follows it folded into its output
  * stage: out = A in + pot in + aux_scale aux (pot and aux may be NULL; aux
- * is `nin` grids of the element type, as `out`).  Together with an operator
+ * is `nin` grids of the element type, as `out`, and may be `out` itself:
+ * such a call is never timed by the tile autotuner).  Together with an operator
  * whose coefficients were scaled on the host it replaces sequences such as
  * the preconditioner's `kin0.apply(d0, q0); q0 -= residuals; axpy(-step,
  * q0, d0); d0 *= -1` (gpaw/preconditioner.py:56-60) by one pass.          */

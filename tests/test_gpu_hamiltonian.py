@@ -190,3 +190,29 @@ def test_apply_fused_aux(cuda, case):
     okin.apply(psi.astype(oracle_dtype(dtype)), o2, ph)
     want2 = 0.3 * o2 - 1.25 * psi.astype(oracle_dtype(dtype))
     assert relerr(out.cpu().numpy(), want2) < TOL[np.dtype(dtype)]
+
+
+@pytest.mark.parametrize('case', ['bloch-c128', 'tma-f64'])
+def test_apply_fused_aux_in_place(cuda, case):
+    """aux read from the output itself (out = A in + vt in + g out) on a shape
+    the autotuner has not seen: its timing launches must not run first."""
+    import torch
+    from gpawdft_b200.fd_operators import Laplace
+    from gpawdft_b200.grid_descriptor import GridDescriptor
+    dtype, N, pbc = ((complex, (10, 24, 32), 1) if case == 'bloch-c128'
+                     else (float, (22, 18, 26), 0))
+    cell = tuple(0.2 * n for n in N)
+    gd = GridDescriptor(N, cell, pbc)
+    ogd = OGD(N, cell, pbc)
+    kin = Laplace(gd, -0.5, 3, dtype)
+    okin = ol.Laplace(ogd, -0.5, 3, oracle_dtype(dtype), BACKEND)
+    psi = rand((2,) + tuple(gd.n_c), dtype, 31)
+    aux = rand((2,) + tuple(gd.n_c), dtype, 32)
+    vt = rand(tuple(gd.n_c), np.float64, 33)
+    ph = None if pbc == 0 else phase_cd_for_k(ogd, (0.2, 0.1, -0.25))
+    want = _oracle(okin, psi, vt, ph) - 0.7 * aux
+    x = torch.from_numpy(psi).cuda()
+    out = torch.from_numpy(aux).cuda()
+    kin.apply_fused(x, out, ph, vt_g=torch.from_numpy(vt).cuda(), aux=out,
+                    aux_scale=-0.7)
+    assert relerr(out.cpu().numpy(), want) < TOL[np.dtype(dtype)]
