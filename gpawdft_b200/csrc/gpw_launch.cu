@@ -61,12 +61,17 @@ static cudaError_t run_star_epi(const StencilArgs& a0, const OpDesc& d, int nbat
   grid.z = a.nchunk * nbatch;
   a.nblk_seg = grid.x * grid.y * a.nchunk;
   const size_t smem = (size_t)C::NSTAGE * C::PS * sizeof(T);
-  auto kern = star_stencil_kernel<T, R, MODE, EPI>;
+  using S = typename EltTraits<T>::S;
+  void (*kern)(StencilArgs, StarCoefsT<S>);
+  if constexpr (sizeof(T) >= 16)
+    kern = star_stencil_kernel_2cta<T, R, MODE, EPI>;
+  else
+    kern = star_stencil_kernel<T, R, MODE, EPI>;
   static std::once_flag once;
   cudaError_t e = cudaSuccess;
   std::call_once(once, [&] { e = smem_optin(kern, smem); });
   if (e != cudaSuccess) return e;
-  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, star_coefs_typed<typename EltTraits<T>::S>(d.sc));  // NT threads
+  kern<<<grid, dim3(C::TZ, C::NTY), smem, st>>>(a, star_coefs_typed<S>(d.sc));  // NT threads
   return cudaGetLastError();
 }
 
@@ -236,7 +241,7 @@ int stencil_blocks_per_member(const OpDesc& d, int mode, const GridView& v, int 
   };
   int nblk;
   if (use_star) {
-    nblk = blocks(32, GPW_STAR_TY, 2 * d.R + 2);
+    nblk = blocks(32, d.real ? GPW_STAR_TY : GPW_STAR_TY / 2, 2 * d.R + 2);  // complex128: half-height tiles
   } else {
     // the tile depends on the element size: the most CTAs over the op's types
     nblk = 0;

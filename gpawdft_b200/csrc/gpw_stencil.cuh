@@ -706,11 +706,14 @@ __global__ void __launch_bounds__(MehrCfg::NT, 2) mehrstellen_kernel(const Stenc
 #ifndef GPW_STAR_NS
 #define GPW_STAR_NS 3
 #endif
+// 16-byte elements (complex128) take half-height tiles: two CTAs of 256
+// threads per SM (star_stencil_kernel_2cta) instead of one of 512, so one
+// CTA's plane barrier overlaps the other's work.
 template <int R, typename T>
 struct StarCfg {
   static constexpr int TZ = 32;
   static constexpr int PY = (sizeof(T) >= 16) ? (GPW_STAR_PY > 2 ? 2 : GPW_STAR_PY) : GPW_STAR_PY;
-  static constexpr int TY = GPW_STAR_TY;
+  static constexpr int TY = (sizeof(T) >= 16) ? GPW_STAR_TY / 2 : GPW_STAR_TY;
   static constexpr int NTY = TY / PY;
   static constexpr int NT = TZ * NTY;
   static constexpr int H = TY + 2 * R, W = TZ + 2 * R, PS = H * W;
@@ -812,9 +815,8 @@ struct StarLoader {
 
 // EPI: an apply with a potential or aux term (a.pot / a.aux); the plain
 // apply is compiled without their loads and branches.
-template <typename T, int R, int MODE, bool EPI = false>
-__global__ void __launch_bounds__(StarCfg<R, T>::NT)
-    star_stencil_kernel(const StencilArgs a, const StarCoefsT<typename EltTraits<T>::S> k) {
+template <typename T, int R, int MODE, bool EPI>
+__device__ __forceinline__ void star_stencil_body(const StencilArgs& a, const StarCoefsT<typename EltTraits<T>::S>& k) {
   using C = StarCfg<R, T>;
   using S = typename EltTraits<T>::S;
   constexpr int PY = C::PY, W = C::W, PS = C::PS, NS = C::NSTAGE;
@@ -962,6 +964,19 @@ __global__ void __launch_bounds__(StarCfg<R, T>::NT)
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * chunk);
     grid_sum_finish(a.gsum, b, blk, a.nblk_seg, tot, red);
   }
+}
+
+template <typename T, int R, int MODE, bool EPI = false>
+__global__ void __launch_bounds__(StarCfg<R, T>::NT)
+    star_stencil_kernel(const StencilArgs a, const StarCoefsT<typename EltTraits<T>::S> k) {
+  star_stencil_body<T, R, MODE, EPI>(a, k);
+}
+
+// 16-byte elements: the same kernel with registers capped for two CTAs per SM
+template <typename T, int R, int MODE, bool EPI = false>
+__global__ void __launch_bounds__(StarCfg<R, T>::NT, 2)
+    star_stencil_kernel_2cta(const StencilArgs a, const StarCoefsT<typename EltTraits<T>::S> k) {
+  star_stencil_body<T, R, MODE, EPI>(a, k);
 }
 
 }  // namespace gpw
